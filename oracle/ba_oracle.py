@@ -1,0 +1,775 @@
+"""CPU oracle: a float64 numpy restatement of ceres-torch's Schur bundle-adjustment path.
+
+TEST INFRASTRUCTURE ONLY. This module is the checker that the CUDA path is
+compared against; the product never imports it. Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference arm may
+load it.
+
+What it restates, function by function (reference paths are relative to the
+ceres-torch project root):
+
+* ``angle_axis_rotate_point``   rotation.py:104-110 (angle-axis -> quaternion, with the
+  theta<=eps branch k = 0.5 - theta^2/48), rotation.py:68-69 (normalize), rotation.py:211-214
+  (unit-quaternion rotate) and rotation.py:221-222.
+* ``snavely_residuals``         examples/simple_bundle_adjuster.py:73-79 (and the residual
+  ``snavely_reprojection(camera, point) - observation`` built at :105).
+* Jacobians                     costs.py:31-44 differentiates that formula with autograd; the
+  oracle carries forward-mode tangents through the same operation sequence (``_Dual``), so it is
+  the same derivative, including the quaternion normalisation.
+* ``LOSSES``                    losses.py:21-133 (Trivial, Huber, SoftLOne, Cauchy, Arctan,
+  Tolerant, Tukey, Scaled, Composed).
+* ``robustify``                 losses.py:158-193 (Ceres corrector: sqrt(rho') scaling, Triggs
+  rank-1 term only when s>0 and rho''>0).
+* ``evaluate``                  problem.py:377-413 / :486-520 (cost = sum 0.5 rho, corrected
+  residuals and Jacobian, gradient J^T r).
+* ``jacobi_damping``            linear.py:539-551.
+* Schur system                  linear.py:794-839 (H = J^T J + diag(d), S = Hbb - Hba Haa^-1 Hab,
+  rhs = gb - Hba Haa^-1 ga) written block-sparsely: Haa is block diagonal (3x3 per point) in BA.
+* ``schur_solve_dense``         linear.py:667-699 (exact solve of S).
+* ``iterative_schur``           linear.py:702-776 with the PCG of linear.py:1216-1256 and the
+  preconditioners of linear.py:462-536 / :1156-1182 (SCHUR_JACOBI = Cholesky of each retained
+  block of S; JACOBI = clamped diagonal; IDENTITY).
+* ``solve``                     solver.py:35-357 (trust-region LM), with :798-802 (model
+  decrease), :805-820 (LM radius), :823-861 (step evaluator), :1165-1175 (convergence tests),
+  :661-676 (restore best state), :714-785 (parameter order, num_eliminate, visibility).
+
+Parity of this restatement is pinned against the reference itself by
+``tests/golden/make_golden.py`` (fixtures generated by running ceres-torch) and
+``tests/test_oracle_golden.py``.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+EPS64 = float(np.finfo(np.float64).eps)
+TINY64 = float(np.finfo(np.float64).tiny)
+
+
+# --------------------------------------------------------------------------------------
+# Forward-mode tangents
+# --------------------------------------------------------------------------------------
+class _Dual:
+    """Value ``v`` [n] with tangents ``d`` [n, k]; just enough algebra for the projection."""
+
+    __slots__ = ("v", "d")
+
+    def __init__(self, v, d):
+        self.v = v
+        self.d = d
+
+    def __add__(self, o):
+        if isinstance(o, _Dual):
+            return _Dual(self.v + o.v, self.d + o.d)
+        return _Dual(self.v + o, self.d)
+
+    __radd__ = __add__
+
+    def __sub__(self, o):
+        if isinstance(o, _Dual):
+            return _Dual(self.v - o.v, self.d - o.d)
+        return _Dual(self.v - o, self.d)
+
+    def __rsub__(self, o):
+        return _Dual(o - self.v, -self.d)
+
+    def __neg__(self):
+        return _Dual(-self.v, -self.d)
+
+    def __mul__(self, o):
+        if isinstance(o, _Dual):
+            return _Dual(self.v * o.v, self.d * o.v[:, None] + o.d * self.v[:, None])
+        return _Dual(self.v * o, self.d * o)
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, o):
+        if isinstance(o, _Dual):
+            q = self.v / o.v
+            return _Dual(q, (self.d - o.d * q[:, None]) / o.v[:, None])
+        return _Dual(self.v / o, self.d / o)
+
+
+def _dsqrt(a: _Dual) -> _Dual:
+    v = np.sqrt(a.v)
+    safe = np.where(v > 0.0, 2.0 * v, 1.0)
+    d = np.where((v > 0.0)[:, None], a.d / safe[:, None], 0.0)
+    return _Dual(v, d)
+
+
+def _dsin(a: _Dual) -> _Dual:
+    return _Dual(np.sin(a.v), a.d * np.cos(a.v)[:, None])
+
+
+def _dcos(a: _Dual) -> _Dual:
+    return _Dual(np.cos(a.v), -a.d * np.sin(a.v)[:, None])
+
+
+def _dwhere(mask, a: _Dual, b: _Dual) -> _Dual:
+    return _Dual(np.where(mask, a.v, b.v), np.where(mask[:, None], a.d, b.d))
+
+
+def _cross(a, b):
+    return [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]
+
+
+def _snavely(cam: list, X: list, with_tangents: bool):
+    """rotation.py:104-110,68-69,211-214 + simple_bundle_adjuster.py:73-79, one op at a time."""
+    aa = cam[0:3]
+    theta = _dsqrt(aa[0] * aa[0] + aa[1] * aa[1] + aa[2] * aa[2])  # torch.linalg.norm
+    half = theta * 0.5
+    small = theta.v <= EPS64
+    one = _Dual(np.ones_like(theta.v), np.zeros_like(theta.d))
+    safe_theta = _dwhere(small, one, theta)
+    k = _dwhere(small, 0.5 - theta * theta / 48.0, _dsin(half) / safe_theta)
+    q = [_dcos(half), k * aa[0], k * aa[1], k * aa[2]]
+    qn = _dsqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+    qn = _dwhere(qn.v < TINY64, _Dual(np.full_like(qn.v, TINY64), np.zeros_like(qn.d)), qn)
+    q = [c / qn for c in q]
+    u = q[1:4]
+    c1 = _cross(u, X)
+    uv = [c * 2.0 for c in c1]
+    c2 = _cross(u, uv)
+    rp = [X[i] + q[0] * uv[i] + c2[i] for i in range(3)]
+    p = [rp[i] + cam[3 + i] for i in range(3)]
+    xp = -p[0] / p[2]
+    yp = -p[1] / p[2]
+    r2 = xp * xp + yp * yp
+    distortion = 1.0 + r2 * (cam[7] + cam[8] * r2)
+    fd = cam[6] * distortion
+    return fd * xp, fd * yp
+
+
+def snavely_residuals_and_jacobians(cameras, points, obs, ci, pi, *, jacobians=True):
+    """Raw (uncorrected) residuals [no,2] and Jacobians Jc [no,2,9], Jp [no,2,3]."""
+    cam = cameras[ci]
+    X = points[pi]
+    n = cam.shape[0]
+    k = 12 if jacobians else 0
+    eye = np.eye(12)
+    cd = [_Dual(cam[:, j].copy(), np.broadcast_to(eye[j, :k], (n, k)).copy()) for j in range(9)]
+    xd = [_Dual(X[:, j].copy(), np.broadcast_to(eye[9 + j, :k], (n, k)).copy()) for j in range(3)]
+    u, v = _snavely(cd, xd, jacobians)
+    r = np.stack([u.v - obs[:, 0], v.v - obs[:, 1]], axis=1)
+    if not jacobians:
+        return r, None, None
+    J = np.stack([u.d, v.d], axis=1)  # [n, 2, 12]
+    return r, np.ascontiguousarray(J[:, :, :9]), np.ascontiguousarray(J[:, :, 9:])
+
+
+def angle_axis_rotate_point(aa: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """rotation.py:221-222 for row-aligned arrays."""
+    n = aa.shape[0]
+    z = np.zeros((n, 0))
+    aad = [_Dual(aa[:, j].copy(), z) for j in range(3)]
+    theta = _dsqrt(aad[0] * aad[0] + aad[1] * aad[1] + aad[2] * aad[2])
+    half = theta * 0.5
+    small = theta.v <= EPS64
+    safe = np.where(small, 1.0, theta.v)
+    kk = np.where(small, 0.5 - theta.v * theta.v / 48.0, np.sin(half.v) / safe)
+    q = np.stack([np.cos(half.v), kk * aa[:, 0], kk * aa[:, 1], kk * aa[:, 2]], axis=1)
+    q = q / np.maximum(np.linalg.norm(q, axis=1, keepdims=True), TINY64)
+    u = q[:, 1:]
+    uv = 2.0 * np.cross(u, X)
+    return X + q[:, :1] * uv + np.cross(u, uv)
+
+
+# --------------------------------------------------------------------------------------
+# Losses (losses.py:21-133) and the corrector (losses.py:158-193)
+# --------------------------------------------------------------------------------------
+def loss_rho(spec: tuple, s: np.ndarray):
+    """Returns (rho0, rho1, rho2) for a loss spec tuple, elementwise over ``s``."""
+    kind = spec[0]
+    if kind == "trivial":
+        return s.copy(), np.ones_like(s), np.zeros_like(s)
+    if kind == "huber":
+        a = float(spec[1])
+        b = a * a
+        mask = s <= b
+        sq = np.sqrt(np.maximum(s, TINY64))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rho0 = np.where(mask, s, 2.0 * a * sq - b)
+            rho1 = np.where(mask, 1.0, a / sq)
+            rho2 = np.where(mask, 0.0, -0.5 * a / (sq * s))
+        return rho0, rho1, rho2
+    if kind == "softlone":
+        b = float(spec[1]) ** 2
+        z = 1.0 + s / b
+        sz = np.sqrt(z)
+        return 2.0 * b * (sz - 1.0), 1.0 / sz, -0.5 / (b * z * sz)
+    if kind == "cauchy":
+        b = float(spec[1]) ** 2
+        z = 1.0 + s / b
+        return b * np.log(z), 1.0 / z, -1.0 / (b * z * z)
+    if kind == "arctan":
+        a = float(spec[1])
+        z = s / a
+        den = 1.0 + z * z
+        return a * np.arctan(z), 1.0 / den, -2.0 * z / (a * den * den)
+    if kind == "tolerant":
+        a, b = float(spec[1]), float(spec[2])
+        z = (s - a) / b
+        c = b * np.logaddexp(0.0, -a / b)
+        rho1 = 1.0 / (1.0 + np.exp(-z))
+        return b * np.logaddexp(0.0, z) - c, rho1, rho1 * (1.0 - rho1) / b
+    if kind == "tukey":
+        a2 = float(spec[1]) ** 2
+        z = s / a2
+        inner = 1.0 - z
+        mask = s <= a2
+        return (np.where(mask, (a2 / 3.0) * (1.0 - inner ** 3), a2 / 3.0),
+                np.where(mask, inner ** 2, 0.0),
+                np.where(mask, -2.0 * inner / a2, 0.0))
+    if kind == "scaled":
+        base = spec[1] if spec[1] is not None else ("trivial",)
+        r0, r1, r2 = loss_rho(base, s)
+        sc = float(spec[2])
+        return sc * r0, sc * r1, sc * r2
+    if kind == "composed":
+        g0, g1, g2 = loss_rho(spec[2], s)
+        f0, f1, f2 = loss_rho(spec[1], g0)
+        return f0, f1 * g1, f2 * g1 * g1 + f1 * g2
+    raise ValueError(f"unknown loss {spec!r}")
+
+
+def robustify(spec, r, Jc=None, Jp=None):
+    """losses.py:158-193 per residual block of size 2. Returns (cost_i, r', Jc', Jp')."""
+    s = np.sum(r * r, axis=1)
+    rho0, rho1, rho2 = loss_rho(spec, s)
+    sqrt_rho1 = np.sqrt(np.maximum(rho1, 0.0))
+    scale = sqrt_rho1.copy()
+    alpha_s = np.zeros_like(s)
+    corr = (s > 0.0) & (rho2 > 0.0)
+    if np.any(corr):
+        if np.any(rho1[corr] <= 0.0):
+            raise ValueError("Loss function has rho'' > 0 but rho' <= 0")
+        disc = 1.0 + 2.0 * s[corr] * rho2[corr] / rho1[corr]
+        alpha = 1.0 - np.sqrt(disc)
+        scale[corr] = sqrt_rho1[corr] / (1.0 - alpha)
+        alpha_s[corr] = alpha / s[corr]
+    r2 = scale[:, None] * r
+    if Jc is None:
+        return 0.5 * rho0, r2, None, None
+    out = []
+    for J in (Jc, Jp):
+        rTj = np.einsum("ni,nij->nj", r, J)
+        Jn = sqrt_rho1[:, None, None] * (J - alpha_s[:, None, None] * r[:, :, None] * rTj[:, None, :])
+        out.append(Jn)
+    return 0.5 * rho0, r2, out[0], out[1]
+
+
+# --------------------------------------------------------------------------------------
+# Problem structure
+# --------------------------------------------------------------------------------------
+@dataclass
+class OracleProblem:
+    cameras: np.ndarray
+    points: np.ndarray
+    observations: np.ndarray
+    camera_index: np.ndarray
+    point_index: np.ndarray
+    loss: tuple = ("trivial",)
+    camera_constant: np.ndarray | None = None
+    point_constant: np.ndarray | None = None
+
+    def __post_init__(self):
+        self.cameras = np.array(self.cameras, dtype=np.float64)
+        self.points = np.array(self.points, dtype=np.float64)
+        self.observations = np.asarray(self.observations, dtype=np.float64)
+        self.camera_index = np.asarray(self.camera_index, dtype=np.int64)
+        self.point_index = np.asarray(self.point_index, dtype=np.int64)
+        nc, npt = self.cameras.shape[0], self.points.shape[0]
+        if self.camera_constant is None:
+            self.camera_constant = np.zeros(nc, dtype=bool)
+        if self.point_constant is None:
+            self.point_constant = np.zeros(npt, dtype=bool)
+        self.active_cams = np.flatnonzero(~self.camera_constant)
+        self.active_pts = np.flatnonzero(~self.point_constant)
+        self.cam_col = np.full(nc, -1, dtype=np.int64)
+        self.cam_col[self.active_cams] = np.arange(self.active_cams.size)
+        self.pt_col = np.full(npt, -1, dtype=np.int64)
+        self.pt_col[self.active_pts] = np.arange(self.active_pts.size)
+
+
+@dataclass
+class Evaluation:
+    cost: float
+    r: np.ndarray
+    Jc: np.ndarray | None = None
+    Jp: np.ndarray | None = None
+
+
+def evaluate(prob: OracleProblem, cameras, points, *, jacobians=True) -> Evaluation:
+    """problem.py:377-413: cost = sum_i 0.5 rho_i; corrected residuals and Jacobians."""
+    r, Jc, Jp = snavely_residuals_and_jacobians(cameras, points, prob.observations, prob.camera_index,
+                                                 prob.point_index, jacobians=jacobians)
+    cost_i, r2, Jc2, Jp2 = robustify(prob.loss, r, Jc, Jp)
+    if jacobians:
+        Jc2 = Jc2 * (~prob.camera_constant[prob.camera_index])[:, None, None]
+        Jp2 = Jp2 * (~prob.point_constant[prob.point_index])[:, None, None]
+    return Evaluation(float(np.sum(cost_i)), r2, Jc2, Jp2)
+
+
+def jacobi_damping(col_sq: np.ndarray, radius: float, min_diag: float, max_diag: float, jacobi_scaling=True):
+    """linear.py:539-551."""
+    diag = col_sq if jacobi_scaling else np.ones_like(col_sq)
+    return np.clip(diag, min_diag, max_diag) / max(radius, EPS64)
+
+
+def _segment_sum(values: np.ndarray, keys: np.ndarray, n: int) -> np.ndarray:
+    out = np.zeros((n,) + values.shape[1:])
+    np.add.at(out, keys, values)
+    return out
+
+
+@dataclass
+class SchurSystem:
+    """Block-sparse pieces of linear.py:794-839 for BA (points eliminated)."""
+
+    Winv: np.ndarray        # [np_a, 3, 3]  Haa^-1 blocks
+    Fi: np.ndarray          # [no, 3, 9]    Jp_i^T Jc_i (Hab row blocks per observation)
+    U: np.ndarray           # [nc_a, 9, 9]  Hbb diagonal blocks (incl. damping)
+    ga: np.ndarray          # [np_a, 3]
+    gb: np.ndarray          # [nc_a, 9]
+    Winv_ga: np.ndarray     # [np_a, 3]
+    rhs: np.ndarray         # [nc_a, 9]
+    pt: np.ndarray          # [no] active point column per obs (-1 constant)
+    cam: np.ndarray         # [no] active camera column per obs (-1 constant)
+    n_cam: int
+    n_pt: int
+
+
+def build_schur(prob: OracleProblem, ev: Evaluation, damping_p: np.ndarray, damping_c: np.ndarray) -> SchurSystem:
+    pt = prob.pt_col[prob.point_index]
+    cam = prob.cam_col[prob.camera_index]
+    n_pt, n_cam = prob.active_pts.size, prob.active_cams.size
+    b = -ev.r
+    vp = pt >= 0
+    vc = cam >= 0
+    W = _segment_sum(np.einsum("nri,nrj->nij", ev.Jp[vp], ev.Jp[vp]), pt[vp], n_pt)
+    W[:, [0, 1, 2], [0, 1, 2]] += damping_p.reshape(n_pt, 3)
+    U = _segment_sum(np.einsum("nri,nrj->nij", ev.Jc[vc], ev.Jc[vc]), cam[vc], n_cam)
+    U[:, np.arange(9), np.arange(9)] += damping_c.reshape(n_cam, 9)
+    ga = _segment_sum(np.einsum("nri,nr->ni", ev.Jp[vp], b[vp]), pt[vp], n_pt)
+    gb = _segment_sum(np.einsum("nri,nr->ni", ev.Jc[vc], b[vc]), cam[vc], n_cam)
+    Winv = np.linalg.inv(W) if n_pt else np.zeros((0, 3, 3))
+    Winv_ga = np.einsum("nij,nj->ni", Winv, ga)
+    Fi = np.einsum("nri,nrj->nij", ev.Jp, ev.Jc)
+    both = vp & vc
+    contrib = np.einsum("nij,ni->nj", Fi[both], Winv_ga[pt[both]])
+    rhs = gb - _segment_sum(contrib, cam[both], n_cam)
+    return SchurSystem(Winv, Fi, U, ga, gb, Winv_ga, rhs, pt, cam, n_cam, n_pt)
+
+
+def schur_matvec(sys: SchurSystem, x: np.ndarray) -> np.ndarray:
+    """S x = Hbb x - Hba Haa^-1 Hab x, streamed per observation (x: [nc_a, 9])."""
+    y = np.einsum("nij,nj->ni", sys.U, x)
+    both = (sys.pt >= 0) & (sys.cam >= 0)
+    pt, cam, F = sys.pt[both], sys.cam[both], sys.Fi[both]
+    t = _segment_sum(np.einsum("nij,nj->ni", F, x[cam]), pt, sys.n_pt)
+    s = np.einsum("nij,nj->ni", sys.Winv, t)
+    y -= _segment_sum(np.einsum("nij,ni->nj", F, s[pt]), cam, sys.n_cam)
+    return y
+
+
+def schur_dense(sys: SchurSystem) -> np.ndarray:
+    """Explicit S [9 nc_a, 9 nc_a] (small problems only)."""
+    n = sys.n_cam
+    S = np.zeros((n, 9, n, 9))
+    S[np.arange(n), :, np.arange(n), :] = sys.U
+    both = (sys.pt >= 0) & (sys.cam >= 0)
+    idx = np.flatnonzero(both)
+    order = idx[np.argsort(sys.pt[idx], kind="stable")]
+    pts = sys.pt[order]
+    bounds = np.flatnonzero(np.diff(pts)) + 1
+    for grp in np.split(order, bounds):
+        if grp.size == 0:
+            continue
+        p = sys.pt[grp[0]]
+        G = sys.Fi[grp]                              # [L, 3, 9]
+        WG = np.einsum("ij,ljk->lik", sys.Winv[p], G)  # [L, 3, 9]
+        blk = np.einsum("lia,mib->lamb", G, WG)      # [L, 9, L, 9]
+        cams = sys.cam[grp]
+        for a in range(grp.size):
+            for b_ in range(grp.size):
+                S[cams[a], :, cams[b_], :] -= blk[a, :, b_, :]
+    return S.reshape(9 * n, 9 * n)
+
+
+def schur_diag_blocks(sys: SchurSystem) -> np.ndarray:
+    """Retained 9x9 diagonal blocks of S (the SCHUR_JACOBI blocks), duplicates of a
+    camera inside one track summed before the W^-1 product."""
+    both = (sys.pt >= 0) & (sys.cam >= 0)
+    idx = np.flatnonzero(both)
+    key = sys.pt[idx] * max(sys.n_cam, 1) + sys.cam[idx]
+    uk, inv = np.unique(key, return_inverse=True)
+    G = _segment_sum(sys.Fi[idx], inv, uk.size)       # [groups, 3, 9]
+    gp = uk // max(sys.n_cam, 1)
+    gc = uk % max(sys.n_cam, 1)
+    blk = np.einsum("gia,gij,gjb->gab", G, sys.Winv[gp], G)
+    D = sys.U.copy()
+    np.subtract.at(D, gc, blk)
+    return D
+
+
+class _Preconditioner:
+    """linear.py:462-536 / :1156-1182 / :53-79 for the retained camera blocks."""
+
+    def __init__(self, kind: str, diag_blocks: np.ndarray):
+        self.kind = kind
+        if kind == "IDENTITY":
+            return
+        if kind == "SCHUR_JACOBI":
+            self.factors = []
+            for blk in diag_blocks:
+                try:
+                    self.factors.append((np.linalg.cholesky(blk), True))
+                except np.linalg.LinAlgError:
+                    self.factors.append((blk, False))
+            return
+        # JACOBI and the other diagonal fallbacks: 1 / clamp(diag(S), eps)
+        d = np.einsum("nii->ni", diag_blocks)
+        self.dinv = 1.0 / np.maximum(d, EPS64)
+
+    def apply(self, r: np.ndarray) -> np.ndarray:
+        if self.kind == "IDENTITY":
+            return r.copy()
+        if self.kind == "SCHUR_JACOBI":
+            z = np.empty_like(r)
+            for c, (f, chol) in enumerate(self.factors):
+                if chol:
+                    y = np.linalg.solve(f, r[c])
+                    z[c] = np.linalg.solve(f.T, y)
+                else:
+                    try:
+                        z[c] = np.linalg.solve(f, r[c])
+                    except np.linalg.LinAlgError:
+                        z[c] = np.linalg.lstsq(f, r[c], rcond=None)[0]
+            return z
+        return self.dinv * r
+
+
+def pcg(matvec, rhs: np.ndarray, prec: _Preconditioner, *, min_iterations=0, max_iterations=500,
+        tolerance=0.1, eps=EPS64):
+    """linear.py:1216-1256 (x0 = 0)."""
+    x = np.zeros_like(rhs)
+    r = rhs.copy()
+    z = prec.apply(r)
+    p = z.copy()
+    rz_old = float(np.sum(r * z))
+    rhs_norm = max(float(np.linalg.norm(rhs)), eps)
+    if min_iterations <= 0 and np.linalg.norm(r) <= tolerance * rhs_norm:
+        return x, 0, True
+    iterations = 0
+    success = False
+    for k in range(max_iterations):
+        Ap = matvec(p)
+        denom = float(np.sum(p * Ap))
+        if abs(denom) <= eps:
+            success = bool(np.linalg.norm(r) <= tolerance * rhs_norm)
+            break
+        alpha = rz_old / denom
+        x = x + alpha * p
+        r = r - alpha * Ap
+        iterations = k + 1
+        if iterations >= min_iterations and np.linalg.norm(r) <= tolerance * rhs_norm:
+            success = True
+            break
+        z = prec.apply(r)
+        rz_new = float(np.sum(r * z))
+        if abs(rz_old) <= eps:
+            break
+        beta = rz_new / rz_old
+        p = z + beta * p
+        rz_old = rz_new
+    return x, iterations, success
+
+
+def back_substitute(sys: SchurSystem, xb: np.ndarray) -> np.ndarray:
+    """xa = Haa^-1 ga - Haa^-1 Hab xb (linear.py:698 / :766)."""
+    both = (sys.pt >= 0) & (sys.cam >= 0)
+    t = _segment_sum(np.einsum("nij,nj->ni", sys.Fi[both], xb[sys.cam[both]]), sys.pt[both], sys.n_pt)
+    return sys.Winv_ga - np.einsum("nij,nj->ni", sys.Winv, t)
+
+
+def solve_step(prob, ev, radius, opts, *, explicit_limit=1800):
+    """Damping (solver.py:135-141) + the Schur linear solve for one LM iteration.
+
+    Returns (step_points [np_a,3], step_cams [nc_a,9], linear iterations)."""
+    pt = prob.pt_col[prob.point_index]
+    cam = prob.cam_col[prob.camera_index]
+    col_p = _segment_sum(np.sum(ev.Jp[pt >= 0] ** 2, axis=1), pt[pt >= 0], prob.active_pts.size)
+    col_c = _segment_sum(np.sum(ev.Jc[cam >= 0] ** 2, axis=1), cam[cam >= 0], prob.active_cams.size)
+    dp = jacobi_damping(col_p, radius, opts.min_lm_diagonal, opts.max_lm_diagonal, opts.jacobi_scaling)
+    dc = jacobi_damping(col_c, radius, opts.min_lm_diagonal, opts.max_lm_diagonal, opts.jacobi_scaling)
+    sys = build_schur(prob, ev, dp, dc)
+    if sys.n_cam == 0:
+        return sys.Winv_ga, np.zeros((0, 9)), 1
+    if opts.linear_solver_type in ("DENSE_SCHUR", "SPARSE_SCHUR"):
+        S = schur_dense(sys)
+        try:
+            xb = np.linalg.solve(S, sys.rhs.reshape(-1))
+        except np.linalg.LinAlgError:
+            xb = np.linalg.lstsq(S, sys.rhs.reshape(-1), rcond=None)[0]
+        xb = xb.reshape(-1, 9)
+        its = 1
+    else:
+        if 9 * sys.n_cam <= explicit_limit:
+            S = schur_dense(sys)
+            mv = lambda v: (S @ v.reshape(-1)).reshape(-1, 9)  # noqa: E731
+        else:
+            mv = lambda v: schur_matvec(sys, v)  # noqa: E731
+        prec = _Preconditioner(opts.preconditioner_type, schur_diag_blocks(sys))
+        xb, its, _ = pcg(mv, sys.rhs, prec, min_iterations=opts.min_linear_solver_iterations,
+                         max_iterations=opts.max_linear_solver_iterations, tolerance=opts.eta)
+    xa = back_substitute(sys, xb)
+    return xa, xb, its
+
+
+# --------------------------------------------------------------------------------------
+# LM driver (solver.py:35-357)
+# --------------------------------------------------------------------------------------
+@dataclass
+class OracleOptions:
+    linear_solver_type: str = "ITERATIVE_SCHUR"
+    preconditioner_type: str = "SCHUR_JACOBI"
+    max_num_iterations: int = 50
+    initial_trust_region_radius: float = 1e4
+    max_trust_region_radius: float = 1e16
+    min_trust_region_radius: float = 1e-32
+    min_relative_decrease: float = 1e-3
+    min_lm_diagonal: float = 1e-6
+    max_lm_diagonal: float = 1e32
+    max_num_consecutive_invalid_steps: int = 5
+    function_tolerance: float = 1e-6
+    gradient_tolerance: float = 1e-10
+    parameter_tolerance: float = 1e-8
+    min_linear_solver_iterations: int = 0
+    max_linear_solver_iterations: int = 500
+    eta: float = 0.1
+    jacobi_scaling: bool = True
+    use_nonmonotonic_steps: bool = False
+    max_consecutive_nonmonotonic_steps: int = 5
+
+
+@dataclass
+class OracleIteration:
+    iteration: int
+    cost: float
+    cost_change: float = 0.0
+    gradient_max_norm: float = 0.0
+    gradient_norm: float = 0.0
+    step_norm: float = 0.0
+    relative_decrease: float = 0.0
+    trust_region_radius: float = 0.0
+    linear_solver_iterations: int = 0
+    step_is_valid: bool = True
+    step_is_successful: bool = True
+
+
+@dataclass
+class OracleResult:
+    initial_cost: float
+    final_cost: float
+    termination: str
+    message: str
+    iterations: list = field(default_factory=list)
+    cameras: np.ndarray | None = None
+    points: np.ndarray | None = None
+    num_successful_steps: int = 0
+    num_unsuccessful_steps: int = 0
+
+
+class StepEvaluator:
+    """solver.py:823-861."""
+
+    def __init__(self, initial_cost, max_nonmono):
+        self.max_nonmono = max(0, int(max_nonmono))
+        self.minimum_cost = self.current_cost = self.reference_cost = self.candidate_cost = initial_cost
+        self.acc_ref = 0.0
+        self.acc_cand = 0.0
+        self.n_nonmono = 0
+
+    def step_quality(self, cost, model_change):
+        if model_change <= 0.0:
+            return float("-inf")
+        rel = (self.current_cost - cost) / model_change
+        hist = (self.reference_cost - cost) / (self.acc_ref + model_change)
+        return max(rel, hist)
+
+    def step_accepted(self, cost, model_change):
+        self.current_cost = cost
+        self.acc_cand += model_change
+        self.acc_ref += model_change
+        if self.current_cost < self.minimum_cost:
+            self.minimum_cost = self.current_cost
+            self.n_nonmono = 0
+            self.candidate_cost = self.current_cost
+            self.acc_cand = 0.0
+        else:
+            self.n_nonmono += 1
+            if self.current_cost > self.candidate_cost:
+                self.candidate_cost = self.current_cost
+                self.acc_cand = 0.0
+        if self.n_nonmono == self.max_nonmono:
+            self.reference_cost = self.candidate_cost
+            self.acc_ref = self.acc_cand
+
+
+def _gradient(prob, ev):
+    pt = prob.pt_col[prob.point_index]
+    cam = prob.cam_col[prob.camera_index]
+    gp = _segment_sum(np.einsum("nri,nr->ni", ev.Jp[pt >= 0], ev.r[pt >= 0]), pt[pt >= 0], prob.active_pts.size)
+    gc = _segment_sum(np.einsum("nri,nr->ni", ev.Jc[cam >= 0], ev.r[cam >= 0]), cam[cam >= 0], prob.active_cams.size)
+    return np.concatenate([gp.reshape(-1), gc.reshape(-1)])
+
+
+def solve(prob: OracleProblem, opts: OracleOptions | None = None) -> OracleResult:
+    """solver.py:35-357 for the LM strategy, no bounds, no inner iterations."""
+    opts = opts or OracleOptions()
+    cams = prob.cameras.copy()
+    pts = prob.points.copy()
+    radius = opts.initial_trust_region_radius
+    decrease_factor = 2.0
+    consecutive_invalid = 0
+    previous_cost = None
+    ev = evaluate(prob, cams, pts)
+    res = OracleResult(ev.cost, ev.cost, "FAILURE", "")
+    best_cost = ev.cost
+    best = (cams.copy(), pts.copy())
+    se = StepEvaluator(ev.cost, opts.max_consecutive_nonmonotonic_steps if opts.use_nonmonotonic_steps else 0)
+    if prob.active_pts.size + prob.active_cams.size == 0:
+        res.termination, res.message = "CONVERGENCE", "No active parameters."
+        res.cameras, res.points = cams, pts
+        return res
+    ncols = 3 * prob.active_pts.size + 9 * prob.active_cams.size
+    terminated = False
+    for iteration in range(opts.max_num_iterations + 1):
+        cost = ev.cost
+        g = _gradient(prob, ev)
+        gmax = float(np.max(np.abs(g))) if g.size else 0.0
+        it = OracleIteration(iteration, cost, gradient_max_norm=gmax, gradient_norm=float(np.linalg.norm(g)),
+                             trust_region_radius=radius)
+        if iteration == 0:
+            res.iterations.append(it)
+            if gmax <= opts.gradient_tolerance:
+                res.termination, res.message = "CONVERGENCE", "Gradient tolerance reached."
+                res.final_cost = cost
+                terminated = True
+                break
+            if opts.max_num_iterations == 0:
+                res.termination, res.message = "NO_CONVERGENCE", "Maximum iterations reached."
+                res.final_cost = cost
+                terminated = True
+                break
+            continue
+        if ncols == 0:
+            res.termination, res.message = "CONVERGENCE", "No active parameters."
+            terminated = True
+            break
+        xa, xb, its = solve_step(prob, ev, radius, opts)
+        step = np.concatenate([xa.reshape(-1), xb.reshape(-1)])
+        if not np.all(np.isfinite(step)):
+            consecutive_invalid += 1
+            radius = radius / decrease_factor
+            decrease_factor *= 2.0
+            it.step_is_valid = it.step_is_successful = False
+            it.linear_solver_iterations = its
+            it.trust_region_radius = radius
+            res.num_unsuccessful_steps += 1
+            if consecutive_invalid >= opts.max_num_consecutive_invalid_steps:
+                res.termination, res.message = "FAILURE", "Too many invalid trust-region steps."
+                terminated = True
+                break
+            res.iterations.append(it)
+            continue
+        new_cams = cams.copy()
+        new_pts = pts.copy()
+        new_pts[prob.active_pts] += xa
+        new_cams[prob.active_cams] += xb
+        cand = evaluate(prob, new_cams, new_pts, jacobians=False)
+        # model decrease: 0.5|r|^2 - 0.5|r + J step|^2 (solver.py:798-802)
+        pt = prob.pt_col[prob.point_index]
+        cam = prob.cam_col[prob.camera_index]
+        Jd = np.zeros_like(ev.r)
+        m = pt >= 0
+        Jd[m] += np.einsum("nij,nj->ni", ev.Jp[m], xa[pt[m]])
+        m = cam >= 0
+        Jd[m] += np.einsum("nij,nj->ni", ev.Jc[m], xb[cam[m]])
+        before = 0.5 * float(np.dot(ev.r.reshape(-1), ev.r.reshape(-1)))
+        after_r = (ev.r + Jd).reshape(-1)
+        model_decrease = max(before - 0.5 * float(np.dot(after_r, after_r)), 0.0)
+        step_is_valid = model_decrease > 0.0
+        rho = se.step_quality(cand.cost, model_decrease) if step_is_valid else 0.0
+        accepted = step_is_valid and rho > opts.min_relative_decrease
+        it.step_norm = float(np.linalg.norm(step))
+        it.cost_change = cost - cand.cost
+        it.relative_decrease = float(rho)
+        it.step_is_valid = step_is_valid
+        it.linear_solver_iterations = its
+        if accepted:
+            consecutive_invalid = 0
+            res.num_successful_steps += 1
+            se.step_accepted(cand.cost, model_decrease)
+            cams, pts = new_cams, new_pts
+            if cand.cost < best_cost:
+                best_cost = cand.cost
+                best = (cams.copy(), pts.copy())
+            res.final_cost = best_cost
+            denom = max(1.0 / 3.0, 1.0 - (2.0 * rho - 1.0) ** 3)
+            radius = min(opts.max_trust_region_radius, radius / denom)
+            decrease_factor = 2.0
+            it.trust_region_radius = radius
+            it.step_is_successful = True
+        else:
+            res.num_unsuccessful_steps += 1
+            radius = radius / decrease_factor
+            decrease_factor *= 2.0
+            it.trust_region_radius = radius
+            it.step_is_successful = False
+        res.iterations.append(it)
+        if accepted:
+            state_norm = math.sqrt(float(np.sum(cams * cams)) + float(np.sum(pts * pts)))
+            if it.step_norm <= opts.parameter_tolerance * (state_norm + opts.parameter_tolerance):
+                res.termination, res.message = "CONVERGENCE", "Parameter tolerance reached."
+                terminated = True
+                break
+            if previous_cost is not None and abs(previous_cost - cand.cost) <= opts.function_tolerance * max(previous_cost, 1.0):
+                res.termination, res.message = "CONVERGENCE", "Function tolerance reached."
+                terminated = True
+                break
+            previous_cost = cand.cost
+            ev = evaluate(prob, cams, pts)
+            g2 = _gradient(prob, ev)
+            if g2.size and float(np.max(np.abs(g2))) <= opts.gradient_tolerance:
+                res.termination, res.message = "CONVERGENCE", "Gradient tolerance reached."
+                res.final_cost = ev.cost
+                terminated = True
+                break
+        if radius <= opts.min_trust_region_radius:
+            res.termination, res.message = "CONVERGENCE", "Minimum trust-region radius reached."
+            terminated = True
+            break
+    if not terminated:
+        res.termination, res.message = "NO_CONVERGENCE", "Maximum iterations reached."
+    if res.termination == "FAILURE" and res.message == "":
+        res.message = "Solver failed."
+    # solver.py:661-676: restore the best state, final cost = best cost
+    res.cameras, res.points = best
+    res.final_cost = best_cost
+    return res
+
+
+def schur_visibility(prob: OracleProblem):
+    """solver.py:744-785: per active camera, the sorted tuple of active points it sees."""
+    sets = [set() for _ in range(prob.active_cams.size)]
+    pt = prob.pt_col[prob.point_index]
+    cam = prob.cam_col[prob.camera_index]
+    for p, c in zip(pt.tolist(), cam.tolist()):
+        if p >= 0 and c >= 0:
+            sets[c].add(p)
+    if not any(sets):
+        return None
+    return tuple(tuple(sorted(s)) for s in sets)
