@@ -1,0 +1,594 @@
+// Device helpers for the Schur bundle-adjustment kernels (sm_100a).
+//
+// Everything here is per-thread register math: the Snavely projection with
+// its analytic Jacobian, the robust losses and the Ceres corrector, small
+// symmetric inverses, and the warp/block reductions the kernels share.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda/atomic>
+#include <math.h>
+#include <stdint.h>
+
+#include "../../include/ceres_b200.h"
+
+namespace cb200 {
+
+constexpr double kEps64 = 2.220446049250313080847e-16;   // float64 machine epsilon
+constexpr double kTiny64 = 2.2250738585072013831e-308;   // smallest normal float64
+constexpr float kEps32 = 1.1920928955078125e-7f;          // float32 machine epsilon
+constexpr int kRec = 24;                                   // Jacobian scalars per slot
+
+template <typename T> struct Eps;
+template <> struct Eps<double> { static __device__ __forceinline__ double v() { return kEps64; } };
+template <> struct Eps<float> { static __device__ __forceinline__ double v() { return (double)kEps32; } };
+
+// ------------------------------------------------------------------------------------
+// Robust losses (ceres-torch losses.py:21-133): rho(s), rho'(s), rho''(s)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double softplus(double x) {
+  // torch.nn.functional.softplus with beta 1 and threshold 20
+  return x > 20.0 ? x : log1p(exp(x));
+}
+
+__device__ inline void loss_base(int kind, double a, double b, double s, double& r0, double& r1, double& r2) {
+  switch (kind) {
+    case CERES_B200_LOSS_HUBER: {
+      const double b2 = a * a;
+      if (s <= b2) { r0 = s; r1 = 1.0; r2 = 0.0; }
+      else {
+        const double sq = sqrt(fmax(s, kTiny64));
+        r0 = 2.0 * a * sq - b2;
+        r1 = a / sq;
+        r2 = -0.5 * a / (sq * s);
+      }
+      return;
+    }
+    case CERES_B200_LOSS_SOFTLONE: {
+      const double b2 = a * a;
+      const double z = 1.0 + s / b2;
+      const double sz = sqrt(z);
+      r0 = 2.0 * b2 * (sz - 1.0);
+      r1 = 1.0 / sz;
+      r2 = -0.5 / (b2 * z * sz);
+      return;
+    }
+    case CERES_B200_LOSS_CAUCHY: {
+      const double b2 = a * a;
+      const double z = 1.0 + s / b2;
+      r0 = b2 * log(z);
+      r1 = 1.0 / z;
+      r2 = -1.0 / (b2 * z * z);
+      return;
+    }
+    case CERES_B200_LOSS_ARCTAN: {
+      const double z = s / a;
+      const double den = 1.0 + z * z;
+      r0 = a * atan(z);
+      r1 = 1.0 / den;
+      r2 = -2.0 * z / (a * den * den);
+      return;
+    }
+    case CERES_B200_LOSS_TOLERANT: {
+      const double z = (s - a) / b;
+      const double c = b * softplus(-a / b);
+      r0 = b * softplus(z) - c;
+      r1 = 1.0 / (1.0 + exp(-z));
+      r2 = r1 * (1.0 - r1) / b;
+      return;
+    }
+    case CERES_B200_LOSS_TUKEY: {
+      const double a2 = a * a;
+      const double z = s / a2;
+      const double inner = 1.0 - z;
+      if (s <= a2) {
+        r0 = (a2 / 3.0) * (1.0 - inner * inner * inner);
+        r1 = inner * inner;
+        r2 = -2.0 * inner / a2;
+      } else {
+        r0 = a2 / 3.0; r1 = 0.0; r2 = 0.0;
+      }
+      return;
+    }
+    default:
+      r0 = s; r1 = 1.0; r2 = 0.0;
+      return;
+  }
+}
+
+struct LossSpec {
+  int kind; double a, b, scale;
+  int inner; double ia, ib, iscale;
+};
+
+__device__ __forceinline__ LossSpec loss_spec(const ceres_b200_ba_t& ba) {
+  return LossSpec{ba.loss_kind, ba.loss_a, ba.loss_b, ba.loss_scale,
+                  ba.inner_loss_kind, ba.inner_a, ba.inner_b, ba.inner_scale};
+}
+
+__device__ inline void loss_eval(const LossSpec& L, double s, double& r0, double& r1, double& r2) {
+  if (L.inner >= 0) {  // ComposedLoss(outer, inner): losses.py:125-133
+    double g0, g1, g2, f0, f1, f2;
+    loss_base(L.inner, L.ia, L.ib, s, g0, g1, g2);
+    g0 *= L.iscale; g1 *= L.iscale; g2 *= L.iscale;
+    loss_base(L.kind, L.a, L.b, g0, f0, f1, f2);
+    r0 = f0; r1 = f1 * g1; r2 = f2 * g1 * g1 + f1 * g2;
+  } else {
+    loss_base(L.kind, L.a, L.b, s, r0, r1, r2);
+  }
+  r0 *= L.scale; r1 *= L.scale; r2 *= L.scale;  // ScaledLoss: losses.py:113-122
+}
+
+// ------------------------------------------------------------------------------------
+// Snavely reprojection with its analytic Jacobian
+// ------------------------------------------------------------------------------------
+// Residual r = f d (xp, yp) - obs with p = R(aa) X + t, xp = -p0/p2, yp = -p1/p2,
+// d = 1 + r2 (k1 + k2 r2) (examples/simple_bundle_adjuster.py:73-79). The rotation
+// goes through the unit quaternion of rotation.py:104-110 (small-angle branch
+// k = 0.5 - theta^2/48 when theta <= eps), normalised (rotation.py:68-69), and
+// applied as X + w uv + u x uv with uv = 2 u x X (rotation.py:211-214). The
+// derivative follows the same chain, including the normalisation, so it equals
+// what autograd produces on the reference (costs.py:31-44), up to rounding.
+struct Proj {
+  double r[2];
+  double jc[2][9];
+  double jp[2][3];
+};
+
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+template <bool kJac>
+__device__ __forceinline__ void snavely(const double* __restrict__ cam, const double X[3], double ox, double oy,
+                                        Proj& o) {
+  const double aa[3] = {cam[0], cam[1], cam[2]};
+  const double th2 = aa[0] * aa[0] + aa[1] * aa[1] + aa[2] * aa[2];
+  const double theta = sqrt(th2);
+  const double half = theta * 0.5;
+  const bool small = theta <= kEps64;
+  double sh, ch;
+  sincos(half, &sh, &ch);
+  const double safe_theta = small ? 1.0 : theta;
+  const double k = small ? 0.5 - theta * theta / 48.0 : sh / safe_theta;
+  double q[4] = {ch, k * aa[0], k * aa[1], k * aa[2]};
+  double qn2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+  double n = sqrt(qn2);
+  const bool clamped = n < kTiny64;
+  if (clamped) n = kTiny64;
+  const double w = q[0] / n;
+  const double u[3] = {q[1] / n, q[2] / n, q[3] / n};
+  double c1[3];
+  cross3(u, X, c1);
+  const double uv[3] = {c1[0] * 2.0, c1[1] * 2.0, c1[2] * 2.0};
+  double c2[3];
+  cross3(u, uv, c2);
+  double p[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) p[i] = (X[i] + w * uv[i] + c2[i]) + cam[3 + i];
+  const double xp = -p[0] / p[2];
+  const double yp = -p[1] / p[2];
+  const double r2 = xp * xp + yp * yp;
+  const double k1 = cam[7], k2 = cam[8], f = cam[6];
+  const double dist = 1.0 + r2 * (k1 + k2 * r2);
+  const double fd = f * dist;
+  o.r[0] = fd * xp - ox;
+  o.r[1] = fd * yp - oy;
+  if (!kJac) return;
+
+  // d q_raw / d aa  (4 x 3)
+  double dth[3];
+  if (theta > 0.0) {
+    dth[0] = aa[0] / theta; dth[1] = aa[1] / theta; dth[2] = aa[2] / theta;
+  } else {
+    dth[0] = dth[1] = dth[2] = 0.0;  // torch.linalg.norm's subgradient at 0
+  }
+  const double dk_dth = small ? -(2.0 * theta) / 48.0 : (ch * 0.5 * theta - sh) / (theta * theta);
+  double dq[4][3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    dq[0][j] = -sh * 0.5 * dth[j];
+    const double dkj = dk_dth * dth[j];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) dq[1 + i][j] = (i == j ? k : 0.0) + aa[i] * dkj;
+  }
+  // normalisation: dqn = (dq - qn (qn . dq)) / n
+  double dqn[4][3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    if (clamped) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dqn[i][j] = dq[i][j] / n;
+    } else {
+      const double qn_dot = (w * dq[0][j] + u[0] * dq[1][j] + u[1] * dq[2][j] + u[2] * dq[3][j]);
+      dqn[0][j] = (dq[0][j] - w * qn_dot) / n;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) dqn[1 + i][j] = (dq[1 + i][j] - u[i] * qn_dot) / n;
+    }
+  }
+  // dp/daa: d(X + w uv + u x uv) = dw uv + w duv + du x uv + u x duv, duv = 2 du x X
+  double dpa[3][3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double du[3] = {dqn[1][j], dqn[2][j], dqn[3][j]};
+    double t1[3];
+    cross3(du, X, t1);
+    const double duv[3] = {2.0 * t1[0], 2.0 * t1[1], 2.0 * t1[2]};
+    double t2[3], t3[3];
+    cross3(du, uv, t2);
+    cross3(u, duv, t3);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) dpa[i][j] = dqn[0][j] * uv[i] + w * duv[i] + t2[i] + t3[i];
+  }
+  // dp/dX = I + 2 w [u]x + 2 [u]x^2, [u]x^2 = u u^T - (u.u) I
+  const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  double M[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) M[i][j] = 2.0 * u[i] * u[j] + (i == j ? 1.0 - 2.0 * uu : 0.0);
+  M[0][1] -= 2.0 * w * u[2]; M[0][2] += 2.0 * w * u[1];
+  M[1][0] += 2.0 * w * u[2]; M[1][2] -= 2.0 * w * u[0];
+  M[2][0] -= 2.0 * w * u[1]; M[2][1] += 2.0 * w * u[0];
+
+  // projection
+  const double inv_p2 = 1.0 / p[2];
+  const double dxp[3] = {-inv_p2, 0.0, -xp * inv_p2};
+  const double dyp[3] = {0.0, -inv_p2, -yp * inv_p2};
+  const double g = k1 + 2.0 * k2 * r2;
+  const double dd_dx = 2.0 * xp * g, dd_dy = 2.0 * yp * g;
+  const double A00 = f * (dist + xp * dd_dx), A01 = f * xp * dd_dy;
+  const double A10 = f * yp * dd_dx, A11 = f * (dist + yp * dd_dy);
+  double Dp[2][3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    Dp[0][m] = A00 * dxp[m] + A01 * dyp[m];
+    Dp[1][m] = A10 * dxp[m] + A11 * dyp[m];
+  }
+#pragma unroll
+  for (int rrow = 0; rrow < 2; ++rrow) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      o.jc[rrow][j] = Dp[rrow][0] * dpa[0][j] + Dp[rrow][1] * dpa[1][j] + Dp[rrow][2] * dpa[2][j];
+      o.jc[rrow][3 + j] = Dp[rrow][j];
+      o.jp[rrow][j] = Dp[rrow][0] * M[0][j] + Dp[rrow][1] * M[1][j] + Dp[rrow][2] * M[2][j];
+    }
+  }
+  o.jc[0][6] = dist * xp; o.jc[1][6] = dist * yp;
+  o.jc[0][7] = f * r2 * xp; o.jc[1][7] = f * r2 * yp;
+  o.jc[0][8] = f * r2 * r2 * xp; o.jc[1][8] = f * r2 * r2 * yp;
+}
+
+// Ceres corrector (losses.py:158-193) applied in place. Returns 0.5 rho0.
+template <bool kJac>
+__device__ __forceinline__ double robustify(const LossSpec& L, Proj& o, unsigned& err) {
+  const double s = o.r[0] * o.r[0] + o.r[1] * o.r[1];
+  double r0, r1, r2;
+  loss_eval(L, s, r0, r1, r2);
+  const double sqrt_rho1 = sqrt(fmax(r1, 0.0));
+  double rscale = sqrt_rho1, alpha_s = 0.0;
+  if (s > 0.0 && r2 > 0.0) {
+    if (r1 <= 0.0) err |= CERES_B200_DEVERR_LOSS;
+    const double alpha = 1.0 - sqrt(1.0 + 2.0 * s * r2 / r1);
+    rscale = sqrt_rho1 / (1.0 - alpha);
+    alpha_s = alpha / s;
+  }
+  if (kJac) {
+    if (alpha_s == 0.0) {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+#pragma unroll
+        for (int j = 0; j < 9; ++j) o.jc[i][j] *= sqrt_rho1;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o.jp[i][j] *= sqrt_rho1;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        const double rTj = o.r[0] * o.jc[0][j] + o.r[1] * o.jc[1][j];
+        o.jc[0][j] = sqrt_rho1 * (o.jc[0][j] - alpha_s * o.r[0] * rTj);
+        o.jc[1][j] = sqrt_rho1 * (o.jc[1][j] - alpha_s * o.r[1] * rTj);
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double rTj = o.r[0] * o.jp[0][j] + o.r[1] * o.jp[1][j];
+        o.jp[0][j] = sqrt_rho1 * (o.jp[0][j] - alpha_s * o.r[0] * rTj);
+        o.jp[1][j] = sqrt_rho1 * (o.jp[1][j] - alpha_s * o.r[1] * rTj);
+      }
+    }
+  }
+  o.r[0] *= rscale;
+  o.r[1] *= rscale;
+  return 0.5 * r0;
+}
+
+// ------------------------------------------------------------------------------------
+// Jacobian record I/O (24 scalars per slot)
+// ------------------------------------------------------------------------------------
+template <typename T> struct Rec { T v[kRec]; };
+
+__device__ __forceinline__ void load_rec(const float* __restrict__ base, size_t slot, float v[kRec]) {
+  const float4* p = reinterpret_cast<const float4*>(base + slot * kRec);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const float4 t = __ldg(p + i);
+    v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
+  }
+}
+__device__ __forceinline__ void load_rec(const double* __restrict__ base, size_t slot, double v[kRec]) {
+  const double2* p = reinterpret_cast<const double2*>(base + slot * kRec);
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const double2 t = __ldg(p + i);
+    v[2 * i] = t.x; v[2 * i + 1] = t.y;
+  }
+}
+// point rows only (the last 6 scalars)
+__device__ __forceinline__ void load_rec_jp(const float* __restrict__ base, size_t slot, float v[6]) {
+  const float2* p = reinterpret_cast<const float2*>(base + slot * kRec + 18);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { const float2 t = __ldg(p + i); v[2 * i] = t.x; v[2 * i + 1] = t.y; }
+}
+__device__ __forceinline__ void load_rec_jp(const double* __restrict__ base, size_t slot, double v[6]) {
+  const double2* p = reinterpret_cast<const double2*>(base + slot * kRec + 18);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { const double2 t = __ldg(p + i); v[2 * i] = t.x; v[2 * i + 1] = t.y; }
+}
+__device__ __forceinline__ void store_rec(float* __restrict__ base, size_t slot, const Proj& o) {
+  float4* p = reinterpret_cast<float4*>(base + slot * kRec);
+  float v[kRec];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) { v[j] = (float)o.jc[0][j]; v[9 + j] = (float)o.jc[1][j]; }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) { v[18 + j] = (float)o.jp[0][j]; v[21 + j] = (float)o.jp[1][j]; }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) p[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+}
+__device__ __forceinline__ void store_rec(double* __restrict__ base, size_t slot, const Proj& o) {
+  double2* p = reinterpret_cast<double2*>(base + slot * kRec);
+  double v[kRec];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) { v[j] = o.jc[0][j]; v[9 + j] = o.jc[1][j]; }
+#pragma unroll
+  for (int j = 0; j < 3; ++j) { v[18 + j] = o.jp[0][j]; v[21 + j] = o.jp[1][j]; }
+#pragma unroll
+  for (int i = 0; i < 12; ++i) p[i] = make_double2(v[2 * i], v[2 * i + 1]);
+}
+
+// symmetric 3x3 stored as (00, 01, 02, 11, 12, 22)
+template <typename T>
+__device__ __forceinline__ void sym3_mul(const T m[6], const double x[3], double y[3]) {
+  y[0] = (double)m[0] * x[0] + (double)m[1] * x[1] + (double)m[2] * x[2];
+  y[1] = (double)m[1] * x[0] + (double)m[3] * x[1] + (double)m[4] * x[2];
+  y[2] = (double)m[2] * x[0] + (double)m[4] * x[1] + (double)m[5] * x[2];
+}
+
+// Inverse of a symmetric 3x3 (float64). Cholesky when positive definite;
+// otherwise the adjugate formula (an LU-equivalent solve for a nonsingular
+// block, as torch.linalg.solve would give).
+__device__ inline void sym3_inverse(const double a[6], double inv[6]) {
+  const double l00sq = a[0];
+  bool pd = l00sq > 0.0;
+  if (pd) {
+    const double l00 = sqrt(l00sq);
+    const double l10 = a[1] / l00, l20 = a[2] / l00;
+    const double l11sq = a[3] - l10 * l10;
+    pd = l11sq > 0.0;
+    if (pd) {
+      const double l11 = sqrt(l11sq);
+      const double l21 = (a[4] - l20 * l10) / l11;
+      const double l22sq = a[5] - l20 * l20 - l21 * l21;
+      pd = l22sq > 0.0;
+      if (pd) {
+        const double l22 = sqrt(l22sq);
+        // L^-1 (lower)
+        const double i00 = 1.0 / l00, i11 = 1.0 / l11, i22 = 1.0 / l22;
+        const double i10 = -l10 * i00 * i11;
+        const double i21 = -l21 * i11 * i22;
+        const double i20 = -(l20 * i00 + l21 * i10) * i22;
+        // A^-1 = L^-T L^-1
+        inv[0] = i00 * i00 + i10 * i10 + i20 * i20;
+        inv[1] = i10 * i11 + i20 * i21;
+        inv[2] = i20 * i22;
+        inv[3] = i11 * i11 + i21 * i21;
+        inv[4] = i21 * i22;
+        inv[5] = i22 * i22;
+        return;
+      }
+    }
+  }
+  const double c00 = a[3] * a[5] - a[4] * a[4];
+  const double c01 = a[2] * a[4] - a[1] * a[5];
+  const double c02 = a[1] * a[4] - a[2] * a[3];
+  const double c11 = a[0] * a[5] - a[2] * a[2];
+  const double c12 = a[1] * a[2] - a[0] * a[4];
+  const double c22 = a[0] * a[3] - a[1] * a[1];
+  const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+  const double id = 1.0 / det;
+  inv[0] = c00 * id; inv[1] = c01 * id; inv[2] = c02 * id;
+  inv[3] = c11 * id; inv[4] = c12 * id; inv[5] = c22 * id;
+}
+
+// Inverse of a 9x9 block (float64, row-major, full storage). Cholesky when
+// positive definite, Gauss-Jordan with partial pivoting otherwise
+// (linear.py:1169-1174: cholesky, else a plain solve of the block).
+__device__ inline void block9_inverse(double A[81], double inv[81]) {
+  double L[81];
+  bool pd = true;
+#pragma unroll 1
+  for (int j = 0; j < 9 && pd; ++j) {
+    double d = A[j * 9 + j];
+    for (int k = 0; k < j; ++k) d -= L[j * 9 + k] * L[j * 9 + k];
+    if (!(d > 0.0)) { pd = false; break; }
+    const double ljj = sqrt(d);
+    L[j * 9 + j] = ljj;
+    for (int i = j + 1; i < 9; ++i) {
+      double s = A[i * 9 + j];
+      for (int k = 0; k < j; ++k) s -= L[i * 9 + k] * L[j * 9 + k];
+      L[i * 9 + j] = s / ljj;
+    }
+  }
+  if (pd) {
+    // solve L L^T X = I column by column
+#pragma unroll 1
+    for (int c = 0; c < 9; ++c) {
+      double y[9];
+      for (int i = 0; i < 9; ++i) {
+        double s = (i == c) ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) s -= L[i * 9 + k] * y[k];
+        y[i] = s / L[i * 9 + i];
+      }
+      for (int i = 8; i >= 0; --i) {
+        double s = y[i];
+        for (int k = i + 1; k < 9; ++k) s -= L[k * 9 + i] * inv[k * 9 + c];
+        inv[i * 9 + c] = s / L[i * 9 + i];
+      }
+    }
+    return;
+  }
+  // Gauss-Jordan with partial pivoting on [A | I]
+  for (int i = 0; i < 81; ++i) inv[i] = (i % 10 == 0) ? 1.0 : 0.0;
+#pragma unroll 1
+  for (int c = 0; c < 9; ++c) {
+    int piv = c;
+    double best = fabs(A[c * 9 + c]);
+    for (int r = c + 1; r < 9; ++r) {
+      const double v = fabs(A[r * 9 + c]);
+      if (v > best) { best = v; piv = r; }
+    }
+    if (piv != c) {
+      for (int k = 0; k < 9; ++k) {
+        double t = A[c * 9 + k]; A[c * 9 + k] = A[piv * 9 + k]; A[piv * 9 + k] = t;
+        t = inv[c * 9 + k]; inv[c * 9 + k] = inv[piv * 9 + k]; inv[piv * 9 + k] = t;
+      }
+    }
+    const double d = 1.0 / A[c * 9 + c];
+    for (int k = 0; k < 9; ++k) { A[c * 9 + k] *= d; inv[c * 9 + k] *= d; }
+    for (int r = 0; r < 9; ++r) {
+      if (r == c) continue;
+      const double fct = A[r * 9 + c];
+      if (fct == 0.0) continue;
+      for (int k = 0; k < 9; ++k) { A[r * 9 + k] -= fct * A[c * 9 + k]; inv[r * 9 + k] -= fct * inv[c * 9 + k]; }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Reductions
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide reduction of NV values (sum, or max where is_max bit set). Result
+// valid in thread 0. smem must hold NV * (blockDim.x / 32) doubles.
+template <int NV>
+__device__ __forceinline__ void block_reduce(double v[NV], unsigned is_max_mask, double* smem) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = ((is_max_mask >> i) & 1u) ? warp_max(v[i]) : warp_sum(v[i]);
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) smem[i * nw + wid] = v[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double acc = smem[i * nw];
+      for (int w = 1; w < nw; ++w) acc = ((is_max_mask >> i) & 1u) ? fmax(acc, smem[i * nw + w]) : acc + smem[i * nw + w];
+      v[i] = acc;
+    }
+  }
+  __syncthreads();
+}
+
+// Deterministic grid reduction: each CTA's thread 0 posts NV partials; the last
+// CTA to arrive folds them in CTA order and writes stats[out_idx[i]] (or ORs/adds
+// into it when accumulate). counter returns to zero afterwards.
+template <int NV>
+__device__ __forceinline__ void grid_finish(const double v[NV], unsigned is_max_mask, double* partials,
+                                            unsigned* counter, double* stats, const int out_idx[NV]) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) partials[(size_t)blockIdx.x * NV + i] = v[i];
+    __threadfence();
+    const unsigned ticket = atomicAdd(counter, 1u);
+    last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double acc = ((is_max_mask >> i) & 1u) ? 0.0 : 0.0;
+      for (unsigned b = 0; b < gridDim.x; ++b) {
+        const double x = *((volatile double*)&partials[(size_t)b * NV + i]);
+        acc = ((is_max_mask >> i) & 1u) ? fmax(acc, x) : acc + x;
+      }
+      stats[out_idx[i]] = acc;
+    }
+    *counter = 0u;
+    __threadfence();
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Grid barrier for the cooperative persistent PCG. Every wait is bounded: after
+// kSpinLimit polls the CTA records CERES_B200_DEVERR_BARRIER in *flag and the
+// barrier reports failure so that all CTAs leave the kernel.
+// ------------------------------------------------------------------------------------
+constexpr unsigned kSpinLimit = 1u << 24;
+
+struct GridBarrier {
+  unsigned* count;
+  unsigned* generation;
+  unsigned* flag;
+};
+
+__device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(*gb.generation);
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(*gb.count);
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> flg(*gb.flag);
+    const unsigned my_gen = gen.load(cuda::memory_order_acquire);
+    int good = 1;
+    if (flg.load(cuda::memory_order_relaxed) != 0u) {
+      good = 0;
+    } else {
+      const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+      if (arrived == gridDim.x - 1) {
+        cnt.store(0u, cuda::memory_order_relaxed);
+        gen.fetch_add(1u, cuda::memory_order_release);
+      } else {
+        unsigned spins = 0;
+        while (gen.load(cuda::memory_order_acquire) == my_gen) {
+          if (flg.load(cuda::memory_order_relaxed) != 0u) { good = 0; break; }
+          if (++spins > kSpinLimit) {
+            flg.fetch_or(CERES_B200_DEVERR_BARRIER, cuda::memory_order_relaxed);
+            good = 0;
+            break;
+          }
+          if (spins > 64) __nanosleep(64);
+        }
+      }
+    }
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+}  // namespace cb200

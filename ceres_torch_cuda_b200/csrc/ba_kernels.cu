@@ -1,0 +1,1243 @@
+// Schur-complement bundle-adjustment kernels for B200 (sm_100a) and their C ABI.
+//
+// Data layout (see include/ceres_b200.h): observations in a sliced-ELL store
+// where warp w owns slices of 32 points (lane = point, sorted by track length)
+// and walks their observations slot by slot; Jacobians are 24-scalar records
+// (96 B in FP32, 192 B in FP64) read with 128-bit loads. Every kernel is
+// bandwidth-bound; all reductions are deterministic (fixed CTA count, fixed
+// fold order) so a solve is bit-reproducible on one device.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "ba_device.cuh"
+
+using namespace cb200;
+
+namespace {
+
+// counters[] slots
+constexpr int kCtrEval = 0, kCtrPoint = 1, kCtrCamera = 2, kCtrStep = 3, kCtrCamStep = 4;
+constexpr int kCtrBarCount = 8, kCtrBarGen = 9, kCtrBarFlag = 10, kCtrError = 12;
+
+constexpr int kWarpBlock = 256;  // threads per CTA of the slice-walking kernels
+
+struct DevInfo {
+  int sms = 0;
+  int max_smem_optin = 0;
+};
+
+DevInfo device_info() {
+  static DevInfo cache[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && cache[dev].sms > 0) return cache[dev];
+  DevInfo d;
+  cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&d.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (dev >= 0 && dev < 64) cache[dev] = d;
+  return d;
+}
+
+inline int slice_grid(const ceres_b200_ba_t& ba, const DevInfo& d) {
+  const int warps = kWarpBlock / 32;
+  int g = (ba.num_slices + warps - 1) / warps;
+  const int cap = d.sms * 8;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return g;
+}
+
+// scratch layout: per-CTA reduction partials of the slice and camera kernels,
+// one auxiliary stats row, then the PCG area.
+constexpr size_t kRedSlots = 8;  // doubles per CTA
+
+inline size_t red_area_bytes(const ceres_b200_ba_t& ba, const DevInfo& d) {
+  int g = slice_grid(ba, d);
+  if (ba.num_cameras > g) g = ba.num_cameras;
+  if (g < 64) g = 64;
+  return ((size_t)g * kRedSlots * sizeof(double) + 255) & ~(size_t)255;
+}
+
+}  // namespace
+
+// ======================================================================================
+// Evaluation: residual, Jacobian, corrector
+// ======================================================================================
+template <typename T, bool kJac>
+__global__ void __launch_bounds__(kWarpBlock) k_evaluate(ceres_b200_ba_t ba, double* partials) {
+  __shared__ double red[kWarpBlock / 32];
+  const LossSpec L = loss_spec(ba);
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  double cost = 0.0;
+  unsigned err = 0;
+  T* __restrict__ jac = reinterpret_cast<T*>(ba.jac);
+  for (int s = gw; s < ba.num_slices; s += nw) {
+    const int q = s * 32 + lane;
+    const int len = ba.slice_len[s];
+    const size_t base = (size_t)ba.slice_base[s];
+    const double X[3] = {ba.points[3 * (size_t)q], ba.points[3 * (size_t)q + 1], ba.points[3 * (size_t)q + 2]};
+    const bool pconst = ba.pt_const[q] != 0;
+    for (int k = 0; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k + lane;
+      const int c = ba.slot_cam[slot];
+      if (c < 0) continue;
+      const double2 ob = reinterpret_cast<const double2*>(ba.slot_obs)[slot];
+      Proj o;
+      snavely<kJac>(ba.cameras + 9 * (size_t)c, X, ob.x, ob.y, o);
+      cost += robustify<kJac>(L, o, err);
+      reinterpret_cast<double2*>(ba.res)[slot] = make_double2(o.r[0], o.r[1]);
+      if (kJac) {
+        if (ba.cam_const[c]) {
+#pragma unroll
+          for (int j = 0; j < 9; ++j) o.jc[0][j] = o.jc[1][j] = 0.0;
+        }
+        if (pconst) {
+#pragma unroll
+          for (int j = 0; j < 3; ++j) o.jp[0][j] = o.jp[1][j] = 0.0;
+        }
+        store_rec(jac, slot, o);
+      }
+    }
+  }
+  if (err) atomicOr(&ba.counters[kCtrError], err);
+  double v[1] = {cost};
+  block_reduce<1>(v, 0u, red);
+  const int out[1] = {CERES_B200_STAT_COST};
+  grid_finish<1>(v, 0u, partials, &ba.counters[kCtrEval], ba.stats, out);
+}
+
+// ======================================================================================
+// Point side: W_p = J_p^T J_p + D_p, its inverse, W^-1 g_a, point gradient
+// ======================================================================================
+template <typename T>
+__global__ void __launch_bounds__(kWarpBlock) k_point_assemble(ceres_b200_ba_t ba, double inv_radius, double mn,
+                                                               double mx, int jacobi_scaling, double* partials) {
+  __shared__ double red[2 * (kWarpBlock / 32)];
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  T* __restrict__ winv = reinterpret_cast<T*>(ba.winv);
+  double gmax = 0.0, gsq = 0.0;
+  for (int s = gw; s < ba.num_slices; s += nw) {
+    const int q = s * 32 + lane;
+    const int len = ba.slice_len[s];
+    const size_t base = (size_t)ba.slice_base[s];
+    double W[6] = {0, 0, 0, 0, 0, 0};
+    double g[3] = {0, 0, 0};
+    for (int k = 0; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k + lane;
+      if (ba.slot_cam[slot] < 0) continue;
+      T jp[6];
+      load_rec_jp(jac, slot, jp);
+      const double2 r = reinterpret_cast<const double2*>(ba.res)[slot];
+      const double a0 = jp[0], a1 = jp[1], a2 = jp[2], b0 = jp[3], b1 = jp[4], b2 = jp[5];
+      W[0] += a0 * a0 + b0 * b0;
+      W[1] += a0 * a1 + b0 * b1;
+      W[2] += a0 * a2 + b0 * b2;
+      W[3] += a1 * a1 + b1 * b1;
+      W[4] += a1 * a2 + b1 * b2;
+      W[5] += a2 * a2 + b2 * b2;
+      g[0] += a0 * r.x + b0 * r.y;
+      g[1] += a1 * r.x + b1 * r.y;
+      g[2] += a2 * r.x + b2 * r.y;
+    }
+    double inv[6] = {0, 0, 0, 0, 0, 0};
+    double wga[3] = {0, 0, 0};
+    if (!ba.pt_const[q]) {
+      const int dg[3] = {0, 3, 5};
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double col = jacobi_scaling ? W[dg[i]] : 1.0;
+        W[dg[i]] += fmin(fmax(col, mn), mx) * inv_radius;
+        gmax = fmax(gmax, fabs(g[i]));
+        gsq += g[i] * g[i];
+      }
+      sym3_inverse(W, inv);
+      const double ga[3] = {-g[0], -g[1], -g[2]};
+      sym3_mul(inv, ga, wga);
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) winv[6 * (size_t)q + i] = (T)inv[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ba.winv_ga[3 * (size_t)q + i] = wga[i];
+  }
+  double v[2] = {gmax, gsq};
+  block_reduce<2>(v, 1u, red);
+  const int out[2] = {CERES_B200_STAT_GMAX_P, CERES_B200_STAT_GSQ_P};
+  grid_finish<2>(v, 1u, partials, &ba.counters[kCtrPoint], ba.stats, out);
+}
+
+// ======================================================================================
+// Camera side: one CTA per camera. Reduces J_c^T (I - J_p W^-1 J_p^T) J_c (the
+// Schur diagonal block before damping), the camera column sums, the gradient and
+// the reduced rhs over the camera's observations, then forms the preconditioner.
+// ======================================================================================
+constexpr int kCamBlock = 128;
+constexpr int kCamAcc = 45 + 9 + 9 + 9;  // V (upper), colsum, g, h
+
+__device__ __forceinline__ int tri9(int j, int l) {  // upper-triangle index, j <= l
+  return j * 9 - (j * (j - 1)) / 2 + (l - j);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t ba, double inv_radius, double mn,
+                                                               double mx, int jacobi_scaling, int precond,
+                                                               double* partials) {
+  __shared__ double sred[kCamAcc * (kCamBlock / 32)];
+  __shared__ double sacc[kCamAcc];
+  __shared__ double sred2[2 * (kCamBlock / 32)];
+  const int c = blockIdx.x;
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
+  double acc[kCamAcc];
+#pragma unroll
+  for (int i = 0; i < kCamAcc; ++i) acc[i] = 0.0;
+  const bool cconst = ba.cam_const[c] != 0;
+  const int e0 = ba.cam_offsets[c], e1 = ba.cam_offsets[c + 1];
+  if (!cconst) {
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+      const int2 ent = reinterpret_cast<const int2*>(ba.cam_entries)[e];
+      const size_t slot = (size_t)ent.x;
+      const int q = ent.y;
+      T rv[kRec];
+      load_rec(jac, slot, rv);
+      const double2 r = reinterpret_cast<const double2*>(ba.res)[slot];
+      double wi[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) wi[i] = (double)winv[6 * (size_t)q + i];
+      const double wg[3] = {ba.winv_ga[3 * (size_t)q], ba.winv_ga[3 * (size_t)q + 1], ba.winv_ga[3 * (size_t)q + 2]};
+      double jp0[3], jp1[3];
+#pragma unroll
+      for (int m = 0; m < 3; ++m) { jp0[m] = rv[18 + m]; jp1[m] = rv[21 + m]; }
+      // P = Jp W^-1 (2x3); B = P Jp^T (2x2); a = Jp W^-1 g_a
+      double P0[3], P1[3];
+      sym3_mul(wi, jp0, P0);
+      sym3_mul(wi, jp1, P1);
+      const double B00 = P0[0] * jp0[0] + P0[1] * jp0[1] + P0[2] * jp0[2];
+      const double B01 = P0[0] * jp1[0] + P0[1] * jp1[1] + P0[2] * jp1[2];
+      const double B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
+      const double a0 = jp0[0] * wg[0] + jp0[1] * wg[1] + jp0[2] * wg[2];
+      const double a1 = jp1[0] * wg[0] + jp1[1] * wg[1] + jp1[2] * wg[2];
+      const double M00 = 1.0 - B00, M01 = -B01, M11 = 1.0 - B11;
+      double K0[9], K1[9];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        const double c0 = rv[j], c1 = rv[9 + j];
+        K0[j] = M00 * c0 + M01 * c1;
+        K1[j] = M01 * c0 + M11 * c1;
+        acc[45 + j] += c0 * c0 + c1 * c1;
+        acc[54 + j] += c0 * r.x + c1 * r.y;
+        acc[63 + j] += c0 * (r.x + a0) + c1 * (r.y + a1);
+      }
+#pragma unroll
+      for (int j = 0; j < 9; ++j)
+#pragma unroll
+        for (int l = j; l < 9; ++l) acc[tri9(j, l)] += (double)rv[j] * K0[l] + (double)rv[9 + j] * K1[l];
+
+      if (ba.has_duplicate_cameras) {
+        // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
+        const int sidx = q >> 5, ln = q & 31;
+        const int len = ba.slice_len[sidx];
+        const size_t sb = (size_t)ba.slice_base[sidx];
+        for (int k = 0; k < len; ++k) {
+          const size_t slot2 = sb + 32 * (size_t)k + ln;
+          if (slot2 == slot || ba.slot_cam[slot2] != c) continue;
+          T rk[kRec];
+          load_rec(jac, slot2, rk);
+          const double C00 = P0[0] * rk[18] + P0[1] * rk[19] + P0[2] * rk[20];
+          const double C01 = P0[0] * rk[21] + P0[1] * rk[22] + P0[2] * rk[23];
+          const double C10 = P1[0] * rk[18] + P1[1] * rk[19] + P1[2] * rk[20];
+          const double C11 = P1[0] * rk[21] + P1[1] * rk[22] + P1[2] * rk[23];
+          for (int j = 0; j < 9; ++j) {
+            const double t0 = (double)rv[j] * C00 + (double)rv[9 + j] * C10;
+            const double t1 = (double)rv[j] * C01 + (double)rv[9 + j] * C11;
+            for (int l = j; l < 9; ++l) acc[tri9(j, l)] -= t0 * (double)rk[l] + t1 * (double)rk[9 + l];
+          }
+        }
+      }
+    }
+  }
+  // block reduction of kCamAcc values
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int i = 0; i < kCamAcc; ++i) {
+    const double v = warp_sum(acc[i]);
+    if (lane == 0) sred[i * nw + wid] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += sred[i * nw + w];
+    sacc[i] = s;
+  }
+  __syncthreads();
+  double gmax = 0.0, gsq = 0.0;
+  if (threadIdx.x == 0) {
+    T* __restrict__ pre = reinterpret_cast<T*>(ba.precond);
+    double* dc = ba.cam_diag + 9 * (size_t)c;
+    double* rh = ba.rhs + 9 * (size_t)c;
+    if (cconst) {
+      for (int j = 0; j < 9; ++j) { dc[j] = 0.0; rh[j] = 0.0; }
+      for (int i = 0; i < 81; ++i) pre[81 * (size_t)c + i] = (T)((i % 10 == 0) ? 1.0 : 0.0);
+    } else {
+      double S[81], inv[81];
+      for (int j = 0; j < 9; ++j) {
+        const double col = jacobi_scaling ? sacc[45 + j] : 1.0;
+        dc[j] = fmin(fmax(col, mn), mx) * inv_radius;
+        rh[j] = -sacc[63 + j];
+        const double gj = sacc[54 + j];
+        gmax = fmax(gmax, fabs(gj));
+        gsq += gj * gj;
+      }
+      for (int j = 0; j < 9; ++j)
+        for (int l = j; l < 9; ++l) {
+          const double v = sacc[tri9(j, l)] + (j == l ? dc[j] : 0.0);
+          S[j * 9 + l] = v;
+          S[l * 9 + j] = v;
+        }
+      if (precond == CERES_B200_PRECOND_SCHUR_JACOBI) {
+        block9_inverse(S, inv);
+      } else {
+        for (int i = 0; i < 81; ++i) inv[i] = 0.0;
+        for (int j = 0; j < 9; ++j)
+          inv[j * 10] = (precond == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(S[j * 10], Eps<T>::v()) : 1.0;
+      }
+      for (int i = 0; i < 81; ++i) pre[81 * (size_t)c + i] = (T)inv[i];
+    }
+  }
+  double v[2] = {gmax, gsq};
+  // only thread 0 holds values; block_reduce of zeros elsewhere is harmless
+  block_reduce<2>(v, 1u, sred2);
+  const int out[2] = {CERES_B200_STAT_GMAX_C, CERES_B200_STAT_GSQ_C};
+  grid_finish<2>(v, 1u, partials, &ba.counters[kCtrCamera], ba.stats, out);
+}
+
+// ======================================================================================
+// Implicit Schur product, point-major: for the points of one slice lane,
+//   t = sum_k Jp_k^T (Jc_k p_c(k)),  s = W^-1 t,  y_c(k) += Jc_k^T (Jc_k p_c(k) - Jp_k s)
+// The accumulation target y is shared memory (per-CTA partial) or global memory.
+// ======================================================================================
+template <typename T, typename TP, typename A>
+__device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int gw,
+                                              int nw) {
+  const int lane = threadIdx.x & 31;
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
+  for (int s = gw; s < ba.num_slices; s += nw) {
+    const int q = s * 32 + lane;
+    const int len = ba.slice_len[s];
+    const size_t base = (size_t)ba.slice_base[s];
+    A t0 = 0, t1 = 0, t2 = 0;
+    for (int k = 0; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k + lane;
+      const int c = ba.slot_cam[slot];
+      if (c < 0) continue;
+      T rv[kRec];
+      load_rec(jac, slot, rv);
+      const TP* pc = pvec + 9 * (size_t)c;
+      A u0 = 0, u1 = 0;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        const A pj = (A)pc[j];
+        u0 += (A)rv[j] * pj;
+        u1 += (A)rv[9 + j] * pj;
+      }
+      t0 += (A)rv[18] * u0 + (A)rv[21] * u1;
+      t1 += (A)rv[19] * u0 + (A)rv[22] * u1;
+      t2 += (A)rv[20] * u0 + (A)rv[23] * u1;
+    }
+    const T* wi = winv + 6 * (size_t)q;
+    const A w0 = (A)wi[0], w1 = (A)wi[1], w2 = (A)wi[2], w3 = (A)wi[3], w4 = (A)wi[4], w5 = (A)wi[5];
+    const A s0 = w0 * t0 + w1 * t1 + w2 * t2;
+    const A s1 = w1 * t0 + w3 * t1 + w4 * t2;
+    const A s2 = w2 * t0 + w4 * t1 + w5 * t2;
+    for (int k = 0; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k + lane;
+      const int c = ba.slot_cam[slot];
+      if (c < 0) continue;
+      T rv[kRec];
+      load_rec(jac, slot, rv);
+      const TP* pc = pvec + 9 * (size_t)c;
+      A u0 = 0, u1 = 0;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        const A pj = (A)pc[j];
+        u0 += (A)rv[j] * pj;
+        u1 += (A)rv[9 + j] * pj;
+      }
+      const A v0 = u0 - ((A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2);
+      const A v1 = u1 - ((A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2);
+      A* yc = y + 9 * (size_t)c;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[j] * v0 + (A)rv[9 + j] * v1);
+    }
+  }
+}
+
+// y = S x with float64 accumulation (global atomics), for tests and refinement.
+template <typename T>
+__global__ void __launch_bounds__(kWarpBlock) k_matvec_points(ceres_b200_ba_t ba, const double* __restrict__ x,
+                                                              double* y) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  matvec_slices<T, double, double>(ba, x, y, gw, nw);
+}
+
+__global__ void k_matvec_diag(ceres_b200_ba_t ba, const double* __restrict__ x, double* y, const double* __restrict__ rhs,
+                              double* out_res) {
+  const int n = 9 * ba.num_cameras;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const double v = y[j] + ba.cam_diag[j] * x[j];
+    y[j] = v;
+    if (out_res) out_res[j] = rhs[j] - v;
+  }
+}
+
+// ======================================================================================
+// Cooperative persistent PCG (linear.py:1216-1256) on the reduced camera system.
+// ======================================================================================
+struct PcgArgs {
+  const double* rhs;   // [n] right-hand side (float64)
+  double* x_out;       // [n] solution (float64); accumulated into when accumulate != 0
+  int accumulate;
+  int min_iterations, max_iterations;
+  double tolerance, eps;
+  int n;               // 9 * num_cameras
+  int cams_per_cta;
+  int smem_vectors;    // 1: p and y staged in shared memory
+  double* part_y_raw;  // [G][n] T  (smem mode)
+  double* part_b;      // [G]
+  double* part_c;      // [G][2]
+  double* result;      // [4]: iterations, success, rnorm, rhs_norm
+};
+
+constexpr int kPcgBlock = 512;
+
+template <typename T>
+__device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const T* __restrict__ r, T* __restrict__ z,
+                                              int c) {
+  const T* M = Minv + 81 * (size_t)c;
+  const T* rc = r + 9 * (size_t)c;
+  double rr[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) rr[j] = (double)rc[j];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s += (double)M[i * 9 + j] * rr[j];
+    z[9 * (size_t)c + i] = (T)s;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double red[2 * (kPcgBlock / 32)];
+  __shared__ double sh_scalar[4];
+  const int n = a.n;
+  T* ps = reinterpret_cast<T*>(smem_raw);
+  T* ys = ps + ((n + 3) & ~3);
+  T* __restrict__ X = reinterpret_cast<T*>(ba.pcg_x);
+  T* __restrict__ R = reinterpret_cast<T*>(ba.pcg_r);
+  T* __restrict__ Z = reinterpret_cast<T*>(ba.pcg_z);
+  T* __restrict__ Pbuf = reinterpret_cast<T*>(ba.pcg_p);
+  T* __restrict__ AP = reinterpret_cast<T*>(ba.pcg_ap);
+  const T* __restrict__ Minv = reinterpret_cast<const T*>(ba.precond);
+  T* part_y = reinterpret_cast<T*>(a.part_y_raw);
+  const GridBarrier gb{&ba.counters[kCtrBarCount], &ba.counters[kCtrBarGen], &ba.counters[kCtrBarFlag]};
+  const int G = gridDim.x;
+  const int c0 = blockIdx.x * a.cams_per_cta;
+  const int c1 = min(ba.num_cameras, c0 + a.cams_per_cta);
+  const int j0 = 9 * c0, j1 = 9 * max(c0, c1);
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (G * blockDim.x) >> 5;
+
+  // ---- init: x = 0, r = rhs, z = M^-1 r, p = z (written at the first phase A)
+  {
+    double rz = 0.0, rr = 0.0;
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+      X[j] = (T)0;
+      R[j] = (T)a.rhs[j];
+    }
+    __syncthreads();
+    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+    __syncthreads();
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+      const double r = (double)R[j], z = (double)Z[j];
+      rz += r * z;
+      rr += r * r;
+    }
+    double v[2] = {rz, rr};
+    block_reduce<2>(v, 0u, red);
+    if (threadIdx.x == 0) { a.part_c[2 * blockIdx.x] = v[0]; a.part_c[2 * blockIdx.x + 1] = v[1]; }
+  }
+  if (!grid_sync(gb)) return;
+  double rz_old = 0.0, rr = 0.0;
+  for (int g = 0; g < G; ++g) { rz_old += a.part_c[2 * g]; rr += a.part_c[2 * g + 1]; }
+  // the rhs norm is taken in float64 from the float64 rhs
+  double rhs_norm;
+  {
+    double v[1] = {0.0};
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) v[0] += a.rhs[j] * a.rhs[j];
+    block_reduce<1>(v, 0u, red);
+    if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
+    if (!grid_sync(gb)) return;
+    double t = 0.0;
+    for (int g = 0; g < G; ++g) t += a.part_b[g];
+    rhs_norm = fmax(sqrt(t), a.eps);
+  }
+  int iterations = 0;
+  bool success = false;
+  double rnorm = sqrt(rr);
+  double beta = 0.0;
+  int cur = 0;
+  if (!(a.min_iterations <= 0 && rnorm <= a.tolerance * rhs_norm)) {
+    for (int k = 0; k < a.max_iterations; ++k) {
+      // ---- phase A: p = z + beta p_old; y = (J_c^T J_c - H_cp W^-1 H_pc) p
+      const int nxt = k == 0 ? 0 : cur ^ 1;
+      T* Pold = Pbuf + (size_t)cur * n;
+      T* Pnew = Pbuf + (size_t)nxt * n;
+      if (a.smem_vectors) {
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+          const T pv = (k == 0) ? Z[j] : (T)((double)Z[j] + beta * (double)Pold[j]);
+          ps[j] = pv;
+          ys[j] = (T)0;
+          if (j >= j0 && j < j1) Pnew[j] = pv;
+        }
+        __syncthreads();
+        matvec_slices<T, T, T>(ba, ps, ys, gw, nw);
+        __syncthreads();
+        T* my = part_y + (size_t)blockIdx.x * n;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) my[j] = ys[j];
+      } else {
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+          Pnew[j] = (k == 0) ? Z[j] : (T)((double)Z[j] + beta * (double)Pold[j]);
+          AP[j] = (T)0;
+        }
+        if (!grid_sync(gb)) return;
+        matvec_slices<T, T, T>(ba, Pnew, AP, gw, nw);
+      }
+      cur = nxt;
+      if (!grid_sync(gb)) return;
+      // ---- phase B: Ap = sum of partials + D p ; partial p.Ap
+      {
+        double v[1] = {0.0};
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+          double y = 0.0;
+          if (a.smem_vectors) {
+            for (int g = 0; g < G; ++g) y += (double)part_y[(size_t)g * n + j];
+          } else {
+            y = (double)AP[j];
+          }
+          const double pj = (double)Pnew[j];
+          y += ba.cam_diag[j] * pj;
+          AP[j] = (T)y;
+          v[0] += pj * y;
+        }
+        block_reduce<1>(v, 0u, red);
+        if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
+      }
+      if (!grid_sync(gb)) return;
+      double denom = 0.0;
+      for (int g = 0; g < G; ++g) denom += a.part_b[g];
+      if (fabs(denom) <= a.eps) {
+        success = rnorm <= a.tolerance * rhs_norm;
+        break;
+      }
+      const double alpha = rz_old / denom;
+      // ---- phase C: x += alpha p ; r -= alpha Ap ; z = M^-1 r ; partial r.z, r.r
+      {
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+          X[j] = (T)((double)X[j] + alpha * (double)Pnew[j]);
+          R[j] = (T)((double)R[j] - alpha * (double)AP[j]);
+        }
+        __syncthreads();
+        for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+        __syncthreads();
+        double v[2] = {0.0, 0.0};
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+          const double r = (double)R[j];
+          v[0] += r * (double)Z[j];
+          v[1] += r * r;
+        }
+        block_reduce<2>(v, 0u, red);
+        if (threadIdx.x == 0) { a.part_c[2 * blockIdx.x] = v[0]; a.part_c[2 * blockIdx.x + 1] = v[1]; }
+      }
+      if (!grid_sync(gb)) return;
+      double rz_new = 0.0;
+      rr = 0.0;
+      for (int g = 0; g < G; ++g) { rz_new += a.part_c[2 * g]; rr += a.part_c[2 * g + 1]; }
+      rnorm = sqrt(rr);
+      iterations = k + 1;
+      if (iterations >= a.min_iterations && rnorm <= a.tolerance * rhs_norm) {
+        success = true;
+        break;
+      }
+      if (fabs(rz_old) <= a.eps) break;
+      beta = rz_new / rz_old;
+      rz_old = rz_new;
+    }
+  } else {
+    success = true;
+  }
+  // ---- output
+  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    const double xv = (double)X[j];
+    a.x_out[j] = a.accumulate ? a.x_out[j] + xv : xv;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.result[0] = (double)iterations;
+    a.result[1] = success ? 1.0 : 0.0;
+    a.result[2] = rnorm;
+    a.result[3] = rhs_norm;
+  }
+  (void)sh_scalar;
+}
+
+// ======================================================================================
+// Step: candidate cameras, then point back-substitution + model decrease + candidate cost
+// ======================================================================================
+__global__ void k_camera_step(ceres_b200_ba_t ba, double* partials) {
+  __shared__ double red[3 * 8];
+  double sq = 0.0, nonfinite = 0.0, state = 0.0;
+  const int n = 9 * ba.num_cameras;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int c = j / 9;
+    double d = ba.cam_const[c] ? 0.0 : ba.step_cameras[j];
+    if (!ba.cam_const[c]) {
+      if (!isfinite(d)) nonfinite += 1.0;
+      sq += d * d;
+    }
+    ba.step_cameras[j] = d;
+    const double xc = ba.cameras[j] + d;
+    ba.cand_cameras[j] = xc;
+    state += xc * xc;
+  }
+  double v[3] = {sq, nonfinite, state};
+  block_reduce<3>(v, 0u, red);
+  const int out[3] = {CERES_B200_STAT_STEP_SQ_C, CERES_B200_STAT_NONFINITE, CERES_B200_STAT_CAND_STATE_SQ_C};
+  grid_finish<3>(v, 0u, partials, &ba.counters[kCtrCamStep], ba.stats, out);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWarpBlock) k_step(ceres_b200_ba_t ba, double* partials) {
+  __shared__ double red[5 * (kWarpBlock / 32)];
+  const LossSpec L = loss_spec(ba);
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
+  double cand = 0.0, model = 0.0, sq = 0.0, nonfinite = 0.0, state = 0.0;
+  unsigned err = 0;
+  for (int s = gw; s < ba.num_slices; s += nw) {
+    const int q = s * 32 + lane;
+    const int len = ba.slice_len[s];
+    const size_t base = (size_t)ba.slice_base[s];
+    double t[3] = {0, 0, 0};
+    for (int k = 0; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k + lane;
+      const int c = ba.slot_cam[slot];
+      if (c < 0) continue;
+      T rv[kRec];
+      load_rec(jac, slot, rv);
+      const double* dc = ba.step_cameras + 9 * (size_t)c;
+      double u0 = 0.0, u1 = 0.0;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) { u0 += (double)rv[j] * dc[j]; u1 += (double)rv[9 + j] * dc[j]; }
+#pragma unroll
+      for (int m = 0; m < 3; ++m) t[m] += (double)rv[18 + m] * u0 + (double)rv[21 + m] * u1;
+    }
+    double dp[3] = {0, 0, 0};
+    const bool pconst = ba.pt_const[q] != 0;
+    if (!pconst) {
+      double wi[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) wi[i] = (double)winv[6 * (size_t)q + i];
+      double wt[3];
+      sym3_mul(wi, t, wt);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        dp[m] = ba.winv_ga[3 * (size_t)q + m] - wt[m];
+        if (!isfinite(dp[m])) nonfinite += 1.0;
+        sq += dp[m] * dp[m];
+      }
+    }
+    double Xc[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      ba.step_points[3 * (size_t)q + m] = dp[m];
+      Xc[m] = ba.points[3 * (size_t)q + m] + dp[m];
+      ba.cand_points[3 * (size_t)q + m] = Xc[m];
+      state += Xc[m] * Xc[m];
+    }
+    for (int k = 0; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k + lane;
+      const int c = ba.slot_cam[slot];
+      if (c < 0) continue;
+      T rv[kRec];
+      load_rec(jac, slot, rv);
+      const double2 r = reinterpret_cast<const double2*>(ba.res)[slot];
+      const double* dc = ba.step_cameras + 9 * (size_t)c;
+      double j0 = 0.0, j1 = 0.0;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) { j0 += (double)rv[j] * dc[j]; j1 += (double)rv[9 + j] * dc[j]; }
+#pragma unroll
+      for (int m = 0; m < 3; ++m) { j0 += (double)rv[18 + m] * dp[m]; j1 += (double)rv[21 + m] * dp[m]; }
+      const double a0 = r.x + j0, a1 = r.y + j1;
+      model += 0.5 * (r.x * r.x + r.y * r.y) - 0.5 * (a0 * a0 + a1 * a1);
+      const double2 ob = reinterpret_cast<const double2*>(ba.slot_obs)[slot];
+      Proj o;
+      snavely<false>(ba.cand_cameras + 9 * (size_t)c, Xc, ob.x, ob.y, o);
+      cand += robustify<false>(L, o, err);
+    }
+  }
+  if (err) atomicOr(&ba.counters[kCtrError], err);
+  double v[5] = {cand, model, sq, nonfinite, state};
+  block_reduce<5>(v, 0u, red);
+  const int out[5] = {CERES_B200_STAT_CAND_COST, CERES_B200_STAT_MODEL, CERES_B200_STAT_STEP_SQ_P,
+                      CERES_B200_STAT_NONFINITE, CERES_B200_STAT_CAND_STATE_SQ_P};
+  // the camera step kernel's non-finite count is added afterwards (k_add_nonfinite)
+  grid_finish<5>(v, 0u, partials, &ba.counters[kCtrStep], ba.stats, out);
+}
+
+__global__ void k_norm_into(const double* __restrict__ v, int n, double* out) {
+  __shared__ double red[8];
+  double a[1] = {0.0};
+  for (int j = threadIdx.x; j < n; j += blockDim.x) a[0] += v[j] * v[j];
+  block_reduce<1>(a, 0u, red);
+  if (threadIdx.x == 0) *out = sqrt(a[0]);
+}
+
+__global__ void k_add_nonfinite(double* stats, const double* cam_nonfinite) {
+  stats[CERES_B200_STAT_NONFINITE] += *cam_nonfinite;
+}
+
+__global__ void k_copy_error(ceres_b200_ba_t ba) {
+  ba.stats[CERES_B200_STAT_ERROR] = (double)(ba.counters[kCtrError] | ba.counters[kCtrBarFlag]);
+}
+
+__global__ void k_copy_result(ceres_b200_ba_t ba, const double* result, double refine_rnorm) {
+  ba.stats[CERES_B200_STAT_PCG_ITERS] = result[0];
+  ba.stats[CERES_B200_STAT_PCG_SUCCESS] = result[1];
+  ba.stats[CERES_B200_STAT_PCG_RNORM] = result[2];
+  ba.stats[CERES_B200_STAT_RHS_NORM] = result[3];
+  ba.stats[CERES_B200_STAT_REFINE_RNORM] = refine_rnorm;
+}
+
+// ======================================================================================
+// Explicit reduced camera matrix and its dense Cholesky solve (the DENSE_SCHUR /
+// SPARSE_SCHUR route: linear.py:667-699, solver.py:788-795). S is float64 [n][n],
+// n = 9 num_cameras, zeroed by the caller.
+// ======================================================================================
+template <typename T>
+__global__ void __launch_bounds__(kWarpBlock) k_schur_explicit(ceres_b200_ba_t ba, double* S, int n) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
+  for (int s = gw; s < ba.num_slices; s += nw) {
+    const int q = s * 32 + lane;
+    const int len = ba.slice_len[s];
+    const size_t base = (size_t)ba.slice_base[s];
+    double wi[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) wi[i] = (double)winv[6 * (size_t)q + i];
+    for (int i = 0; i < len; ++i) {
+      const size_t si = base + 32 * (size_t)i + lane;
+      const int ci = ba.slot_cam[si];
+      if (ci < 0 || ba.cam_const[ci]) continue;
+      T ri[kRec];
+      load_rec(jac, si, ri);
+      const double jp0[3] = {(double)ri[18], (double)ri[19], (double)ri[20]};
+      const double jp1[3] = {(double)ri[21], (double)ri[22], (double)ri[23]};
+      double P0[3], P1[3];
+      sym3_mul(wi, jp0, P0);
+      sym3_mul(wi, jp1, P1);
+      for (int k = 0; k < len; ++k) {
+        const size_t sk = base + 32 * (size_t)k + lane;
+        const int ck = ba.slot_cam[sk];
+        if (ck < 0 || ba.cam_const[ck]) continue;
+        T rk[kRec];
+        load_rec(jac, sk, rk);
+        const double C00 = P0[0] * rk[18] + P0[1] * rk[19] + P0[2] * rk[20];
+        const double C01 = P0[0] * rk[21] + P0[1] * rk[22] + P0[2] * rk[23];
+        const double C10 = P1[0] * rk[18] + P1[1] * rk[19] + P1[2] * rk[20];
+        const double C11 = P1[0] * rk[21] + P1[1] * rk[22] + P1[2] * rk[23];
+        const double d = (i == k) ? 1.0 : 0.0;
+        const double M00 = d - C00, M01 = -C01, M10 = -C10, M11 = d - C11;
+        for (int a = 0; a < 9; ++a) {
+          const double t0 = (double)ri[a] * M00 + (double)ri[9 + a] * M10;
+          const double t1 = (double)ri[a] * M01 + (double)ri[9 + a] * M11;
+          double* row = S + (size_t)(9 * ci + a) * n + 9 * (size_t)ck;
+#pragma unroll
+          for (int b = 0; b < 9; ++b) atomicAdd(row + b, t0 * (double)rk[b] + t1 * (double)rk[9 + b]);
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_dense_diag(ceres_b200_ba_t ba, double* S, int n) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int c = j / 9;
+    if (ba.cam_const[c]) S[(size_t)j * n + j] = 1.0;
+    else S[(size_t)j * n + j] += ba.cam_diag[j];
+  }
+}
+
+constexpr int kCholSmemMax = 160;  // n * n doubles fit in one CTA's shared memory
+
+// One-CTA Cholesky solve of S x = rhs in shared memory (n <= kCholSmemMax).
+__global__ void __launch_bounds__(1024) k_chol_smem(const double* __restrict__ S, const double* __restrict__ rhs,
+                                                    double* __restrict__ x, int n, unsigned* err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* A = reinterpret_cast<double*>(smem_raw);
+  double* y = A + (size_t)n * n;
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) A[i] = S[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = rhs[i];
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (threadIdx.x == 0) {
+      const double d = A[j * n + j];
+      if (!(d > 0.0)) bad = 1;
+      A[j * n + j] = sqrt(fmax(d, kTiny64));
+    }
+    __syncthreads();
+    const double ljj = A[j * n + j];
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[i * n + j] /= ljj;
+    __syncthreads();
+    const int m = n - j - 1;
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+      const int i = j + 1 + t / m, k = j + 1 + t % m;
+      if (k <= i) A[i * n + k] -= A[i * n + j] * A[k * n + j];
+    }
+    __syncthreads();
+  }
+  // forward L y = b, backward L^T x = y (one warp, column-oriented)
+  if (threadIdx.x < 32) {
+    for (int j = 0; j < n; ++j) {
+      const double yj = y[j] / A[j * n + j];
+      __syncwarp();
+      if (threadIdx.x == 0) y[j] = yj;
+      for (int i = j + 1 + threadIdx.x; i < n; i += 32) y[i] -= A[i * n + j] * yj;
+      __syncwarp();
+    }
+    for (int j = n - 1; j >= 0; --j) {
+      double s = 0.0;
+      for (int i = j + 1 + threadIdx.x; i < n; i += 32) s += A[i * n + j] * y[i];
+      s = warp_sum(s);
+      if (threadIdx.x == 0) y[j] = (y[j] - s) / A[j * n + j];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = y[i];
+  if (threadIdx.x == 0 && bad) atomicOr(err, 4u);
+}
+
+// Cooperative right-looking Cholesky in global memory for larger n; the lower
+// triangle of A is overwritten by L. Every barrier wait is bounded.
+__global__ void __launch_bounds__(512) k_chol_global(double* A, int n, GridBarrier gb, unsigned* err) {
+  for (int j = 0; j < n; ++j) {
+    if (blockIdx.x == 0) {
+      __shared__ double ljj;
+      if (threadIdx.x == 0) {
+        const double d = A[(size_t)j * n + j];
+        if (!(d > 0.0)) atomicOr(err, 4u);
+        ljj = sqrt(fmax(d, kTiny64));
+        A[(size_t)j * n + j] = ljj;
+      }
+      __syncthreads();
+      for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + j] /= ljj;
+    }
+    if (!grid_sync(gb)) return;
+    const size_t m = (size_t)(n - j - 1);
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < m * m; t += (size_t)gridDim.x * blockDim.x) {
+      const int i = j + 1 + (int)(t / m), k = j + 1 + (int)(t % m);
+      if (k <= i) A[(size_t)i * n + k] -= A[(size_t)i * n + j] * A[(size_t)k * n + j];
+    }
+    if (!grid_sync(gb)) return;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_tri_solve(const double* __restrict__ Lm, const double* __restrict__ rhs,
+                                                    double* __restrict__ x, int n) {
+  // x holds y during the forward pass; column-oriented updates by the whole CTA
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = rhs[i];
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    __shared__ double yj;
+    if (threadIdx.x == 0) { yj = x[j] / Lm[(size_t)j * n + j]; x[j] = yj; }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) x[i] -= Lm[(size_t)i * n + j] * yj;
+    __syncthreads();
+  }
+  __shared__ double red[32];
+  for (int j = n - 1; j >= 0; --j) {
+    double v[1] = {0.0};
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) v[0] += Lm[(size_t)i * n + j] * x[i];
+    block_reduce<1>(v, 0u, red);
+    if (threadIdx.x == 0) x[j] = (x[j] - v[0]) / Lm[(size_t)j * n + j];
+    __syncthreads();
+  }
+}
+
+// ======================================================================================
+// C ABI
+// ======================================================================================
+namespace {
+
+bool valid(const ceres_b200_ba_t* ba) {
+  if (!ba) return false;
+  if (ba->num_cameras < 0 || ba->num_points < 0 || ba->num_slices < 0 || ba->num_slots < 0) return false;
+  if (ba->num_points != 32 * ba->num_slices) return false;
+  if (ba->precision != CERES_B200_FP64 && ba->precision != CERES_B200_FP32) return false;
+  if (!ba->counters || !ba->stats) return false;
+  if (ba->num_slices > 0 && (!ba->slice_base || !ba->slice_len || !ba->slot_cam || !ba->slot_obs || !ba->jac ||
+                             !ba->res || !ba->cameras || !ba->points || !ba->pt_const))
+    return false;
+  if (ba->num_cameras > 0 && (!ba->cam_offsets || !ba->cam_const || !ba->cam_diag || !ba->rhs || !ba->precond))
+    return false;
+  return true;
+}
+
+int check_launch() {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "ceres_b200: CUDA error %s\n", cudaGetErrorString(e));
+    return CERES_B200_ECUDA;
+  }
+  return CERES_B200_OK;
+}
+
+struct PcgLayout {
+  int grid = 0;
+  int cams_per_cta = 0;
+  int smem_vectors = 0;
+  size_t dyn_smem = 0;
+  size_t aux = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0, total = 0;
+};
+
+template <typename T>
+int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
+  const DevInfo d = device_info();
+  const int n = 9 * ba.num_cameras;
+  const size_t vec_bytes = (size_t)((n + 3) & ~3) * sizeof(T);
+  const size_t static_smem = 2 * (kPcgBlock / 32) * sizeof(double) + 64;
+  L.smem_vectors = (2 * vec_bytes + static_smem <= (size_t)d.max_smem_optin - 1024) ? 1 : 0;
+  L.dyn_smem = L.smem_vectors ? 2 * vec_bytes : 0;
+  auto kern = k_pcg<T>;
+  if (L.dyn_smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.dyn_smem) != cudaSuccess)
+      return CERES_B200_ESMEM;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPcgBlock, L.dyn_smem) != cudaSuccess || per_sm < 1)
+    return CERES_B200_ECOOP;
+  L.grid = d.sms * per_sm;
+  const int needed_for_cams = ba.num_cameras > 0 ? ba.num_cameras : 1;
+  L.cams_per_cta = (needed_for_cams + L.grid - 1) / L.grid;
+  size_t off = red_area_bytes(ba, d);
+  L.aux = off;
+  off += 256;
+  L.part_y = off;
+  off += L.smem_vectors ? (size_t)L.grid * n * sizeof(T) : 0;
+  off = (off + 255) & ~(size_t)255;
+  L.part_b = off;
+  off += (size_t)L.grid * sizeof(double);
+  L.part_c = off;
+  off += (size_t)L.grid * 2 * sizeof(double);
+  L.result = off;
+  off += 8 * sizeof(double);
+  off = (off + 255) & ~(size_t)255;
+  L.x64 = off;
+  off += (size_t)n * sizeof(double);
+  L.r64 = off;
+  off += (size_t)n * sizeof(double);
+  L.total = (off + 255) & ~(size_t)255;
+  return CERES_B200_OK;
+}
+
+int scratch_bytes_impl(const ceres_b200_ba_t& ba, size_t& bytes) {
+  PcgLayout L;
+  const int rc = ba.precision == CERES_B200_FP32 ? pcg_layout<float>(ba, L) : pcg_layout<double>(ba, L);
+  if (rc) return rc;
+  bytes = L.total;
+  return CERES_B200_OK;
+}
+
+template <typename T>
+int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int accumulate, int precond,
+               int min_it, int max_it, double tol, cudaStream_t st, const PcgLayout& L, char* scratch) {
+  (void)precond;
+  PcgArgs a;
+  a.rhs = rhs;
+  a.x_out = x_out;
+  a.accumulate = accumulate;
+  a.min_iterations = min_it;
+  a.max_iterations = max_it;
+  a.tolerance = tol;
+  a.eps = (double)Eps<T>::v();
+  a.n = 9 * ba.num_cameras;
+  a.cams_per_cta = L.cams_per_cta;
+  a.smem_vectors = L.smem_vectors;
+  a.part_y_raw = reinterpret_cast<double*>(scratch + L.part_y);
+  a.part_b = reinterpret_cast<double*>(scratch + L.part_b);
+  a.part_c = reinterpret_cast<double*>(scratch + L.part_c);
+  a.result = reinterpret_cast<double*>(scratch + L.result);
+  // barrier words start at zero for every launch
+  if (cudaMemsetAsync(&ba.counters[kCtrBarCount], 0, 3 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
+  ceres_b200_ba_t bcopy = ba;
+  void* args[] = {&bcopy, &a};
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg<T>, dim3(L.grid), dim3(kPcgBlock), args,
+                                                    L.dyn_smem, st);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "ceres_b200: cooperative PCG launch failed: %s\n", cudaGetErrorString(e));
+    return CERES_B200_ECOOP;
+  }
+  return CERES_B200_OK;
+}
+
+// y = S x (float64 accumulation; the Jacobian is read in its stored precision T).
+// When rhs and res are given, res = rhs - y as well.
+template <typename T>
+int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, const double* rhs, double* res, cudaStream_t st) {
+  const DevInfo d = device_info();
+  const int n = 9 * ba.num_cameras;
+  if (cudaMemsetAsync(y, 0, (size_t)n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
+  if (ba.num_slices > 0) k_matvec_points<T><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, x, y);
+  k_matvec_diag<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(ba, x, y, rhs, res);
+  return check_launch();
+}
+
+template <typename T>
+int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, double tol, int max_ref, cudaStream_t st) {
+  PcgLayout L;
+  int rc = pcg_layout<T>(ba, L);
+  if (rc) return rc;
+  if (!ba.scratch || (size_t)ba.scratch_bytes < L.total) return CERES_B200_EINVAL;
+  char* scratch = reinterpret_cast<char*>(ba.scratch);
+  const int n = 9 * ba.num_cameras;
+  if (n == 0) return CERES_B200_OK;
+  rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, precond, min_it, max_it, tol, st, L, scratch);
+  if (rc) return rc;
+  double* result = reinterpret_cast<double*>(scratch + L.result);
+  k_copy_result<<<1, 1, 0, st>>>(ba, result, -1.0);
+  if (max_ref > 0 && sizeof(T) == sizeof(float)) {
+    // float64 refinement: res = rhs - S x (float64 accumulation); solve S dx = res; x += dx
+    double* y64 = reinterpret_cast<double*>(scratch + L.x64);
+    double* r64 = reinterpret_cast<double*>(scratch + L.r64);
+    for (int it = 0; it < max_ref; ++it) {
+      rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
+      if (rc) return rc;
+      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, precond, 0, max_it, tol, st, L, scratch);
+      if (rc) return rc;
+    }
+    rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
+    if (rc) return rc;
+    k_norm_into<<<1, 256, 0, st>>>(r64, n, ba.stats + CERES_B200_STAT_REFINE_RNORM);
+  }
+  k_copy_error<<<1, 1, 0, st>>>(ba);
+  return check_launch();
+}
+
+}  // namespace
+
+extern "C" {
+
+int ceres_b200_abi_version(void) { return CERES_B200_ABI_VERSION; }
+
+int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out) {
+  if (!ba || !bytes_out) return CERES_B200_EINVAL;
+  size_t b = 0;
+  const int rc = scratch_bytes_impl(*ba, b);
+  if (rc) return rc;
+  *bytes_out = (int64_t)b;
+  return CERES_B200_OK;
+}
+
+int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* stream) {
+  if (!valid(ba) || !ba->scratch) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevInfo d = device_info();
+  const int grid = slice_grid(*ba, d);
+  double* partials = reinterpret_cast<double*>(ba->scratch);
+  if (ba->precision == CERES_B200_FP32) {
+    if (with_jacobian) k_evaluate<float, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+    else k_evaluate<float, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+  } else {
+    if (with_jacobian) k_evaluate<double, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+    else k_evaluate<double, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+  }
+  k_copy_error<<<1, 1, 0, st>>>(*ba);
+  return check_launch();
+}
+
+int ceres_b200_ba_point_assemble(const ceres_b200_ba_t* ba, double radius, double min_diagonal, double max_diagonal,
+                                 int jacobi_scaling, void* stream) {
+  if (!valid(ba) || !ba->scratch || !ba->winv || !ba->winv_ga) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevInfo d = device_info();
+  const double inv_radius = 1.0 / fmax(radius, kEps64);
+  double* partials = reinterpret_cast<double*>(ba->scratch);
+  const int grid = slice_grid(*ba, d);
+  if (ba->precision == CERES_B200_FP32)
+    k_point_assemble<float><<<grid, kWarpBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal, jacobi_scaling,
+                                                         partials);
+  else
+    k_point_assemble<double><<<grid, kWarpBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal, jacobi_scaling,
+                                                          partials);
+  return check_launch();
+}
+
+int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, double min_diagonal, double max_diagonal,
+                                  int jacobi_scaling, int preconditioner, void* stream) {
+  if (!valid(ba) || !ba->scratch) return CERES_B200_EINVAL;
+  if (preconditioner < CERES_B200_PRECOND_IDENTITY || preconditioner > CERES_B200_PRECOND_SCHUR_JACOBI)
+    return CERES_B200_EINVAL;
+  if (ba->num_cameras == 0) return CERES_B200_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const double inv_radius = 1.0 / fmax(radius, kEps64);
+  double* partials = reinterpret_cast<double*>(ba->scratch);
+  if (ba->precision == CERES_B200_FP32)
+    k_camera_assemble<float><<<ba->num_cameras, kCamBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal,
+                                                                    jacobi_scaling, preconditioner, partials);
+  else
+    k_camera_assemble<double><<<ba->num_cameras, kCamBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal,
+                                                                     jacobi_scaling, preconditioner, partials);
+  return check_launch();
+}
+
+int ceres_b200_ba_pcg(const ceres_b200_ba_t* ba, int preconditioner, int min_iterations, int max_iterations,
+                      double tolerance, int max_refinements, void* stream) {
+  if (!valid(ba) || max_iterations < 0 || min_iterations < 0 || max_refinements < 0) return CERES_B200_EINVAL;
+  if (!ba->pcg_x || !ba->pcg_r || !ba->pcg_z || !ba->pcg_p || !ba->pcg_ap || !ba->step_cameras) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ba->precision == CERES_B200_FP32)
+    return pcg_impl<float>(*ba, preconditioner, min_iterations, max_iterations, tolerance, max_refinements, st);
+  return pcg_impl<double>(*ba, preconditioner, min_iterations, max_iterations, tolerance, max_refinements, st);
+}
+
+int ceres_b200_ba_schur_matvec(const ceres_b200_ba_t* ba, const double* x, double* y, void* stream) {
+  if (!valid(ba) || !x || !y) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = 9 * ba->num_cameras;
+  if (n == 0) return CERES_B200_OK;
+  if (ba->precision == CERES_B200_FP32) return matvec64<float>(*ba, x, y, nullptr, nullptr, st);
+  return matvec64<double>(*ba, x, y, nullptr, nullptr, st);
+}
+
+int ceres_b200_ba_step(const ceres_b200_ba_t* ba, void* stream) {
+  if (!valid(ba) || !ba->scratch || !ba->cand_cameras || !ba->cand_points || !ba->step_points) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevInfo d = device_info();
+  double* partials = reinterpret_cast<double*>(ba->scratch);
+  // camera candidates; their non-finite count goes to a scratch double
+  const int n = 9 * ba->num_cameras;
+  const int cgrid = n > 0 ? ((n + 255) / 256 < 64 ? (n + 255) / 256 : 64) : 1;
+  PcgLayout L;
+  const int lrc = ba->precision == CERES_B200_FP32 ? pcg_layout<float>(*ba, L) : pcg_layout<double>(*ba, L);
+  if (lrc) return lrc;
+  if ((size_t)ba->scratch_bytes < L.total) return CERES_B200_EINVAL;
+  ceres_b200_ba_t b2 = *ba;
+  double* cam_stats = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + L.aux);
+  b2.stats = cam_stats;
+  k_camera_step<<<cgrid, 256, 0, st>>>(b2, partials);
+  const int grid = slice_grid(*ba, d);
+  if (ba->precision == CERES_B200_FP32) k_step<float><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+  else k_step<double><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+  // STEP_SQ_C and the camera non-finite count into the shared stats
+  k_add_nonfinite<<<1, 1, 0, st>>>(ba->stats, cam_stats + CERES_B200_STAT_NONFINITE);
+  cudaMemcpyAsync(ba->stats + CERES_B200_STAT_STEP_SQ_C, cam_stats + CERES_B200_STAT_STEP_SQ_C, sizeof(double),
+                  cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(ba->stats + CERES_B200_STAT_CAND_STATE_SQ_C, cam_stats + CERES_B200_STAT_CAND_STATE_SQ_C,
+                  sizeof(double), cudaMemcpyDeviceToDevice, st);
+  k_copy_error<<<1, 1, 0, st>>>(*ba);
+  return check_launch();
+}
+
+int ceres_b200_dense_cholesky_solve(double* H, const double* rhs, double* x, int64_t n64, uint32_t* flags,
+                                    void* stream) {
+  if (!H || !rhs || !x || !flags || n64 < 0 || n64 > (int64_t)1 << 30) return CERES_B200_EINVAL;
+  const int n = (int)n64;
+  if (n == 0) return CERES_B200_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevInfo d = device_info();
+  if (n <= kCholSmemMax) {
+    const size_t smem = ((size_t)n * n + n) * sizeof(double);
+    if (cudaFuncSetAttribute(k_chol_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return CERES_B200_ESMEM;
+    k_chol_smem<<<1, 1024, smem, st>>>(H, rhs, x, n, flags + 3);
+    return check_launch();
+  }
+  if (cudaMemsetAsync(flags, 0, 3 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_global, 512, 0) != cudaSuccess || per_sm < 1)
+    return CERES_B200_ECOOP;
+  GridBarrier gb{flags, flags + 1, flags + 2};
+  unsigned* errp = flags + 3;
+  int nn = n;
+  void* args[] = {&H, &nn, &gb, &errp};
+  if (cudaLaunchCooperativeKernel((const void*)k_chol_global, dim3(d.sms * per_sm), dim3(512), args, 0, st) !=
+      cudaSuccess)
+    return CERES_B200_ECOOP;
+  k_tri_solve<<<1, 1024, 0, st>>>(H, rhs, x, n);
+  return check_launch();
+}
+
+int ceres_b200_dense_schur_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out) {
+  if (!ba || !bytes_out || ba->num_cameras < 0) return CERES_B200_EINVAL;
+  const int64_t n = 9 * (int64_t)ba->num_cameras;
+  *bytes_out = n * n * (int64_t)sizeof(double);
+  return CERES_B200_OK;
+}
+
+int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, void* stream) {
+  if (!valid(ba) || !ba->step_cameras) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = 9 * ba->num_cameras;
+  if (n == 0) return CERES_B200_OK;
+  if (!work) return CERES_B200_EINVAL;
+  const DevInfo d = device_info();
+  if (cudaMemsetAsync(work, 0, (size_t)n * n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
+  if (ba->num_slices > 0) {
+    if (ba->precision == CERES_B200_FP32)
+      k_schur_explicit<float><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, work, n);
+    else
+      k_schur_explicit<double><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, work, n);
+  }
+  k_dense_diag<<<(n + 255) / 256, 256, 0, st>>>(*ba, work, n);
+  if (n <= kCholSmemMax) {
+    const size_t smem = ((size_t)n * n + n) * sizeof(double);
+    if (cudaFuncSetAttribute(k_chol_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return CERES_B200_ESMEM;
+    k_chol_smem<<<1, 1024, smem, st>>>(work, ba->rhs, ba->step_cameras, n, &ba->counters[kCtrError]);
+  } else {
+    if (cudaMemsetAsync(&ba->counters[kCtrBarCount], 0, 3 * sizeof(uint32_t), st) != cudaSuccess)
+      return CERES_B200_ECUDA;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_global, 512, 0) != cudaSuccess || per_sm < 1)
+      return CERES_B200_ECOOP;
+    GridBarrier gb{&ba->counters[kCtrBarCount], &ba->counters[kCtrBarGen], &ba->counters[kCtrBarFlag]};
+    unsigned* errp = &ba->counters[kCtrError];
+    int nn = n;
+    void* args[] = {&work, &nn, &gb, &errp};
+    if (cudaLaunchCooperativeKernel((const void*)k_chol_global, dim3(d.sms * per_sm), dim3(512), args, 0, st) !=
+        cudaSuccess)
+      return CERES_B200_ECOOP;
+    k_tri_solve<<<1, 1024, 0, st>>>(work, ba->rhs, ba->step_cameras, n);
+  }
+  k_copy_error<<<1, 1, 0, st>>>(*ba);
+  return check_launch();
+}
+
+}  // extern "C"

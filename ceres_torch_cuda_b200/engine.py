@@ -1,0 +1,633 @@
+"""Device-resident bundle-adjustment state and the Levenberg-Marquardt driver.
+
+``BAEngine`` owns every device buffer of one problem (allocated with torch),
+builds the sliced-ELL observation store on the GPU, and drives the C-ABI
+kernels. ``run_lm`` is the trust-region loop of ceres-torch's
+``_trust_region_solve`` (solver.py:35-357) with the same decisions, counters
+and termination messages; the only host/device traffic per LM iteration is one
+read of a 256-byte control block (two on accepted steps).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from .losses import device_loss
+from .types import (CallbackReturnType, IterationSummary, LinearSolverType, LoggingType, PreconditionerType,
+                    SolverOptions, SolverSummary, TerminationType, TrustRegionStrategyType)
+
+_PRECOND = {
+    PreconditionerType.IDENTITY: _lib.PRECOND_IDENTITY,
+    PreconditionerType.JACOBI: _lib.PRECOND_JACOBI,
+    PreconditionerType.SCHUR_JACOBI: _lib.PRECOND_SCHUR_JACOBI,
+}
+
+PRECISIONS = ("fp64", "mixed")
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+@dataclass
+class Layout:
+    """Sliced-ELL observation store (see include/ceres_b200.h)."""
+
+    num_slices: int
+    num_slots: int
+    max_slice_len: int
+    has_duplicate_cameras: bool
+    slice_base: torch.Tensor      # int32 [S]
+    slice_len: torch.Tensor       # int32 [S]
+    slot_cam: torch.Tensor        # int32 [slots]
+    slot_obs: torch.Tensor        # float64 [slots, 2]
+    slot_of_obs: torch.Tensor     # int64 [no]  slot of each input observation
+    cam_offsets: torch.Tensor     # int32 [nc+1]
+    cam_entries: torch.Tensor     # int32 [no, 2]  (slot, q)
+    lane_point: torch.Tensor      # int64 [32 S]  original point id of each lane, -1 padding
+    point_order: torch.Tensor     # int64 [np]   q -> point id for q < np
+
+
+def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observations: torch.Tensor,
+                 num_cameras: int, num_points: int) -> Layout:
+    """Bucket observations by point (stable in observation order) into slices of
+    32 points sorted by track length, and list them per camera. GPU torch ops."""
+    dev = camera_index.device
+    no = int(camera_index.numel())
+    ci = camera_index.to(torch.int64)
+    pi = point_index.to(torch.int64)
+    counts = torch.bincount(pi, minlength=num_points) if no else torch.zeros(num_points, dtype=torch.int64, device=dev)
+    order = torch.argsort(-counts, stable=True)
+    num_slices = (num_points + 31) // 32
+    np_pad = 32 * num_slices
+    lane_point = torch.full((np_pad,), -1, dtype=torch.int64, device=dev)
+    lane_point[:num_points] = order
+    counts_q = torch.zeros(np_pad, dtype=torch.int64, device=dev)
+    counts_q[:num_points] = counts[order]
+    slice_len = counts_q.view(num_slices, 32).amax(dim=1) if num_slices else counts_q[:0]
+    csum = torch.cumsum(slice_len, 0)
+    slice_base = 32 * (csum - slice_len)
+    num_slots = int(32 * int(csum[-1])) if num_slices else 0
+    inv_order = torch.empty(num_points, dtype=torch.int64, device=dev)
+    inv_order[order] = torch.arange(num_points, device=dev)
+    if no:
+        obs_sorted = torch.argsort(pi, stable=True)
+        pstart = torch.cumsum(counts, 0) - counts
+        rank = torch.empty(no, dtype=torch.int64, device=dev)
+        rank[obs_sorted] = torch.arange(no, device=dev) - pstart[pi[obs_sorted]]
+        q = inv_order[pi]
+        slot = slice_base[q // 32] + 32 * rank + (q % 32)
+    else:
+        q = torch.zeros(0, dtype=torch.int64, device=dev)
+        slot = q
+    slot_cam = torch.full((max(num_slots, 1),), -1, dtype=torch.int32, device=dev)
+    slot_obs = torch.zeros((max(num_slots, 1), 2), dtype=torch.float64, device=dev)
+    if no:
+        slot_cam[slot] = ci.to(torch.int32)
+        slot_obs[slot] = observations.to(torch.float64)
+    key = ci * max(num_slots, 1) + slot
+    perm = torch.argsort(key)
+    cam_entries = torch.stack([slot[perm], q[perm]], dim=1).to(torch.int32).contiguous()
+    cam_counts = torch.bincount(ci, minlength=num_cameras) if no else torch.zeros(num_cameras, dtype=torch.int64,
+                                                                                    device=dev)
+    cam_offsets = torch.zeros(num_cameras + 1, dtype=torch.int64, device=dev)
+    cam_offsets[1:] = torch.cumsum(cam_counts, 0)
+    has_dup = False
+    if no:
+        pk = torch.sort(pi * max(num_cameras, 1) + ci).values
+        has_dup = bool((pk[1:] == pk[:-1]).any()) if no > 1 else False
+    return Layout(
+        num_slices=num_slices, num_slots=num_slots,
+        max_slice_len=int(slice_len.max()) if num_slices else 0,
+        has_duplicate_cameras=has_dup,
+        slice_base=slice_base.to(torch.int32).contiguous(), slice_len=slice_len.to(torch.int32).contiguous(),
+        slot_cam=slot_cam, slot_obs=slot_obs, slot_of_obs=slot,
+        cam_offsets=cam_offsets.to(torch.int32), cam_entries=cam_entries if no else torch.zeros((1, 2), dtype=torch.int32, device=dev),
+        lane_point=lane_point, point_order=order,
+    )
+
+
+class BAEngine:
+    """All device state of one bundle-adjustment problem."""
+
+    def __init__(self, cameras: torch.Tensor, points: torch.Tensor, observations: torch.Tensor,
+                 camera_index: torch.Tensor, point_index: torch.Tensor, *, loss=None,
+                 camera_constant: torch.Tensor | None = None, point_constant: torch.Tensor | None = None,
+                 precision: str = "fp64", layout: Layout | None = None):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {PRECISIONS}")
+        if cameras.device.type != "cuda":
+            raise _lib.NativeLibraryError("the bundle-adjustment engine needs CUDA tensors")
+        self.lib = _lib.load()
+        self.device = cameras.device
+        dev = self.device
+        self.precision = precision
+        self.nc = int(cameras.shape[0])
+        self.np = int(points.shape[0])
+        self.no = int(observations.shape[0])
+        if cameras.shape[1:] != (9,) or points.shape[1:] != (3,) or observations.shape[1:] != (2,):
+            raise ValueError("expected cameras [nc,9], points [np,3], observations [no,2]")
+        if camera_index.numel() != self.no or point_index.numel() != self.no:
+            raise ValueError("camera_index and point_index need one entry per observation")
+        if self.no:
+            cmin, cmax = int(camera_index.min()), int(camera_index.max())
+            pmin, pmax = int(point_index.min()), int(point_index.max())
+            if cmin < 0 or cmax >= self.nc or pmin < 0 or pmax >= self.np:
+                raise ValueError("camera_index / point_index out of range")
+        if not torch.isfinite(observations).all():
+            raise ValueError("observations must be finite")
+        self.layout = layout or build_layout(camera_index.to(dev), point_index.to(dev), observations.to(dev),
+                                             self.nc, self.np)
+        L = self.layout
+        self.np_pad = 32 * L.num_slices
+        T = torch.float32 if precision == "mixed" else torch.float64
+        self.T = T
+        f64 = dict(dtype=torch.float64, device=dev)
+        cc = torch.zeros(self.nc, dtype=torch.uint8, device=dev)
+        if camera_constant is not None:
+            cc = camera_constant.to(dev).to(torch.uint8).contiguous()
+        pc = torch.ones(max(self.np_pad, 1), dtype=torch.uint8, device=dev)
+        if self.np:
+            src = torch.zeros(self.np, dtype=torch.uint8, device=dev) if point_constant is None else \
+                point_constant.to(dev).to(torch.uint8)
+            pc[:self.np] = src[L.point_order]
+        self.cam_const = cc
+        self.pt_const = pc
+        nslot = max(L.num_slots, 1)
+        npq = max(self.np_pad, 1)
+        ncq = max(self.nc, 1)
+        self.cameras = torch.zeros((ncq, 9), **f64)
+        self.cand_cameras = torch.zeros((ncq, 9), **f64)
+        self.best_cameras = torch.zeros((ncq, 9), **f64)
+        self.points = torch.zeros((npq, 3), **f64)
+        self.cand_points = torch.zeros((npq, 3), **f64)
+        self.best_points = torch.zeros((npq, 3), **f64)
+        self.jac = torch.zeros((nslot, 24), dtype=T, device=dev)
+        self.res = torch.zeros((nslot, 2), **f64)
+        self.winv = torch.zeros((npq, 6), dtype=T, device=dev)
+        self.winv_ga = torch.zeros((npq, 3), **f64)
+        self.step_points = torch.zeros((npq, 3), **f64)
+        self.cam_diag = torch.zeros((ncq, 9), **f64)
+        self.precond = torch.zeros((ncq, 81), dtype=T, device=dev)
+        self.rhs = torch.zeros((ncq, 9), **f64)
+        self.step_cameras = torch.zeros((ncq, 9), **f64)
+        self.pcg = {k: torch.zeros(9 * ncq, dtype=T, device=dev) for k in ("x", "r", "z", "ap")}
+        self.pcg["p"] = torch.zeros(2 * 9 * ncq, dtype=T, device=dev)
+        self.ctl = torch.zeros(_lib.CTL_BYTES, dtype=torch.uint8, device=dev)
+        self.ctl_host = torch.zeros(_lib.CTL_BYTES, dtype=torch.uint8, pin_memory=True)
+        self.dense_work: torch.Tensor | None = None
+        self.struct = _lib.BAStruct()
+        s = self.struct
+        s.num_cameras, s.num_observations, s.num_points = self.nc, self.no, self.np_pad
+        s.num_slices, s.num_slots, s.max_slice_len = L.num_slices, L.num_slots, L.max_slice_len
+        s.precision = _lib.FP32 if precision == "mixed" else _lib.FP64
+        s.has_duplicate_cameras = int(L.has_duplicate_cameras)
+        for k, v in device_loss(loss).items():
+            setattr(s, k, v)
+        s.slice_base, s.slice_len = _ptr(L.slice_base), _ptr(L.slice_len)
+        s.slot_cam, s.slot_obs = _ptr(L.slot_cam), _ptr(L.slot_obs)
+        s.cam_offsets, s.cam_entries = _ptr(L.cam_offsets), _ptr(L.cam_entries)
+        s.cam_const, s.pt_const = _ptr(self.cam_const), _ptr(self.pt_const)
+        s.jac, s.res = _ptr(self.jac), _ptr(self.res)
+        s.winv, s.winv_ga, s.step_points = _ptr(self.winv), _ptr(self.winv_ga), _ptr(self.step_points)
+        s.cam_diag, s.precond, s.rhs, s.step_cameras = (_ptr(self.cam_diag), _ptr(self.precond), _ptr(self.rhs),
+                                                        _ptr(self.step_cameras))
+        s.pcg_x, s.pcg_r, s.pcg_z = _ptr(self.pcg["x"]), _ptr(self.pcg["r"]), _ptr(self.pcg["z"])
+        s.pcg_p, s.pcg_ap = _ptr(self.pcg["p"]), _ptr(self.pcg["ap"])
+        s.counters = self.ctl.data_ptr() + _lib.CTL_COUNTERS
+        s.stats = self.ctl.data_ptr()
+        self._bind_params()
+        nbytes = ctypes.c_int64(0)
+        with torch.cuda.device(dev):
+            _lib.check(self.lib.ceres_b200_scratch_bytes(ctypes.byref(s), ctypes.byref(nbytes)), "scratch size")
+        self.scratch = torch.zeros(int(nbytes.value), dtype=torch.uint8, device=dev)
+        s.scratch, s.scratch_bytes = self.scratch.data_ptr(), int(nbytes.value)
+        self.set_parameters(cameras, points)
+
+    # ---------------------------------------------------------------- parameters
+    def _bind_params(self):
+        s = self.struct
+        s.cameras, s.points = _ptr(self.cameras), _ptr(self.points)
+        s.cand_cameras, s.cand_points = _ptr(self.cand_cameras), _ptr(self.cand_points)
+
+    def set_parameters(self, cameras: torch.Tensor, points: torch.Tensor) -> None:
+        if self.nc:
+            self.cameras[: self.nc].copy_(cameras.to(self.device, torch.float64))
+        if self.np:
+            self.points[: self.np].copy_(points.to(self.device, torch.float64)[self.layout.point_order])
+
+    def get_parameters(self, which: str = "current") -> tuple[torch.Tensor, torch.Tensor]:
+        cams = {"current": self.cameras, "candidate": self.cand_cameras, "best": self.best_cameras}[which]
+        pts_q = {"current": self.points, "candidate": self.cand_points, "best": self.best_points}[which]
+        pts = torch.empty((self.np, 3), dtype=torch.float64, device=self.device)
+        if self.np:
+            pts[self.layout.point_order] = pts_q[: self.np]
+        return cams[: self.nc].clone(), pts
+
+    def accept(self) -> None:
+        """The candidate becomes the current state (pointer swap)."""
+        self.cameras, self.cand_cameras = self.cand_cameras, self.cameras
+        self.points, self.cand_points = self.cand_points, self.points
+        self._bind_params()
+
+    def save_best(self) -> None:
+        self.best_cameras.copy_(self.cameras)
+        self.best_points.copy_(self.points)
+
+    def restore_best(self) -> None:
+        self.cameras.copy_(self.best_cameras)
+        self.points.copy_(self.best_points)
+
+    # ---------------------------------------------------------------- kernels
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _call(self, name: str, *args) -> None:
+        fn = getattr(self.lib, name)
+        with torch.cuda.device(self.device):
+            _lib.check(fn(ctypes.byref(self.struct), *args, self._stream()), name)
+
+    def evaluate(self, with_jacobian: bool = True) -> None:
+        self._call("ceres_b200_ba_evaluate", int(with_jacobian))
+
+    def assemble(self, radius: float, options: SolverOptions, precond: int) -> None:
+        self._call("ceres_b200_ba_point_assemble", float(radius), float(options.min_lm_diagonal),
+                   float(options.max_lm_diagonal), int(options.jacobi_scaling))
+        self._call("ceres_b200_ba_camera_assemble", float(radius), float(options.min_lm_diagonal),
+                   float(options.max_lm_diagonal), int(options.jacobi_scaling), int(precond))
+
+    def pcg(self, precond: int, min_iterations: int, max_iterations: int, tolerance: float,
+            max_refinements: int = 0) -> None:
+        self._call("ceres_b200_ba_pcg", int(precond), int(min_iterations), int(max_iterations), float(tolerance),
+                   int(max_refinements))
+
+    def dense_solve(self) -> None:
+        if self.nc == 0:
+            return
+        if self.dense_work is None:
+            nbytes = ctypes.c_int64(0)
+            _lib.check(self.lib.ceres_b200_dense_schur_bytes(ctypes.byref(self.struct), ctypes.byref(nbytes)),
+                       "dense work size")
+            self.dense_work = torch.empty(max(int(nbytes.value) // 8, 1), dtype=torch.float64, device=self.device)
+        self._call("ceres_b200_ba_dense_schur_solve", self.dense_work.data_ptr())
+
+    def schur_matvec(self, x: torch.Tensor) -> torch.Tensor:
+        x = x.to(self.device, torch.float64).contiguous()
+        y = torch.zeros(9 * self.nc, dtype=torch.float64, device=self.device)
+        self._call("ceres_b200_ba_schur_matvec", x.data_ptr(), y.data_ptr())
+        return y
+
+    def step(self) -> None:
+        self._call("ceres_b200_ba_step")
+
+    def read_stats(self) -> np.ndarray:
+        self.ctl_host.copy_(self.ctl, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        raw = self.ctl_host.numpy()
+        stats = np.frombuffer(raw, dtype=np.float64, count=_lib.NSTATS).copy()
+        err = int(stats[_lib.STAT_ERROR])
+        if err & _lib.DEVERR_LOSS:
+            raise ValueError("Loss function has rho'' > 0 but rho' <= 0")
+        if err & _lib.DEVERR_BARRIER:
+            raise _lib.NativeLibraryError("a grid barrier of the cooperative PCG timed out")
+        if err & _lib.DEVERR_NOT_PD:
+            raise _lib.NativeLibraryError("the reduced camera matrix is not positive definite")
+        return stats
+
+    # ---------------------------------------------------------------- views for tests
+    def slot_view(self):
+        """(residuals [no,2], Jc [no,2,9], Jp [no,2,3]) in input observation order."""
+        slots = self.layout.slot_of_obs
+        r = self.res[slots]
+        J = self.jac[slots].to(torch.float64)
+        return r, J[:, :18].reshape(-1, 2, 9), J[:, 18:].reshape(-1, 2, 3)
+
+
+# ======================================================================================
+# Levenberg-Marquardt (solver.py:35-357 for the LM strategy)
+# ======================================================================================
+class _StepEvaluator:
+    """solver.py:823-861: relative and historical step quality."""
+
+    def __init__(self, initial_cost: float, max_nonmonotonic: int):
+        self.max_nonmonotonic = max(0, int(max_nonmonotonic))
+        self.minimum_cost = self.current_cost = self.reference_cost = self.candidate_cost = initial_cost
+        self.acc_reference = 0.0
+        self.acc_candidate = 0.0
+        self.nonmonotonic = 0
+
+    def step_quality(self, cost: float, model_change: float) -> float:
+        if model_change <= 0.0:
+            return float("-inf")
+        relative = (self.current_cost - cost) / model_change
+        historical = (self.reference_cost - cost) / (self.acc_reference + model_change)
+        return max(relative, historical)
+
+    def step_accepted(self, cost: float, model_change: float) -> None:
+        self.current_cost = cost
+        self.acc_candidate += model_change
+        self.acc_reference += model_change
+        if cost < self.minimum_cost:
+            self.minimum_cost = cost
+            self.nonmonotonic = 0
+            self.candidate_cost = cost
+            self.acc_candidate = 0.0
+        else:
+            self.nonmonotonic += 1
+            if cost > self.candidate_cost:
+                self.candidate_cost = cost
+                self.acc_candidate = 0.0
+        if self.nonmonotonic == self.max_nonmonotonic:
+            self.reference_cost = self.candidate_cost
+            self.acc_reference = self.acc_candidate
+
+
+class _LMRadius:
+    """solver.py:805-820."""
+
+    def __init__(self, radius: float, max_radius: float):
+        self.radius = radius
+        self.max_radius = max_radius
+        self.decrease_factor = 2.0
+
+    def accepted(self, quality: float) -> float:
+        self.radius = min(self.max_radius, self.radius / max(1.0 / 3.0, 1.0 - (2.0 * quality - 1.0) ** 3))
+        self.decrease_factor = 2.0
+        return self.radius
+
+    def rejected(self) -> float:
+        self.radius = self.radius / self.decrease_factor
+        self.decrease_factor *= 2.0
+        return self.radius
+
+
+@dataclass
+class LMResult:
+    summary: SolverSummary
+    time_to_tolerance: float | None = None
+
+
+def _log(options: SolverOptions, it: IterationSummary) -> None:
+    if not options.minimizer_progress_to_stdout or options.logging_type is LoggingType.SILENT:
+        return
+    print(f"{it.iteration:4d}: f:{it.cost: .6e} d:{it.cost_change: .3e} g:{it.gradient_max_norm: .3e} "
+          f"h:{it.step_norm: .3e} rho:{it.relative_decrease: .3e} mu:{it.trust_region_radius: .3e}")
+
+
+def linear_solver_kind(options: SolverOptions) -> str:
+    lst = options.linear_solver_type
+    if lst in (LinearSolverType.DENSE_SCHUR, LinearSolverType.SPARSE_SCHUR):
+        return "dense"
+    if lst is LinearSolverType.ITERATIVE_SCHUR:
+        if options.preconditioner_type not in _PRECOND:
+            raise NotImplementedError(
+                f"ITERATIVE_SCHUR with {options.preconditioner_type.value} is not implemented on the GPU path "
+                "(IDENTITY, JACOBI and SCHUR_JACOBI are)")
+        if options.use_spse_initialization:
+            raise NotImplementedError("use_spse_initialization is not implemented on the GPU path")
+        return "iterative"
+    raise NotImplementedError(f"{lst.value} is not a Schur solver; the GPU path implements DENSE_SCHUR, "
+                              "SPARSE_SCHUR and ITERATIVE_SCHUR")
+
+
+def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, start: float,
+           num_active_columns: int, max_refinements: int = 1, target_cost: float | None = None,
+           on_state=None) -> LMResult:
+    """The trust-region loop. ``summary`` arrives with the preprocessing fields set.
+
+    ``target_cost``: when given, the wall time at which the best cost first
+    drops to or below it is returned as ``time_to_tolerance``.
+    ``on_state(engine, which)``: copies device parameters to the caller's
+    tensors (used for callbacks that look at the parameters).
+    """
+    kind = linear_solver_kind(options)
+    precond = _PRECOND.get(options.preconditioner_type, _lib.PRECOND_SCHUR_JACOBI)
+    refinements = max_refinements if engine.precision == "mixed" else 0
+    lm = _LMRadius(options.initial_trust_region_radius, options.max_trust_region_radius)
+    radius = lm.radius
+    consecutive_invalid = 0
+    previous_cost: float | None = None
+    minimizer_start = time.perf_counter()
+    ttt: float | None = None
+
+    t0 = time.perf_counter()
+    engine.evaluate(True)
+    engine.assemble(radius, options, precond)
+    st = engine.read_stats()
+    eval_time = time.perf_counter() - t0
+    summary.jacobian_evaluation_time_in_seconds += eval_time
+    cost = float(st[_lib.STAT_COST])
+    gmax = max(st[_lib.STAT_GMAX_P], st[_lib.STAT_GMAX_C])
+    gnorm = math.sqrt(st[_lib.STAT_GSQ_P] + st[_lib.STAT_GSQ_C])
+    summary.initial_cost = cost
+    summary.final_cost = cost
+    best_cost = cost
+    engine.save_best()
+    best_is_current = True
+    if target_cost is not None and best_cost <= target_cost:
+        ttt = time.perf_counter() - start
+    evaluator = _StepEvaluator(cost, options.max_consecutive_nonmonotonic_steps if options.use_nonmonotonic_steps else 0)
+    need_assemble = False
+    terminated = False
+
+    def finalize() -> LMResult:
+        if summary.minimizer_time_in_seconds == 0.0:
+            summary.minimizer_time_in_seconds = time.perf_counter() - minimizer_start
+        post = time.perf_counter()
+        if not best_is_current:
+            engine.restore_best()
+        summary.final_cost = best_cost
+        summary.postprocessor_time_in_seconds += time.perf_counter() - post
+        summary.total_time_in_seconds = time.perf_counter() - start
+        return LMResult(summary, ttt)
+
+    if num_active_columns == 0:
+        summary.termination_type = TerminationType.CONVERGENCE
+        summary.message = "No active parameters."
+        return finalize()
+
+    for iteration in range(options.max_num_iterations + 1):
+        it_start = time.perf_counter()
+        jac_time = 0.0
+        if need_assemble:
+            t0 = time.perf_counter()
+            engine.assemble(radius, options, precond)
+            need_assemble = False
+            jac_time = time.perf_counter() - t0
+        summary.num_jacobian_evaluations += 1
+        it = IterationSummary(iteration=iteration, step_is_valid=True, step_is_successful=True, cost=cost,
+                              gradient_norm=gnorm, gradient_max_norm=gmax, trust_region_radius=radius,
+                              eta=options.eta, jacobian_evaluation_time_in_seconds=jac_time)
+        if iteration == 0:
+            it.iteration_time_in_seconds = time.perf_counter() - it_start
+            it.cumulative_time_in_seconds = time.perf_counter() - start
+            summary.iterations.append(it)
+            _log(options, it)
+            if gmax <= options.gradient_tolerance:
+                summary.termination_type = TerminationType.CONVERGENCE
+                summary.message = "Gradient tolerance reached."
+                summary.final_cost = cost
+                terminated = True
+                break
+            if options.max_num_iterations == 0:
+                summary.termination_type = TerminationType.NO_CONVERGENCE
+                summary.message = "Maximum iterations reached."
+                summary.final_cost = cost
+                terminated = True
+                break
+            continue
+
+        lin_start = time.perf_counter()
+        if kind == "dense":
+            engine.dense_solve()
+            lin_iters = 1
+        else:
+            engine.pcg(precond, options.min_linear_solver_iterations, options.max_linear_solver_iterations,
+                       options.eta, refinements)
+        engine.step()
+        st = engine.read_stats()
+        lin_time = time.perf_counter() - lin_start
+        if kind != "dense":
+            lin_iters = int(st[_lib.STAT_PCG_ITERS]) if engine.nc else 1
+        summary.num_linear_solves += 1
+        summary.linear_solver_time_in_seconds += lin_time
+
+        if st[_lib.STAT_NONFINITE] > 0:
+            consecutive_invalid += 1
+            radius = lm.rejected()
+            need_assemble = True
+            it.step_is_valid = False
+            it.step_is_successful = False
+            it.linear_solver_iterations = lin_iters
+            it.linear_solver_time_in_seconds = lin_time
+            it.step_solver_time_in_seconds = lin_time
+            it.trust_region_radius = radius
+            it.iteration_time_in_seconds = time.perf_counter() - it_start
+            it.cumulative_time_in_seconds = time.perf_counter() - start
+            summary.num_unsuccessful_steps += 1
+            if consecutive_invalid >= options.max_num_consecutive_invalid_steps:
+                summary.termination_type = TerminationType.FAILURE
+                summary.message = "Too many invalid trust-region steps."
+                terminated = True
+                break
+            summary.iterations.append(it)
+            _log(options, it)
+            continue
+
+        summary.num_residual_evaluations += 1
+        candidate_cost = float(st[_lib.STAT_CAND_COST])
+        model_decrease = max(float(st[_lib.STAT_MODEL]), 0.0)
+        step_is_valid = model_decrease > 0.0
+        rho = evaluator.step_quality(candidate_cost, model_decrease) if step_is_valid else 0.0
+        accepted = step_is_valid and rho > options.min_relative_decrease
+        step_norm = math.sqrt(st[_lib.STAT_STEP_SQ_P] + st[_lib.STAT_STEP_SQ_C])
+        it.step_norm = step_norm
+        it.cost_change = cost - candidate_cost
+        it.relative_decrease = float(rho)
+        it.step_is_valid = step_is_valid
+        it.linear_solver_iterations = lin_iters
+        it.linear_solver_time_in_seconds = lin_time
+        it.step_solver_time_in_seconds = lin_time
+        it.iteration_time_in_seconds = time.perf_counter() - it_start
+        it.cumulative_time_in_seconds = time.perf_counter() - start
+
+        if accepted:
+            consecutive_invalid = 0
+            summary.num_successful_steps += 1
+            evaluator.step_accepted(candidate_cost, model_decrease)
+            engine.accept()
+            if candidate_cost < best_cost:
+                best_cost = candidate_cost
+                best_is_current = True
+                if options.use_nonmonotonic_steps:
+                    engine.save_best()
+                it.step_is_nonmonotonic = False
+            else:
+                if best_is_current and options.use_nonmonotonic_steps:
+                    pass  # best buffers already hold the best state
+                best_is_current = False
+                it.step_is_nonmonotonic = candidate_cost > best_cost
+            if target_cost is not None and ttt is None and best_cost <= target_cost:
+                ttt = time.perf_counter() - start
+            summary.final_cost = best_cost
+            radius = lm.accepted(rho)
+            it.trust_region_radius = radius
+            it.step_is_successful = True
+        else:
+            summary.num_unsuccessful_steps += 1
+            radius = lm.rejected()
+            it.trust_region_radius = radius
+            it.step_is_successful = False
+            need_assemble = True
+
+        summary.iterations.append(it)
+        _log(options, it)
+        if options.callbacks:
+            if on_state is not None and options.update_state_every_iteration:
+                on_state(engine, "best" if (options.use_nonmonotonic_steps and not best_is_current) else "current")
+            stop = None
+            for callback in options.callbacks:
+                result = callback(it)
+                if result is CallbackReturnType.SOLVER_ABORT:
+                    summary.termination_type = TerminationType.USER_FAILURE
+                    summary.message = "User callback aborted."
+                    stop = True
+                    break
+                if result is CallbackReturnType.SOLVER_TERMINATE_SUCCESSFULLY:
+                    summary.termination_type = TerminationType.USER_SUCCESS
+                    summary.message = "User callback terminated successfully."
+                    stop = True
+                    break
+            if stop:
+                return finalize()
+
+        if accepted:
+            state_norm = math.sqrt(st[_lib.STAT_CAND_STATE_SQ_P] + st[_lib.STAT_CAND_STATE_SQ_C])
+            if step_norm <= options.parameter_tolerance * (state_norm + options.parameter_tolerance):
+                summary.termination_type = TerminationType.CONVERGENCE
+                summary.message = "Parameter tolerance reached."
+                terminated = True
+                break
+            if previous_cost is not None and abs(previous_cost - candidate_cost) <= \
+                    options.function_tolerance * max(previous_cost, 1.0):
+                summary.termination_type = TerminationType.CONVERGENCE
+                summary.message = "Function tolerance reached."
+                terminated = True
+                break
+            previous_cost = candidate_cost
+            t0 = time.perf_counter()
+            engine.evaluate(True)
+            engine.assemble(radius, options, precond)
+            st = engine.read_stats()
+            jt = time.perf_counter() - t0
+            summary.jacobian_evaluation_time_in_seconds += jt
+            summary.num_jacobian_evaluations += 1
+            cost = float(st[_lib.STAT_COST])
+            gmax = max(st[_lib.STAT_GMAX_P], st[_lib.STAT_GMAX_C])
+            gnorm = math.sqrt(st[_lib.STAT_GSQ_P] + st[_lib.STAT_GSQ_C])
+            if gmax <= options.gradient_tolerance:
+                summary.termination_type = TerminationType.CONVERGENCE
+                summary.message = "Gradient tolerance reached."
+                summary.final_cost = cost
+                terminated = True
+                break
+        if radius <= options.min_trust_region_radius:
+            summary.termination_type = TerminationType.CONVERGENCE
+            summary.message = "Minimum trust-region radius reached."
+            terminated = True
+            break
+        if time.perf_counter() - start >= options.max_solver_time_in_seconds:
+            summary.termination_type = TerminationType.NO_CONVERGENCE
+            summary.message = "Maximum solver time reached."
+            terminated = True
+            break
+    if not terminated:
+        summary.termination_type = TerminationType.NO_CONVERGENCE
+        summary.message = "Maximum iterations reached."
+    return finalize()

@@ -1,0 +1,247 @@
+/*
+ * ceres_b200.h - C ABI of the B200 (sm_100a) Schur bundle-adjustment kernels.
+ *
+ * Plain C: raw device pointers, sizes and a cudaStream_t (passed as void*).
+ * Every entry point returns 0 on success or a negative CERES_B200_E* code and
+ * never allocates device memory; the caller owns every buffer named in
+ * ceres_b200_ba_t (the Python host allocates them with torch).
+ *
+ * The reference (ceres-torch) computes this path in Python/PyTorch on a dense
+ * Jacobian; each entry point below names the reference code it replaces
+ * (paths relative to the ceres-torch project root).
+ */
+#ifndef CERES_B200_H
+#define CERES_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CERES_B200_ABI_VERSION 1
+
+/* status codes */
+#define CERES_B200_OK 0
+#define CERES_B200_EINVAL (-1)       /* bad argument (null pointer, size, enum) */
+#define CERES_B200_ECUDA (-2)        /* a CUDA launch/runtime call failed */
+#define CERES_B200_ESMEM (-3)        /* shared memory request above the device limit */
+#define CERES_B200_ECOOP (-4)        /* cooperative launch not possible */
+#define CERES_B200_ETOOBIG (-5)      /* size above a fixed capacity */
+
+/* device-side error bits, OR-ed into stats[CERES_B200_STAT_ERROR] */
+#define CERES_B200_DEVERR_LOSS 1     /* rho'' > 0 but rho' <= 0 (losses.py:177-179) */
+#define CERES_B200_DEVERR_BARRIER 2  /* a grid barrier wait hit its iteration limit */
+#define CERES_B200_DEVERR_NOT_PD 4   /* the dense reduced camera matrix was not positive definite */
+
+/* loss kinds (losses.py:21-133) */
+enum {
+  CERES_B200_LOSS_TRIVIAL = 0,
+  CERES_B200_LOSS_HUBER = 1,
+  CERES_B200_LOSS_SOFTLONE = 2,
+  CERES_B200_LOSS_CAUCHY = 3,
+  CERES_B200_LOSS_ARCTAN = 4,
+  CERES_B200_LOSS_TOLERANT = 5,
+  CERES_B200_LOSS_TUKEY = 6
+};
+
+/* preconditioners for the reduced camera system (types.py:26-33) */
+enum {
+  CERES_B200_PRECOND_IDENTITY = 0,
+  CERES_B200_PRECOND_JACOBI = 1,
+  CERES_B200_PRECOND_SCHUR_JACOBI = 2
+};
+
+/* precision of the Jacobian store, point-block inverses and PCG vectors */
+enum { CERES_B200_FP64 = 0, CERES_B200_FP32 = 1 };
+
+/* indices into the float64 stats vector (length CERES_B200_NSTATS) */
+enum {
+  CERES_B200_STAT_COST = 0,          /* sum_i 0.5 rho(|r_i|^2) at the current parameters */
+  CERES_B200_STAT_GMAX_P = 1,        /* max |J^T r| over point columns */
+  CERES_B200_STAT_GSQ_P = 2,         /* |J^T r|^2 over point columns */
+  CERES_B200_STAT_GMAX_C = 3,        /* max |J^T r| over camera columns */
+  CERES_B200_STAT_GSQ_C = 4,         /* |J^T r|^2 over camera columns */
+  CERES_B200_STAT_CAND_COST = 5,     /* cost at the candidate parameters */
+  CERES_B200_STAT_MODEL = 6,         /* 0.5|r|^2 - 0.5|r + J step|^2 (not clamped) */
+  CERES_B200_STAT_STEP_SQ_P = 7,     /* |step|^2 over point columns */
+  CERES_B200_STAT_STEP_SQ_C = 8,     /* |step|^2 over camera columns */
+  CERES_B200_STAT_NONFINITE = 9,     /* count of non-finite step entries */
+  CERES_B200_STAT_PCG_ITERS = 10,    /* PCG iterations of the last solve */
+  CERES_B200_STAT_PCG_SUCCESS = 11,  /* 1 if the PCG met its tolerance */
+  CERES_B200_STAT_PCG_RNORM = 12,    /* |r| at PCG exit */
+  CERES_B200_STAT_ERROR = 13,        /* OR of CERES_B200_DEVERR_* bits */
+  CERES_B200_STAT_RHS_NORM = 14,     /* |rhs| of the reduced camera system */
+  CERES_B200_STAT_REFINE_RNORM = 15, /* float64 residual |rhs - S x| after refinement */
+  CERES_B200_STAT_CAND_STATE_SQ_P = 16, /* |candidate points|^2 (all point blocks) */
+  CERES_B200_STAT_CAND_STATE_SQ_C = 17, /* |candidate cameras|^2 (all camera blocks) */
+  CERES_B200_NSTATS = 18
+};
+
+/*
+ * Device-resident state of one bundle-adjustment problem.
+ *
+ * Observations live in a sliced-ELL "point-major" store: points are sorted by
+ * track length (descending, stable in point id) and cut into slices of 32;
+ * lane l of slice s owns point q = 32 s + l (q is the "sorted point" index);
+ * observation k of that point sits in slot slice_base[s] + 32 k + l.
+ * Padding slots carry slot_cam = -1. A camera-major list (cam_offsets /
+ * cam_entries) names, for each camera, the (slot, q) pairs of its
+ * observations in increasing slot order.
+ *
+ * Jacobian records are 24 scalars per slot (camera row 0 [9], camera row 1
+ * [9], point row 0 [3], point row 1 [3]) of float (FP32) or double (FP64).
+ */
+typedef struct ceres_b200_ba_t {
+  int32_t num_cameras;
+  int32_t num_observations;  /* real observations (entries of the camera-major list) */
+  int32_t num_points;        /* sorted point slots = 32 * num_slices (padded) */
+  int32_t num_slices;
+  int32_t num_slots;         /* sum over slices of 32 * slice_len */
+  int32_t max_slice_len;
+  int32_t precision;         /* CERES_B200_FP64 / CERES_B200_FP32 */
+  int32_t has_duplicate_cameras; /* 1 if some point sees one camera twice */
+  int32_t loss_kind;         /* CERES_B200_LOSS_* */
+  double loss_a, loss_b;     /* loss parameters (a; b only for Tolerant) */
+  double loss_scale;         /* ScaledLoss factor (1 when unscaled) */
+  int32_t inner_loss_kind;   /* ComposedLoss inner kind, -1 when not composed */
+  int32_t pad0;
+  double inner_a, inner_b;
+  double inner_scale;        /* ScaledLoss factor of the inner loss (1 when unscaled) */
+
+  /* structure (read-only) */
+  const int32_t* slice_base;   /* [num_slices] first slot of the slice (multiple of 32) */
+  const int32_t* slice_len;    /* [num_slices] observations per lane (max over lanes) */
+  const int32_t* slot_cam;     /* [num_slots] camera of the slot, -1 padding */
+  const double* slot_obs;      /* [num_slots][2] observed pixel */
+  const int32_t* cam_offsets;  /* [num_cameras + 1] */
+  const int32_t* cam_entries;  /* [num_observations][2] (slot, q) grouped by camera */
+  const uint8_t* cam_const;    /* [num_cameras] 1 = constant camera block */
+  const uint8_t* pt_const;     /* [num_points] 1 = constant point or padding lane */
+
+  /* parameters (float64 master copies) */
+  double* cameras;             /* [num_cameras][9] current */
+  double* points;              /* [num_points][3] current (sorted-point order) */
+  double* cand_cameras;        /* [num_cameras][9] candidate = current + step */
+  double* cand_points;         /* [num_points][3] */
+
+  /* per-slot evaluation */
+  void* jac;                   /* [num_slots][24] float or double */
+  double* res;                 /* [num_slots][2] corrected residuals */
+
+  /* point-side Schur pieces */
+  void* winv;                  /* [num_points][6] (W + D_p)^-1, symmetric, float or double */
+  double* winv_ga;             /* [num_points][3] W^-1 g_a with g_a = -J_p^T r */
+  double* step_points;         /* [num_points][3] */
+
+  /* camera-side Schur pieces */
+  double* cam_diag;            /* [num_cameras][9] damping D_c added to the diagonal */
+  void* precond;               /* [num_cameras][81] preconditioner inverse blocks, float or double */
+  double* rhs;                 /* [num_cameras][9] reduced right-hand side */
+  double* step_cameras;        /* [num_cameras][9] */
+
+  /* PCG vectors, float or double, [num_cameras][9] each */
+  void* pcg_x;
+  void* pcg_r;
+  void* pcg_z;
+  void* pcg_p;                 /* [2][num_cameras][9] double-buffered direction */
+  void* pcg_ap;
+
+  /* scratch owned by the caller */
+  void* scratch;               /* per-CTA partial sums; see ceres_b200_scratch_bytes */
+  int64_t scratch_bytes;
+  uint32_t* counters;          /* [16] zero-initialised once; kernels leave them zero */
+  double* stats;               /* [CERES_B200_NSTATS] */
+} ceres_b200_ba_t;
+
+/* ABI version of the loaded library (CERES_B200_ABI_VERSION). */
+int ceres_b200_abi_version(void);
+
+/* Bytes of scratch the PCG and reductions need for this problem on this device. */
+int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out);
+
+/*
+ * Residuals, Jacobian and robust correction at ba->cameras / ba->points.
+ * Writes ba->res, ba->jac (when with_jacobian) and stats[COST].
+ * Replaces Problem.evaluate (problem.py:377-413, :486-520), the autodiff
+ * Jacobian of the Snavely residual (costs.py:31-44 over
+ * examples/simple_bundle_adjuster.py:73-79, rotation.py:104-110, :211-222)
+ * and the Ceres corrector (losses.py:158-193).
+ */
+int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* stream);
+
+/*
+ * Point side of the Schur system for a trust-region radius: Jacobi damping
+ * D_p (linear.py:539-551), W_p = J_p^T J_p + D_p inverted per point
+ * (linear.py:808 on the block-diagonal Haa), W^-1 g_a, and the point
+ * gradient stats. Replaces the Haa part of linear.py:794-839.
+ */
+int ceres_b200_ba_point_assemble(const ceres_b200_ba_t* ba, double radius, double min_diagonal,
+                                 double max_diagonal, int jacobi_scaling, void* stream);
+
+/*
+ * Camera side: damping D_c, reduced rhs = g_b - H_ba W^-1 g_a, camera
+ * gradient stats and the preconditioner blocks of S (SCHUR_JACOBI: inverse
+ * of each 9x9 diagonal block of S, Cholesky with an LU fallback as in
+ * linear.py:1156-1182; JACOBI: 1/max(diag S, eps), linear.py:530).
+ * Replaces the Hbb / rhs part of linear.py:794-839 and linear.py:462-536.
+ */
+int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, double min_diagonal,
+                                  double max_diagonal, int jacobi_scaling, int preconditioner,
+                                  void* stream);
+
+/*
+ * Preconditioned conjugate gradients on S x = rhs with the implicit Schur
+ * product S p = (U + D_c) p - H_ba W^-1 H_ab p streamed from the Jacobian
+ * store, in one cooperative persistent launch (x0 = 0; stop when
+ * |r| <= tolerance * max(|rhs|, eps) after min_iterations).
+ * Writes ba->step_cameras and stats[PCG_*]. With FP32 precision and
+ * max_refinements > 0, float64 refinement passes recompute rhs - S x with
+ * float64 accumulation and solve for a correction.
+ * Replaces linear.py:702-776 and the PCG of linear.py:1216-1256.
+ */
+int ceres_b200_ba_pcg(const ceres_b200_ba_t* ba, int preconditioner, int min_iterations,
+                      int max_iterations, double tolerance, int max_refinements, void* stream);
+
+/*
+ * y = S x for a camera vector x (float64 in and out, accumulated in float64
+ * from the stored Jacobian). Replaces the S @ p of linear.py:1237.
+ */
+int ceres_b200_ba_schur_matvec(const ceres_b200_ba_t* ba, const double* x, double* y, void* stream);
+
+/*
+ * Back-substitution of the point step (linear.py:766), candidate parameters
+ * x + step (problem.py:462-474, manifolds.py:81-82), the model decrease
+ * 0.5|r|^2 - 0.5|r + J step|^2 (solver.py:798-802) and the candidate cost
+ * (solver.py:216), in one pass over the observations.
+ */
+int ceres_b200_ba_step(const ceres_b200_ba_t* ba, void* stream);
+
+/*
+ * Exact solve of the reduced camera system: assembles the explicit float64
+ * S = H_bb - H_ba H_aa^-1 H_ab (+ D_c) into work (ceres_b200_dense_schur_bytes
+ * bytes) and solves S x = rhs by Cholesky (one CTA in shared memory up to
+ * 17 cameras, a cooperative global-memory factorisation above that). Writes
+ * ba->step_cameras. Replaces schur_solve_dense (linear.py:667-699), which the
+ * reference reaches for DENSE_SCHUR and, via solver.py:791-792, SPARSE_SCHUR,
+ * and the dense block-Schur split of native/cuda/ceres_torch_cuda_kernel.cu:107-132.
+ */
+int ceres_b200_dense_schur_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out);
+int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, void* stream);
+
+/*
+ * Cholesky solve of a dense symmetric positive definite float64 system
+ * H x = rhs (H [n][n] row-major, overwritten by its factor). flags points to
+ * four zero-initialised uint32 words (three for the grid barrier, one for
+ * CERES_B200_DEVERR_NOT_PD). Used by the dense-A registry backends after
+ * H = A^T A + diag(d) is formed; replaces the at::linalg_solve calls of
+ * native/cuda/ceres_torch_cuda_kernel.cu:93-105.
+ */
+int ceres_b200_dense_cholesky_solve(double* H, const double* rhs, double* x, int64_t n, uint32_t* flags,
+                                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CERES_B200_H */
