@@ -1,0 +1,385 @@
+"""Benchmark: bundle-adjustment LM time-to-tolerance on the 6M-observation ring problem.
+
+Workload (default): configuration 2 of the benchmark set - 1,500 cameras on a
+ring of radius 10, 1,000,000 points in [-3,3]^3, track length Geometric(0.2)+2
+capped at 100 (about 6.0M observations), Cauchy loss (scale 2 px),
+ITERATIVE_SCHUR + SCHUR_JACOBI, seeded synthetic data.
+
+A step is one complete LM solve from the same initial state. The metric is the
+wall time from ``solve`` entry until the running best cost is within 1e-6
+relative of the float64 GPU solve's final cost (the float64 path is checked
+against the CPU oracle at smaller sizes by the test-suite). ``value`` is the
+median over the timed steps of the mixed-precision path with inputs resident in
+HBM; ``e2e`` repeats it through the public API from pinned host buffers (H2D
+of the inputs and D2H of the solution inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs are independent replicas (one problem per rank, weak scaling);
+the reported time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BA LM time-to-tol (5M obs), mixed vs FP64 on GPU; served-solve p50/p99 ms"
+UNIT = "s"
+REL_TOL = 1e-6
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples: list[tuple[float, float, str]] = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return self
+
+        def reader():
+            for line in self.proc.stdout:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 7:
+                    try:
+                        self.samples.append((float(parts[0]), float(parts[1]), ",".join(parts[2:])))
+                    except ValueError:
+                        pass
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        return self
+
+    def stop(self) -> dict:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [s[0] for s in self.samples]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, flags in self.samples:
+            vals = flags.split(",")
+            for name, v in zip(names, vals[1:]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(args):
+    from ceres_torch_cuda_b200 import synthetic as S
+
+    if args.config == 2:
+        return S.ba_config(2, scale=args.scale)
+    if args.config == 1:
+        return S.ba_config(1, scale=args.scale)
+    return S.ba_config(0, scale=args.scale)
+
+
+def solver_options(tc, data):
+    lst = tc.LinearSolverType.DENSE_SCHUR if data.description.startswith("config0") else \
+        tc.LinearSolverType.ITERATIVE_SCHUR
+    return tc.SolverOptions(linear_solver_type=lst, preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI,
+                            max_num_iterations=50)
+
+
+def loss_of(tc, data):
+    kind = data.loss[0]
+    if kind == "cauchy":
+        return tc.CauchyLoss(float(data.loss[1]))
+    if kind == "huber":
+        return tc.HuberLoss(float(data.loss[1]))
+    return None
+
+
+# --------------------------------------------------------------------------------------
+# CPU baseline: the float64 numpy oracle (a restatement of the reference algorithm)
+# --------------------------------------------------------------------------------------
+def cpu_sample(full_obs: int, small: bool = False) -> dict:
+    from ceres_torch_cuda_b200 import synthetic as S
+    from oracle import ba_oracle as O
+
+    nc, npts = (30, 1000) if small else (150, 10000)
+    d = S.make_ring_ba(nc, npts, seed=102, loss=("cauchy", 2.0))
+    p = O.OracleProblem(d.cameras, d.points, d.observations, d.camera_index, d.point_index, d.loss)
+    t0 = time.perf_counter()
+    r = O.solve(p, O.OracleOptions(linear_solver_type="ITERATIVE_SCHUR", preconditioner_type="SCHUR_JACOBI",
+                                   explicit_schur_limit=0))
+    dt = time.perf_counter() - t0
+    scale = full_obs / d.num_observations
+    return {"seconds": dt, "value": dt * scale, "obs": d.num_observations, "iterations": len(r.iterations),
+            "sample": (f"float64 numpy oracle, full LM solve of a ring BA with {nc} cameras / {npts} points / "
+                       f"{d.num_observations} observations (Cauchy 2, ITERATIVE_SCHUR + SCHUR_JACOBI), "
+                       f"{dt:.1f} s scaled by the observation ratio x{scale:.1f}")}
+
+
+def run_reference(args):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    data = make_workload(args)
+    full_obs = data.num_observations
+    for _ in range(args.warmup):
+        cpu_sample(full_obs, small=True)
+    vals, samples = [], []
+    for _ in range(args.steps):
+        s = cpu_sample(full_obs)
+        vals.append(s["value"])
+        samples.append(s)
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median(s["seconds"] for s in samples),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": data.description, "observations": full_obs, "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": samples[-1]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import ceres_torch_cuda_b200 as tc
+    from ceres_torch_cuda_b200 import _lib
+
+    world, rank, local = _dist()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", world_size=world, rank=rank,
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+    data = make_workload(args)
+    loss = loss_of(tc, data)
+    opts = solver_options(tc, data)
+    h = {
+        "cameras": torch.from_numpy(data.cameras).pin_memory(),
+        "points": torch.from_numpy(data.points).pin_memory(),
+        "observations": torch.from_numpy(data.observations).pin_memory(),
+        "camera_index": torch.from_numpy(data.camera_index).pin_memory(),
+        "point_index": torch.from_numpy(data.point_index).pin_memory(),
+    }
+    d0 = {k: v.to(dev) for k, v in h.items()}
+
+    def problem_from_device():
+        return tc.BundleAdjustmentProblem(d0["cameras"].clone(), d0["points"].clone(), d0["observations"],
+                                          d0["camera_index"], d0["point_index"], loss=loss)
+
+    # float64 GPU solve: the target cost and the FP64 time-to-solution
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s64 = tc.solve(opts, problem_from_device(), precision="fp64")
+    torch.cuda.synchronize()
+    fp64_seconds = time.perf_counter() - t0
+    target = s64.final_cost * (1.0 + REL_TOL)
+    s64b = tc.solve(opts, problem_from_device(), precision="fp64", target_cost=target)
+    fp64_ttt = s64b.time_to_tolerance_in_seconds
+
+    for _ in range(args.warmup):
+        tc.solve(opts, problem_from_device(), precision="mixed", target_cost=target)
+
+    sampler = ClockSampler(local).start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.ceres_b200_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ttts, summaries = [], []
+    for _ in range(args.steps):
+        s = tc.solve(opts, problem_from_device(), precision="mixed", target_cost=target)
+        ttts.append(s.time_to_tolerance_in_seconds if s.time_to_tolerance_in_seconds is not None else float("inf"))
+        summaries.append(s)
+    ev1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = int(lib.ceres_b200_launch_count() - launches0)
+    ms_total = ev0.elapsed_time(ev1)
+    ttt_med = statistics.median(ttts)
+
+    # profile pass: per-kernel CUDA-event times on one more solve (same stream)
+    prob = problem_from_device()
+    s_prof, eng = tc.solve(opts, prob, precision="mixed", target_cost=target, return_engine=True)
+    prof = profile_kernels(tc, eng, opts)
+
+    # e2e through the public API from pinned host buffers
+    e2e_vals = []
+    bytes_in = sum(v.numel() * v.element_size() for v in h.values())
+    bytes_out = data.cameras.nbytes + data.points.nbytes
+    out_c = torch.empty_like(h["cameras"]).pin_memory()
+    out_p = torch.empty_like(h["points"]).pin_memory()
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dd = {k: v.to(dev, non_blocking=True) for k, v in h.items()}
+        pe = tc.BundleAdjustmentProblem(dd["cameras"], dd["points"], dd["observations"], dd["camera_index"],
+                                        dd["point_index"], loss=loss)
+        se = tc.solve(opts, pe, precision="mixed", target_cost=target)
+        out_c.copy_(pe.cameras, non_blocking=True)
+        out_p.copy_(pe.points, non_blocking=True)
+        torch.cuda.synchronize()
+        total = time.perf_counter() - t0
+        # time-to-tolerance through the API: transfer + the solve's own time-to-tolerance + result copy
+        e2e_vals.append(total - (se.total_time_in_seconds - (se.time_to_tolerance_in_seconds or se.total_time_in_seconds)))
+    e2e = statistics.median(e2e_vals)
+
+    value = ttt_med
+    if world > 1:
+        t = torch.tensor([value, e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        value, e2e = float(t[0]), float(t[1])
+
+    if rank == 0:
+        cpu = cpu_sample(data.num_observations) if not args.no_cpu_baseline else None
+        peaks = {}
+        pk = ROOT / "MEASURED_PEAKS.json"
+        if pk.exists():
+            peaks = json.loads(pk.read_text())
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        pcg = prof["pcg"]
+        achieved = pcg["bytes_per_launch"] / (pcg["ms_per_launch"] * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / max(args.steps, 1), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32+f64", "data": "synthetic",
+            "config": {"workload": data.description, "cameras": data.num_cameras, "points": data.num_points,
+                       "observations": data.num_observations, "precision": "mixed",
+                       "solver": "ITERATIVE_SCHUR+SCHUR_JACOBI", "l2": "inputs larger than L2 (Jacobian store "
+                       f"{prof['jac_bytes'] / 1e6:.0f} MB)", "parallelism": f"replicas x{world}"},
+            "fp64": {"time_to_tol_s": fp64_ttt, "solve_s": fp64_seconds, "final_cost": s64.final_cost,
+                     "iterations": len(s64.iterations)},
+            "mixed": {"final_cost": summaries[-1].final_cost, "iterations": len(summaries[-1].iterations),
+                      "rel_err_vs_fp64": abs(summaries[-1].final_cost - s64.final_cost) / s64.final_cost,
+                      "solve_s": statistics.median(s.total_time_in_seconds for s in summaries),
+                      "speedup_vs_fp64_ttt": (fp64_ttt / value) if fp64_ttt else None},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "kernel": "k_pcg (implicit-Schur PCG, per launch)",
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"},
+            "kernels": prof["table"],
+            "cpu_baseline": None if cpu is None else {"value": cpu["value"], "unit": UNIT, "cores": 1, "kind": "port",
+                                                      "sample": cpu["sample"]},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in), "d2h_bytes_per_step": int(bytes_out)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def profile_kernels(tc, eng, opts) -> dict:
+    """CUDA-event times of each kernel group on the engine's stream, at the solved
+    state, with algorithmic bytes per launch (FP32 Jacobian store)."""
+    import torch
+
+    from ceres_torch_cuda_b200 import _lib
+
+    no = eng.no
+    slots = eng.layout.num_slots
+    npq = eng.np_pad
+    nc = eng.nc
+    jb = 4 if eng.precision == "mixed" else 8
+    rec = 24 * jb
+    radius = 1e4
+    reps = 5
+
+    def timed(fn):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    t_eval = timed(lambda: eng.evaluate(True))
+    t_point = timed(lambda: eng._call("ceres_b200_ba_point_assemble", radius, 1e-6, 1e32, 1))
+    t_cam = timed(lambda: eng._call("ceres_b200_ba_camera_assemble", radius, 1e-6, 1e32, 1, 2))
+    iters = 20
+    t_pcg = timed(lambda: eng.pcg(2, iters, iters, 0.0, 0))
+    st = eng.read_stats()
+    iters_done = int(st[_lib.STAT_PCG_ITERS])
+    t_step = timed(lambda: eng.step())
+    # algorithmic bytes (compulsory traffic) per launch
+    b_eval = no * (16 + 4 + 16 + rec) + slots * 4 + npq * 24 + nc * 72
+    b_point = no * (6 * jb + 16) + slots * 4 + npq * (6 * jb + 24)
+    b_cam = no * (rec + 16 + 8 + 6 * jb + 24) + nc * (81 * jb + 27 * 8)
+    b_pcg = iters_done * (no * rec + slots * 4 + npq * 6 * jb)
+    b_step = no * (rec + 16 + 16) + slots * 4 + npq * (6 * jb + 24 + 24 * 3)
+    table = {}
+    for name, ms, b in (("evaluate", t_eval, b_eval), ("point_assemble", t_point, b_point),
+                        ("camera_assemble", t_cam, b_cam), ("pcg", t_pcg, b_pcg), ("step", t_step, b_step)):
+        table[name] = {"ms_per_launch": ms, "bytes_per_launch": b, "gbs": b / (ms * 1e-3) / 1e9}
+    table["pcg"]["iterations_per_launch"] = iters_done
+    table["pcg"]["ms_per_iteration"] = t_pcg / max(iters_done, 1)
+    return {"table": table, "pcg": table["pcg"], "jac_bytes": slots * rec}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2, choices=[0, 1, 2])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

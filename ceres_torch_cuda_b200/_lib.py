@@ -74,6 +74,8 @@ _P = ctypes.POINTER(BAStruct)
 # name -> (restype, argtypes); every symbol include/ceres_b200.h declares
 SIGNATURES = {
     "ceres_b200_abi_version": (c_int32, []),
+    "ceres_b200_ba_struct_bytes": (c_int32, []),
+    "ceres_b200_launch_count": (ctypes.c_uint64, []),
     "ceres_b200_scratch_bytes": (c_int32, [_P, ctypes.POINTER(c_int64)]),
     "ceres_b200_ba_evaluate": (c_int32, [_P, c_int32, c_void_p]),
     "ceres_b200_ba_point_assemble": (c_int32, [_P, c_double, c_double, c_double, c_int32, c_void_p]),
@@ -115,6 +117,8 @@ def load(*, build_if_missing: bool = False) -> ctypes.CDLL:
         fn.argtypes = args
     if lib.ceres_b200_abi_version() != ABI_VERSION:
         raise NativeLibraryError(f"{path} has ABI {lib.ceres_b200_abi_version()}, expected {ABI_VERSION}")
+    if lib.ceres_b200_ba_struct_bytes() != ctypes.sizeof(BAStruct):
+        raise NativeLibraryError("ceres_b200_ba_t layout differs between the library and this binding")
     _LIB = lib
     return lib
 

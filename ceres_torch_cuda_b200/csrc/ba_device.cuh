@@ -558,6 +558,7 @@ struct GridBarrier {
 
 __device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
   __shared__ int ok;
+  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(*gb.generation);
@@ -585,10 +586,15 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
         }
       }
     }
+    __threadfence();
     ok = good;
   }
   __syncthreads();
   return ok != 0;
 }
+
+// Loads of data another CTA wrote in this launch go around L1 (L1 is not
+// coherent across SMs).
+template <typename T> __device__ __forceinline__ T ld_cross(const T* p) { return __ldcg(p); }
 
 }  // namespace cb200

@@ -16,6 +16,10 @@ using namespace cb200;
 
 namespace {
 
+// kernels launched by this library since load (reported by ceres_b200_launch_count)
+unsigned long long g_launches = 0;
+inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+
 // counters[] slots
 constexpr int kCtrEval = 0, kCtrPoint = 1, kCtrCamera = 2, kCtrStep = 3, kCtrCamStep = 4;
 constexpr int kCtrBarCount = 8, kCtrBarGen = 9, kCtrBarFlag = 10, kCtrError = 12;
@@ -321,7 +325,7 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t b
 //   t = sum_k Jp_k^T (Jc_k p_c(k)),  s = W^-1 t,  y_c(k) += Jc_k^T (Jc_k p_c(k) - Jp_k s)
 // The accumulation target y is shared memory (per-CTA partial) or global memory.
 // ======================================================================================
-template <typename T, typename TP, typename A>
+template <typename T, typename TP, typename A, bool kCrossP = false>
 __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int gw,
                                               int nw) {
   const int lane = threadIdx.x & 31;
@@ -342,7 +346,7 @@ __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const T
       A u0 = 0, u1 = 0;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
-        const A pj = (A)pc[j];
+        const A pj = kCrossP ? (A)ld_cross(pc + j) : (A)pc[j];
         u0 += (A)rv[j] * pj;
         u1 += (A)rv[9 + j] * pj;
       }
@@ -365,7 +369,7 @@ __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const T
       A u0 = 0, u1 = 0;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
-        const A pj = (A)pc[j];
+        const A pj = kCrossP ? (A)ld_cross(pc + j) : (A)pc[j];
         u0 += (A)rv[j] * pj;
         u1 += (A)rv[9 + j] * pj;
       }
@@ -478,7 +482,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   }
   if (!grid_sync(gb)) return;
   double rz_old = 0.0, rr = 0.0;
-  for (int g = 0; g < G; ++g) { rz_old += a.part_c[2 * g]; rr += a.part_c[2 * g + 1]; }
+  for (int g = 0; g < G; ++g) { rz_old += ld_cross(a.part_c + 2 * g); rr += ld_cross(a.part_c + 2 * g + 1); }
   // the rhs norm is taken in float64 from the float64 rhs
   double rhs_norm;
   {
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
     if (!grid_sync(gb)) return;
     double t = 0.0;
-    for (int g = 0; g < G; ++g) t += a.part_b[g];
+    for (int g = 0; g < G; ++g) t += ld_cross(a.part_b + g);
     rhs_norm = fmax(sqrt(t), a.eps);
   }
   int iterations = 0;
@@ -504,7 +508,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
       T* Pnew = Pbuf + (size_t)nxt * n;
       if (a.smem_vectors) {
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
-          const T pv = (k == 0) ? Z[j] : (T)((double)Z[j] + beta * (double)Pold[j]);
+          const T pv = (k == 0) ? ld_cross(Z + j) : (T)((double)ld_cross(Z + j) + beta * (double)ld_cross(Pold + j));
           ps[j] = pv;
           ys[j] = (T)0;
           if (j >= j0 && j < j1) Pnew[j] = pv;
@@ -520,7 +524,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
           AP[j] = (T)0;
         }
         if (!grid_sync(gb)) return;
-        matvec_slices<T, T, T>(ba, Pnew, AP, gw, nw);
+        matvec_slices<T, T, T, true>(ba, Pnew, AP, gw, nw);
       }
       cur = nxt;
       if (!grid_sync(gb)) return;
@@ -530,9 +534,9 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
           double y = 0.0;
           if (a.smem_vectors) {
-            for (int g = 0; g < G; ++g) y += (double)part_y[(size_t)g * n + j];
+            for (int g = 0; g < G; ++g) y += (double)ld_cross(part_y + (size_t)g * n + j);
           } else {
-            y = (double)AP[j];
+            y = (double)ld_cross(AP + j);
           }
           const double pj = (double)Pnew[j];
           y += ba.cam_diag[j] * pj;
@@ -544,7 +548,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
       }
       if (!grid_sync(gb)) return;
       double denom = 0.0;
-      for (int g = 0; g < G; ++g) denom += a.part_b[g];
+      for (int g = 0; g < G; ++g) denom += ld_cross(a.part_b + g);
       if (fabs(denom) <= a.eps) {
         success = rnorm <= a.tolerance * rhs_norm;
         break;
@@ -571,7 +575,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
       if (!grid_sync(gb)) return;
       double rz_new = 0.0;
       rr = 0.0;
-      for (int g = 0; g < G; ++g) { rz_new += a.part_c[2 * g]; rr += a.part_c[2 * g + 1]; }
+      for (int g = 0; g < G; ++g) { rz_new += ld_cross(a.part_c + 2 * g); rr += ld_cross(a.part_c + 2 * g + 1); }
       rnorm = sqrt(rr);
       iterations = k + 1;
       if (iterations >= a.min_iterations && rnorm <= a.tolerance * rhs_norm) {
@@ -998,6 +1002,7 @@ int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int 
   if (cudaMemsetAsync(&ba.counters[kCtrBarCount], 0, 3 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
   ceres_b200_ba_t bcopy = ba;
   void* args[] = {&bcopy, &a};
+  count_launch();
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg<T>, dim3(L.grid), dim3(kPcgBlock), args,
                                                     L.dyn_smem, st);
   if (e != cudaSuccess) {
@@ -1014,7 +1019,8 @@ int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, const double
   const DevInfo d = device_info();
   const int n = 9 * ba.num_cameras;
   if (cudaMemsetAsync(y, 0, (size_t)n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
-  if (ba.num_slices > 0) k_matvec_points<T><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, x, y);
+  if (ba.num_slices > 0) { count_launch(); k_matvec_points<T><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, x, y); }
+  count_launch();
   k_matvec_diag<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(ba, x, y, rhs, res);
   return check_launch();
 }
@@ -1031,6 +1037,7 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
   rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, precond, min_it, max_it, tol, st, L, scratch);
   if (rc) return rc;
   double* result = reinterpret_cast<double*>(scratch + L.result);
+  count_launch();
   k_copy_result<<<1, 1, 0, st>>>(ba, result, -1.0);
   if (max_ref > 0 && sizeof(T) == sizeof(float)) {
     // float64 refinement: res = rhs - S x (float64 accumulation); solve S dx = res; x += dx
@@ -1044,8 +1051,10 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
     }
     rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
     if (rc) return rc;
+    count_launch();
     k_norm_into<<<1, 256, 0, st>>>(r64, n, ba.stats + CERES_B200_STAT_REFINE_RNORM);
   }
+  count_launch();
   k_copy_error<<<1, 1, 0, st>>>(ba);
   return check_launch();
 }
@@ -1055,6 +1064,10 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
 extern "C" {
 
 int ceres_b200_abi_version(void) { return CERES_B200_ABI_VERSION; }
+
+uint64_t ceres_b200_launch_count(void) { return (uint64_t)__atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int ceres_b200_ba_struct_bytes(void) { return (int)sizeof(ceres_b200_ba_t); }
 
 int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out) {
   if (!ba || !bytes_out) return CERES_B200_EINVAL;
@@ -1072,12 +1085,13 @@ int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* s
   const int grid = slice_grid(*ba, d);
   double* partials = reinterpret_cast<double*>(ba->scratch);
   if (ba->precision == CERES_B200_FP32) {
-    if (with_jacobian) k_evaluate<float, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
-    else k_evaluate<float, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+    if (with_jacobian) { count_launch(); k_evaluate<float, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    else { count_launch(); k_evaluate<float, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
   } else {
-    if (with_jacobian) k_evaluate<double, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
-    else k_evaluate<double, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+    if (with_jacobian) { count_launch(); k_evaluate<double, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    else { count_launch(); k_evaluate<double, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
   }
+  count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
   return check_launch();
 }
@@ -1090,6 +1104,7 @@ int ceres_b200_ba_point_assemble(const ceres_b200_ba_t* ba, double radius, doubl
   const double inv_radius = 1.0 / fmax(radius, kEps64);
   double* partials = reinterpret_cast<double*>(ba->scratch);
   const int grid = slice_grid(*ba, d);
+  count_launch();
   if (ba->precision == CERES_B200_FP32)
     k_point_assemble<float><<<grid, kWarpBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal, jacobi_scaling,
                                                          partials);
@@ -1108,6 +1123,7 @@ int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, doub
   cudaStream_t st = (cudaStream_t)stream;
   const double inv_radius = 1.0 / fmax(radius, kEps64);
   double* partials = reinterpret_cast<double*>(ba->scratch);
+  count_launch();
   if (ba->precision == CERES_B200_FP32)
     k_camera_assemble<float><<<ba->num_cameras, kCamBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal,
                                                                     jacobi_scaling, preconditioner, partials);
@@ -1151,16 +1167,19 @@ int ceres_b200_ba_step(const ceres_b200_ba_t* ba, void* stream) {
   ceres_b200_ba_t b2 = *ba;
   double* cam_stats = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + L.aux);
   b2.stats = cam_stats;
+  count_launch();
   k_camera_step<<<cgrid, 256, 0, st>>>(b2, partials);
   const int grid = slice_grid(*ba, d);
-  if (ba->precision == CERES_B200_FP32) k_step<float><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
-  else k_step<double><<<grid, kWarpBlock, 0, st>>>(*ba, partials);
+  if (ba->precision == CERES_B200_FP32) { count_launch(); k_step<float><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+  else { count_launch(); k_step<double><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
   // STEP_SQ_C and the camera non-finite count into the shared stats
+  count_launch();
   k_add_nonfinite<<<1, 1, 0, st>>>(ba->stats, cam_stats + CERES_B200_STAT_NONFINITE);
   cudaMemcpyAsync(ba->stats + CERES_B200_STAT_STEP_SQ_C, cam_stats + CERES_B200_STAT_STEP_SQ_C, sizeof(double),
                   cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(ba->stats + CERES_B200_STAT_CAND_STATE_SQ_C, cam_stats + CERES_B200_STAT_CAND_STATE_SQ_C,
                   sizeof(double), cudaMemcpyDeviceToDevice, st);
+  count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
   return check_launch();
 }
@@ -1176,6 +1195,7 @@ int ceres_b200_dense_cholesky_solve(double* H, const double* rhs, double* x, int
     const size_t smem = ((size_t)n * n + n) * sizeof(double);
     if (cudaFuncSetAttribute(k_chol_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return CERES_B200_ESMEM;
+    count_launch();
     k_chol_smem<<<1, 1024, smem, st>>>(H, rhs, x, n, flags + 3);
     return check_launch();
   }
@@ -1187,9 +1207,11 @@ int ceres_b200_dense_cholesky_solve(double* H, const double* rhs, double* x, int
   unsigned* errp = flags + 3;
   int nn = n;
   void* args[] = {&H, &nn, &gb, &errp};
+  count_launch();
   if (cudaLaunchCooperativeKernel((const void*)k_chol_global, dim3(d.sms * per_sm), dim3(512), args, 0, st) !=
       cudaSuccess)
     return CERES_B200_ECOOP;
+  count_launch();
   k_tri_solve<<<1, 1024, 0, st>>>(H, rhs, x, n);
   return check_launch();
 }
@@ -1210,16 +1232,19 @@ int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, voi
   const DevInfo d = device_info();
   if (cudaMemsetAsync(work, 0, (size_t)n * n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
   if (ba->num_slices > 0) {
+    count_launch();
     if (ba->precision == CERES_B200_FP32)
       k_schur_explicit<float><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, work, n);
     else
       k_schur_explicit<double><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, work, n);
   }
+  count_launch();
   k_dense_diag<<<(n + 255) / 256, 256, 0, st>>>(*ba, work, n);
   if (n <= kCholSmemMax) {
     const size_t smem = ((size_t)n * n + n) * sizeof(double);
     if (cudaFuncSetAttribute(k_chol_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       return CERES_B200_ESMEM;
+    count_launch();
     k_chol_smem<<<1, 1024, smem, st>>>(work, ba->rhs, ba->step_cameras, n, &ba->counters[kCtrError]);
   } else {
     if (cudaMemsetAsync(&ba->counters[kCtrBarCount], 0, 3 * sizeof(uint32_t), st) != cudaSuccess)
@@ -1231,11 +1256,14 @@ int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, voi
     unsigned* errp = &ba->counters[kCtrError];
     int nn = n;
     void* args[] = {&work, &nn, &gb, &errp};
+    count_launch();
     if (cudaLaunchCooperativeKernel((const void*)k_chol_global, dim3(d.sms * per_sm), dim3(512), args, 0, st) !=
         cudaSuccess)
       return CERES_B200_ECOOP;
+    count_launch();
     k_tri_solve<<<1, 1024, 0, st>>>(work, ba->rhs, ba->step_cameras, n);
   }
+  count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
   return check_launch();
 }

@@ -157,6 +157,12 @@ typedef struct ceres_b200_ba_t {
 /* ABI version of the loaded library (CERES_B200_ABI_VERSION). */
 int ceres_b200_abi_version(void);
 
+/* sizeof(ceres_b200_ba_t) as compiled into the library (binding check). */
+int ceres_b200_ba_struct_bytes(void);
+
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t ceres_b200_launch_count(void);
+
 /* Bytes of scratch the PCG and reductions need for this problem on this device. */
 int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out);
 

@@ -552,6 +552,7 @@ class OracleOptions:
     jacobi_scaling: bool = True
     use_nonmonotonic_steps: bool = False
     max_consecutive_nonmonotonic_steps: int = 5
+    explicit_schur_limit: int = 1800  # PCG on an explicit S up to this many camera columns
 
 
 @dataclass
@@ -669,7 +670,7 @@ def solve(prob: OracleProblem, opts: OracleOptions | None = None) -> OracleResul
             res.termination, res.message = "CONVERGENCE", "No active parameters."
             terminated = True
             break
-        xa, xb, its = solve_step(prob, ev, radius, opts)
+        xa, xb, its = solve_step(prob, ev, radius, opts, explicit_limit=opts.explicit_schur_limit)
         step = np.concatenate([xa.reshape(-1), xb.reshape(-1)])
         if not np.all(np.isfinite(step)):
             consecutive_invalid += 1

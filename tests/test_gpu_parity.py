@@ -1,0 +1,256 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU oracle and with
+results of the ceres-torch reference itself.
+
+Tolerances (float64 path): evaluation, Schur pieces and products 1e-10
+relative; LM solves: final cost 1e-9 relative to the reference's, parameters
+1e-5 relative, identical iteration counts where the oracle/reference agree.
+Mixed path (FP32 Jacobian/PCG, float64 cost and refinement): final cost within
+1e-6 relative of the float64 result, iteration count within +-2.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ba_oracle as O
+from tests import _golden as G
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda"
+
+
+def _tc():
+    import ceres_torch_cuda_b200 as tc
+    return tc
+
+
+def _loss_obj(spec):
+    tc = _tc()
+    kind = spec[0]
+    if kind == "trivial":
+        return None
+    return {"huber": tc.HuberLoss, "cauchy": tc.CauchyLoss, "softlone": tc.SoftLOneLoss, "arctan": tc.ArctanLoss,
+            "tukey": tc.TukeyLoss}[kind](float(spec[1]))
+
+
+def _engine(d, precision="fp64", cam_const=None):
+    tc = _tc()
+    meta = d["meta"]
+    nc = d["cameras"].shape[0]
+    cc = G.constant_mask(nc, meta["constant_cameras"]) if cam_const is None else cam_const
+    t = lambda a, dt=torch.float64: torch.as_tensor(a).to(DEV, dt)  # noqa: E731
+    return tc.BAEngine(t(d["cameras"]), t(d["points"]), t(d["observations"]), t(d["camera_index"], torch.int64),
+                       t(d["point_index"], torch.int64), loss=_loss_obj(G.loss_spec(meta["loss"])),
+                       camera_constant=t(cc, torch.bool), precision=precision)
+
+
+def _oracle_problem(d):
+    meta = d["meta"]
+    nc = d["cameras"].shape[0]
+    return O.OracleProblem(d["cameras"], d["points"], d["observations"], d["camera_index"], d["point_index"],
+                           G.loss_spec(meta["loss"]), camera_constant=G.constant_mask(nc, meta["constant_cameras"]))
+
+
+@pytest.mark.parametrize("name", G.BA_CASES + ["config0_dense"])
+def test_evaluate_matches_reference(name):
+    d = G.load(name)
+    eng = _engine(d)
+    eng.evaluate(True)
+    st = eng.read_stats()
+    np.testing.assert_allclose(st[0], d["eval_cost"], rtol=1e-11)
+    r, Jc, Jp = (x.cpu().numpy() for x in eng.slot_view())
+    np.testing.assert_allclose(r, d["eval_residuals"], rtol=1e-10, atol=1e-9)
+    scale = max(1.0, float(np.abs(d["eval_Jc"]).max()))
+    np.testing.assert_allclose(Jc, d["eval_Jc"], rtol=1e-9, atol=1e-11 * scale)
+    np.testing.assert_allclose(Jp, d["eval_Jp"], rtol=1e-9, atol=1e-11 * scale)
+
+
+@pytest.mark.parametrize("name", ["ba_small_iterative", "ba_huber_outliers", "ba_cauchy", "config1_small"])
+def test_schur_pieces_match_oracle(name):
+    d = G.load(name)
+    eng = _engine(d)
+    p = _oracle_problem(d)
+    tc = _tc()
+    opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                            preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI)
+    radius = 123.0
+    eng.evaluate(True)
+    eng.assemble(radius, opts, 2)
+    st = eng.read_stats()
+    ev = O.evaluate(p, p.cameras, p.points)
+    g = O._gradient(p, ev)
+    np.testing.assert_allclose(max(st[1], st[3]), np.max(np.abs(g)), rtol=1e-10)
+    np.testing.assert_allclose(st[2] + st[4], np.sum(g * g), rtol=1e-10)
+    # oracle Schur system with the same damping
+    pt = p.pt_col[p.point_index]
+    cam = p.cam_col[p.camera_index]
+    col_p = O._segment_sum(np.sum(ev.Jp ** 2, axis=1), pt, p.active_pts.size)
+    col_c = O._segment_sum(np.sum(ev.Jc ** 2, axis=1), cam, p.active_cams.size)
+    dp = O.jacobi_damping(col_p, radius, 1e-6, 1e32)
+    dc = O.jacobi_damping(col_c, radius, 1e-6, 1e32)
+    sys = O.build_schur(p, ev, dp, dc)
+    rhs = eng.rhs[: eng.nc].cpu().numpy()
+    np.testing.assert_allclose(rhs, sys.rhs, rtol=1e-9, atol=1e-9 * np.abs(sys.rhs).max())
+    # S x for a random x
+    x = np.random.default_rng(0).normal(size=(eng.nc, 9))
+    y = eng.schur_matvec(torch.as_tensor(x.reshape(-1))).cpu().numpy().reshape(-1, 9)
+    y_ref = O.schur_matvec(sys, x)
+    np.testing.assert_allclose(y, y_ref, rtol=1e-9, atol=1e-9 * np.abs(y_ref).max())
+    # preconditioner blocks are inverses of the S diagonal blocks
+    D = O.schur_diag_blocks(sys)
+    Minv = eng.precond[: eng.nc].cpu().numpy().reshape(-1, 9, 9)
+    np.testing.assert_allclose(Minv, np.linalg.inv(D), rtol=1e-8, atol=1e-10 * np.abs(np.linalg.inv(D)).max())
+
+
+@pytest.mark.parametrize("name", ["ba_small_iterative", "ba_cauchy", "config1_small", "config2_small"])
+def test_pcg_matches_oracle(name):
+    d = G.load(name)
+    eng = _engine(d)
+    p = _oracle_problem(d)
+    tc = _tc()
+    opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                            preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI)
+    radius = 1e4
+    eng.evaluate(True)
+    eng.assemble(radius, opts, 2)
+    for tol, its in ((0.1, 500), (1e-8, 500), (0.0, 7)):
+        eng.pcg(2, 0, its, tol)
+        st = eng.read_stats()
+        ev = O.evaluate(p, p.cameras, p.points)
+        opts_o = O.OracleOptions(eta=tol, max_linear_solver_iterations=its)
+        xa, xb, n_it = O.solve_step(p, ev, radius, opts_o, explicit_limit=0)
+        assert int(st[10]) == n_it, (tol, int(st[10]), n_it)
+        xg = eng.step_cameras[: eng.nc].cpu().numpy()
+        np.testing.assert_allclose(xg, xb, rtol=1e-7, atol=1e-9 * np.abs(xb).max())
+
+
+@pytest.mark.parametrize("name", G.BA_CASES + G.BIG_CASES)
+def test_lm_solve_matches_reference(name):
+    tc = _tc()
+    d = G.load(name)
+    meta = d["meta"]
+    nc = d["cameras"].shape[0]
+    t = lambda a, dt=torch.float64: torch.as_tensor(a).to(DEV, dt)  # noqa: E731
+    prob = tc.BundleAdjustmentProblem(t(d["cameras"]), t(d["points"]), t(d["observations"]),
+                                      t(d["camera_index"], torch.int64), t(d["point_index"], torch.int64),
+                                      loss=_loss_obj(G.loss_spec(meta["loss"])),
+                                      camera_constant=t(G.constant_mask(nc, meta["constant_cameras"]), torch.bool))
+    opts = tc.SolverOptions(max_num_iterations=meta["max_num_iterations"],
+                            linear_solver_type=getattr(tc.LinearSolverType, meta["solver"]),
+                            preconditioner_type=getattr(tc.PreconditionerType, meta["preconditioner"]))
+    s = tc.solve(opts, prob, precision="fp64")
+    if name == "ba_const_camera_jacobi":  # chaotic trajectory (see test_oracle_golden)
+        np.testing.assert_allclose(s.final_cost, meta["final_cost"], rtol=1e-3)
+        return
+    assert s.termination_type.value == meta["termination"]
+    assert abs(len(s.iterations) - meta["num_iterations"]) <= 0, (len(s.iterations), meta["num_iterations"])
+    np.testing.assert_allclose(s.initial_cost, meta["initial_cost"], rtol=1e-11)
+    np.testing.assert_allclose(s.final_cost, meta["final_cost"], rtol=1e-9)
+    np.testing.assert_allclose(prob.cameras.cpu().numpy(), d["final_cameras"], rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(prob.points.cpu().numpy(), d["final_points"], rtol=1e-5, atol=1e-7)
+    lin = [it.linear_solver_iterations for it in s.iterations]
+    np.testing.assert_array_equal(lin, d["trace"][:, 7].astype(int))
+
+
+@pytest.mark.parametrize("name", ["ba_small_iterative", "ba_huber_outliers", "ba_cauchy", "config1_small",
+                                  "config2_small"])
+def test_mixed_precision_reaches_fp64_cost(name):
+    tc = _tc()
+    d = G.load(name)
+    meta = d["meta"]
+    t = lambda a, dt=torch.float64: torch.as_tensor(a).to(DEV, dt)  # noqa: E731
+    prob = tc.BundleAdjustmentProblem(t(d["cameras"]), t(d["points"]), t(d["observations"]),
+                                      t(d["camera_index"], torch.int64), t(d["point_index"], torch.int64),
+                                      loss=_loss_obj(G.loss_spec(meta["loss"])))
+    opts = tc.SolverOptions(max_num_iterations=meta["max_num_iterations"],
+                            linear_solver_type=getattr(tc.LinearSolverType, meta["solver"]),
+                            preconditioner_type=getattr(tc.PreconditionerType, meta["preconditioner"]))
+    s = tc.solve(opts, prob, precision="mixed")
+    assert s.precision == "mixed"
+    np.testing.assert_allclose(s.final_cost, meta["final_cost"], rtol=1e-6)
+    if meta["termination"] == "CONVERGENCE":
+        assert abs(len(s.iterations) - meta["num_iterations"]) <= 2
+
+
+def test_problem_api_round_trip():
+    """Problem of SnavelyReprojectionError blocks, as the BAL example builds it."""
+    tc = _tc()
+    d = G.load("ba_small_dense")
+    cams = torch.tensor(d["cameras"], device=DEV)
+    pts = torch.tensor(d["points"], device=DEV)
+    problem = tc.Problem()
+    cb = [cams[i] for i in range(cams.shape[0])]
+    pb = [pts[i] for i in range(pts.shape[0])]
+    for c in cb:
+        problem.AddParameterBlock(c)
+    for p_ in pb:
+        problem.AddParameterBlock(p_)
+        problem.SetParameterBlockOrderingGroup(p_, 0)
+    for c, p_, o in zip(d["camera_index"].tolist(), d["point_index"].tolist(), d["observations"]):
+        problem.AddResidualBlock(tc.SnavelyReprojectionError(o[0], o[1]), None, [cb[c], pb[p_]])
+    s = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.SPARSE_SCHUR), problem)
+    assert s.linear_solver_type_used is tc.LinearSolverType.DENSE_SCHUR
+    assert len(s.iterations) == d["meta"]["num_iterations"]
+    np.testing.assert_allclose(s.final_cost, d["meta"]["final_cost"], rtol=1e-9)
+    np.testing.assert_allclose(cams.cpu().numpy(), d["final_cameras"], rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(pts.cpu().numpy(), d["final_points"], rtol=1e-5, atol=1e-7)
+
+
+def test_duplicate_camera_observations():
+    """A point seen twice by one camera exercises the cross terms of the Schur diagonal."""
+    from ceres_torch_cuda_b200 import synthetic as S
+
+    data = S.make_small_ba(4, 40, 3, seed=9)
+    ci = np.concatenate([data.camera_index, data.camera_index[:6]])
+    pi = np.concatenate([data.point_index, data.point_index[:6]])
+    obs = np.concatenate([data.observations, data.observations[:6] + 0.5])
+    p = O.OracleProblem(data.cameras, data.points, obs, ci, pi)
+    ref = O.solve(p, O.OracleOptions(linear_solver_type="ITERATIVE_SCHUR"))
+    tc = _tc()
+    prob = tc.BundleAdjustmentProblem.from_arrays(data.cameras, data.points, obs, ci, pi)
+    s = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                                  preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI), prob)
+    assert len(s.iterations) == len(ref.iterations)
+    np.testing.assert_allclose(s.final_cost, ref.final_cost, rtol=1e-9)
+    ref_d = O.solve(p, O.OracleOptions(linear_solver_type="DENSE_SCHUR"))
+    prob2 = tc.BundleAdjustmentProblem.from_arrays(data.cameras, data.points, obs, ci, pi)
+    s2 = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.DENSE_SCHUR), prob2)
+    np.testing.assert_allclose(s2.final_cost, ref_d.final_cost, rtol=1e-9)
+
+
+def test_points_without_observations_and_empty_problem():
+    tc = _tc()
+    from ceres_torch_cuda_b200 import synthetic as S
+
+    data = S.make_small_ba(3, 30, 3, seed=12)
+    pts = np.concatenate([data.points, np.ones((5, 3))])  # 5 unobserved points
+    p = O.OracleProblem(data.cameras, pts, data.observations, data.camera_index, data.point_index)
+    ref = O.solve(p, O.OracleOptions(linear_solver_type="ITERATIVE_SCHUR"))
+    prob = tc.BundleAdjustmentProblem.from_arrays(data.cameras, pts, data.observations, data.camera_index,
+                                                  data.point_index)
+    s = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                                  preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI), prob)
+    np.testing.assert_allclose(s.final_cost, ref.final_cost, rtol=1e-9)
+    np.testing.assert_allclose(prob.points[-5:].cpu().numpy(), 1.0)
+    # no observations at all: cost 0, gradient 0 -> converged at iteration 0
+    empty = tc.BundleAdjustmentProblem.from_arrays(data.cameras, data.points, np.zeros((0, 2)),
+                                                   np.zeros(0, np.int64), np.zeros(0, np.int64))
+    s0 = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR), empty)
+    assert s0.final_cost == 0.0 and s0.termination_type.value == "CONVERGENCE"
+
+
+def test_invalid_step_path_with_nonfinite_observation_scale():
+    """A non-finite step (huge focal length) takes the invalid-step path without a GPU fault."""
+    tc = _tc()
+    from ceres_torch_cuda_b200 import synthetic as S
+
+    data = S.make_small_ba(3, 20, 3, seed=13)
+    cams = data.cameras.copy()
+    cams[0, 6] = 1e308
+    prob = tc.BundleAdjustmentProblem.from_arrays(cams, data.points, data.observations, data.camera_index,
+                                                  data.point_index)
+    s = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                                  max_num_iterations=10), prob)
+    assert s.termination_type.value in ("FAILURE", "CONVERGENCE", "NO_CONVERGENCE")
