@@ -41,7 +41,7 @@ def is_stale() -> bool:
 
 def nvcc_command(output: Path, extra: list[str] | None = None) -> list[str]:
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    return [nvcc, *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+    return [nvcc, *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "--Werror", "all-warnings", "-Xcompiler", "-fPIC", "-shared",
             f"-I{INCLUDE}", "-o", str(output), *[str(CSRC / s) for s in SOURCES], *(extra or [])]
 
 

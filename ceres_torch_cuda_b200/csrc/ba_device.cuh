@@ -20,8 +20,8 @@ constexpr float kEps32 = 1.1920928955078125e-7f;          // float32 machine eps
 constexpr int kRec = 24;                                   // Jacobian scalars per slot
 
 template <typename T> struct Eps;
-template <> struct Eps<double> { static __device__ __forceinline__ double v() { return kEps64; } };
-template <> struct Eps<float> { static __device__ __forceinline__ double v() { return (double)kEps32; } };
+template <> struct Eps<double> { static __host__ __device__ __forceinline__ double v() { return kEps64; } };
+template <> struct Eps<float> { static __host__ __device__ __forceinline__ double v() { return (double)kEps32; } };
 
 // ------------------------------------------------------------------------------------
 // Robust losses (ceres-torch losses.py:21-133): rho(s), rho'(s), rho''(s)

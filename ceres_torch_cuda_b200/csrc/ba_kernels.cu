@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include "ba_device.cuh"
 
@@ -18,6 +19,24 @@ namespace {
 
 // kernels launched by this library since load (reported by ceres_b200_launch_count)
 unsigned long long g_launches = 0;
+
+// CERES_B200_TRACE=1 in the environment prints each host-side step to stderr.
+bool trace_on() {
+  static int on = -1;
+  if (on < 0) {
+    const char* v = getenv("CERES_B200_TRACE");
+    on = (v && v[0] == '1') ? 1 : 0;
+  }
+  return on == 1;
+}
+#define CB_TRACE(...)                        \
+  do {                                       \
+    if (trace_on()) {                        \
+      fprintf(stderr, "[ceres_b200] " __VA_ARGS__); \
+      fprintf(stderr, "\n");                 \
+      fflush(stderr);                        \
+    }                                        \
+  } while (0)
 inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 
 // counters[] slots
@@ -417,15 +436,17 @@ struct PcgArgs {
   double* part_b;      // [G]
   double* part_c;      // [G][2]
   double* result;      // [4]: iterations, success, rnorm, rhs_norm
+  const double* norm_ref;  // when set: the tolerance is relative to *norm_ref, not |rhs|
+  const double* gate;      // when set and *gate == 0: do nothing (refinement after a failed solve)
 };
 
 constexpr int kPcgBlock = 512;
 
 template <typename T>
-__device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const T* __restrict__ r, T* __restrict__ z,
-                                              int c) {
+__device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const double* __restrict__ r,
+                                              double* __restrict__ z, int c) {
   const T* M = Minv + 81 * (size_t)c;
-  const T* rc = r + 9 * (size_t)c;
+  const double* rc = r + 9 * (size_t)c;
   double rr[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) rr[j] = (double)rc[j];
@@ -434,7 +455,7 @@ __device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const 
     double s = 0.0;
 #pragma unroll
     for (int j = 0; j < 9; ++j) s += (double)M[i * 9 + j] * rr[j];
-    z[9 * (size_t)c + i] = (T)s;
+    z[9 * (size_t)c + i] = s;
   }
 }
 
@@ -442,15 +463,17 @@ template <typename T>
 __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[2 * (kPcgBlock / 32)];
-  __shared__ double sh_scalar[4];
+  __shared__ double sred[kPcgBlock];
   const int n = a.n;
   T* ps = reinterpret_cast<T*>(smem_raw);
   T* ys = ps + ((n + 3) & ~3);
-  T* __restrict__ X = reinterpret_cast<T*>(ba.pcg_x);
-  T* __restrict__ R = reinterpret_cast<T*>(ba.pcg_r);
-  T* __restrict__ Z = reinterpret_cast<T*>(ba.pcg_z);
-  T* __restrict__ Pbuf = reinterpret_cast<T*>(ba.pcg_p);
-  T* __restrict__ AP = reinterpret_cast<T*>(ba.pcg_ap);
+  // PCG state vectors are float64 in both precisions; the product S p streams the
+  // Jacobian store in T with T accumulation.
+  double* __restrict__ X = reinterpret_cast<double*>(ba.pcg_x);
+  double* __restrict__ R = reinterpret_cast<double*>(ba.pcg_r);
+  double* __restrict__ Z = reinterpret_cast<double*>(ba.pcg_z);
+  double* __restrict__ Pbuf = reinterpret_cast<double*>(ba.pcg_p);
+  double* __restrict__ AP = reinterpret_cast<double*>(ba.pcg_ap);
   const T* __restrict__ Minv = reinterpret_cast<const T*>(ba.precond);
   T* part_y = reinterpret_cast<T*>(a.part_y_raw);
   const GridBarrier gb{&ba.counters[kCtrBarCount], &ba.counters[kCtrBarGen], &ba.counters[kCtrBarFlag]};
@@ -461,12 +484,19 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (G * blockDim.x) >> 5;
 
+  if (a.gate != nullptr && *a.gate == 0.0) {
+    // refinement after a solve that did not converge: leave x as it is
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.result[0] = 0.0; a.result[1] = 0.0; a.result[2] = 0.0; a.result[3] = 0.0;
+    }
+    return;
+  }
   // ---- init: x = 0, r = rhs, z = M^-1 r, p = z (written at the first phase A)
   {
     double rz = 0.0, rr = 0.0;
     for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-      X[j] = (T)0;
-      R[j] = (T)a.rhs[j];
+      X[j] = 0.0;
+      R[j] = a.rhs[j];
     }
     __syncthreads();
     for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
@@ -493,7 +523,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     if (!grid_sync(gb)) return;
     double t = 0.0;
     for (int g = 0; g < G; ++g) t += ld_cross(a.part_b + g);
-    rhs_norm = fmax(sqrt(t), a.eps);
+    rhs_norm = fmax(a.norm_ref != nullptr ? *a.norm_ref : sqrt(t), a.eps);
   }
   int iterations = 0;
   bool success = false;
@@ -504,12 +534,12 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     for (int k = 0; k < a.max_iterations; ++k) {
       // ---- phase A: p = z + beta p_old; y = (J_c^T J_c - H_cp W^-1 H_pc) p
       const int nxt = k == 0 ? 0 : cur ^ 1;
-      T* Pold = Pbuf + (size_t)cur * n;
-      T* Pnew = Pbuf + (size_t)nxt * n;
+      double* Pold = Pbuf + (size_t)cur * n;
+      double* Pnew = Pbuf + (size_t)nxt * n;
       if (a.smem_vectors) {
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
-          const T pv = (k == 0) ? ld_cross(Z + j) : (T)((double)ld_cross(Z + j) + beta * (double)ld_cross(Pold + j));
-          ps[j] = pv;
+          const double pv = (k == 0) ? ld_cross(Z + j) : ld_cross(Z + j) + beta * ld_cross(Pold + j);
+          ps[j] = (T)pv;
           ys[j] = (T)0;
           if (j >= j0 && j < j1) Pnew[j] = pv;
         }
@@ -520,28 +550,51 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
         for (int j = threadIdx.x; j < n; j += blockDim.x) my[j] = ys[j];
       } else {
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-          Pnew[j] = (k == 0) ? Z[j] : (T)((double)Z[j] + beta * (double)Pold[j]);
-          AP[j] = (T)0;
+          Pnew[j] = (k == 0) ? Z[j] : Z[j] + beta * Pold[j];
+          AP[j] = 0.0;
         }
         if (!grid_sync(gb)) return;
-        matvec_slices<T, T, T, true>(ba, Pnew, AP, gw, nw);
+        matvec_slices<T, double, double, true>(ba, Pnew, AP, gw, nw);
       }
       cur = nxt;
       if (!grid_sync(gb)) return;
       // ---- phase B: Ap = sum of partials + D p ; partial p.Ap
       {
         double v[1] = {0.0};
-        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-          double y = 0.0;
-          if (a.smem_vectors) {
-            for (int g = 0; g < G; ++g) y += (double)ld_cross(part_y + (size_t)g * n + j);
-          } else {
-            y = (double)ld_cross(AP + j);
+        const int m = j1 - j0;
+        const int S = (m > 0 && m <= (int)blockDim.x) ? (int)blockDim.x / m : 1;
+        if (a.smem_vectors && m > 0 && m <= (int)blockDim.x) {
+          // the G partial products of my components, summed by S thread groups in parallel
+          double acc = 0.0;
+          const int t = threadIdx.x;
+          if (t < m * S) {
+            const int jj = j0 + t % m;
+            for (int g = t / m; g < G; g += S) acc += (double)ld_cross(part_y + (size_t)g * n + jj);
           }
-          const double pj = (double)Pnew[j];
-          y += ba.cam_diag[j] * pj;
-          AP[j] = (T)y;
-          v[0] += pj * y;
+          sred[t] = acc;
+          __syncthreads();
+          if (t < m) {
+            double y = 0.0;
+            for (int s2 = 0; s2 < S; ++s2) y += sred[t + m * s2];
+            const int j = j0 + t;
+            const double pj = Pnew[j];
+            y += ba.cam_diag[j] * pj;
+            AP[j] = y;
+            v[0] += pj * y;
+          }
+        } else {
+          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            double y = 0.0;
+            if (a.smem_vectors) {
+              for (int g = 0; g < G; ++g) y += (double)ld_cross(part_y + (size_t)g * n + j);
+            } else {
+              y = (double)ld_cross(AP + j);
+            }
+            const double pj = Pnew[j];
+            y += ba.cam_diag[j] * pj;
+            AP[j] = y;
+            v[0] += pj * y;
+          }
         }
         block_reduce<1>(v, 0u, red);
         if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
@@ -557,8 +610,8 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
       // ---- phase C: x += alpha p ; r -= alpha Ap ; z = M^-1 r ; partial r.z, r.r
       {
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-          X[j] = (T)((double)X[j] + alpha * (double)Pnew[j]);
-          R[j] = (T)((double)R[j] - alpha * (double)AP[j]);
+          X[j] = X[j] + alpha * Pnew[j];
+          R[j] = R[j] - alpha * AP[j];
         }
         __syncthreads();
         for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
@@ -600,7 +653,6 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     a.result[2] = rnorm;
     a.result[3] = rhs_norm;
   }
-  (void)sh_scalar;
 }
 
 // ======================================================================================
@@ -724,6 +776,10 @@ __global__ void k_add_nonfinite(double* stats, const double* cam_nonfinite) {
 
 __global__ void k_copy_error(ceres_b200_ba_t ba) {
   ba.stats[CERES_B200_STAT_ERROR] = (double)(ba.counters[kCtrError] | ba.counters[kCtrBarFlag]);
+}
+
+__global__ void k_add_refinement(ceres_b200_ba_t ba, const double* rref) {
+  ba.stats[CERES_B200_STAT_PCG_ITERS] += rref[0];
 }
 
 __global__ void k_copy_result(ceres_b200_ba_t ba, const double* result, double refine_rnorm) {
@@ -980,9 +1036,9 @@ int scratch_bytes_impl(const ceres_b200_ba_t& ba, size_t& bytes) {
 }
 
 template <typename T>
-int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int accumulate, int precond,
-               int min_it, int max_it, double tol, cudaStream_t st, const PcgLayout& L, char* scratch) {
-  (void)precond;
+int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int accumulate, int min_it, int max_it,
+               double tol, cudaStream_t st, const PcgLayout& L, char* scratch, double* result, const double* norm_ref,
+               const double* gate) {
   PcgArgs a;
   a.rhs = rhs;
   a.x_out = x_out;
@@ -997,18 +1053,24 @@ int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int 
   a.part_y_raw = reinterpret_cast<double*>(scratch + L.part_y);
   a.part_b = reinterpret_cast<double*>(scratch + L.part_b);
   a.part_c = reinterpret_cast<double*>(scratch + L.part_c);
-  a.result = reinterpret_cast<double*>(scratch + L.result);
+  a.result = result;
+  a.norm_ref = norm_ref;
+  a.gate = gate;
   // barrier words start at zero for every launch
+  CB_TRACE("pcg: memset barrier words");
   if (cudaMemsetAsync(&ba.counters[kCtrBarCount], 0, 3 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
   ceres_b200_ba_t bcopy = ba;
   void* args[] = {&bcopy, &a};
   count_launch();
+  CB_TRACE("pcg: cooperative launch grid=%d block=%d smem=%zu n=%d cams/cta=%d smem_vectors=%d", L.grid, kPcgBlock,
+           L.dyn_smem, a.n, a.cams_per_cta, a.smem_vectors);
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg<T>, dim3(L.grid), dim3(kPcgBlock), args,
                                                     L.dyn_smem, st);
   if (e != cudaSuccess) {
     fprintf(stderr, "ceres_b200: cooperative PCG launch failed: %s\n", cudaGetErrorString(e));
     return CERES_B200_ECOOP;
   }
+  CB_TRACE("pcg: launched (%s)", trace_on() ? cudaGetErrorString(cudaStreamSynchronize(st)) : "");
   return CERES_B200_OK;
 }
 
@@ -1028,26 +1090,34 @@ int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, const double
 template <typename T>
 int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, double tol, int max_ref, cudaStream_t st) {
   PcgLayout L;
+  CB_TRACE("pcg: layout");
   int rc = pcg_layout<T>(ba, L);
+  CB_TRACE("pcg: layout rc=%d grid=%d total=%zu scratch=%lld", rc, L.grid, L.total, (long long)ba.scratch_bytes);
   if (rc) return rc;
   if (!ba.scratch || (size_t)ba.scratch_bytes < L.total) return CERES_B200_EINVAL;
   char* scratch = reinterpret_cast<char*>(ba.scratch);
   const int n = 9 * ba.num_cameras;
   if (n == 0) return CERES_B200_OK;
-  rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, precond, min_it, max_it, tol, st, L, scratch);
-  if (rc) return rc;
+  (void)precond;
   double* result = reinterpret_cast<double*>(scratch + L.result);
+  rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, min_it, max_it, tol, st, L, scratch, result, nullptr, nullptr);
+  if (rc) return rc;
   count_launch();
   k_copy_result<<<1, 1, 0, st>>>(ba, result, -1.0);
   if (max_ref > 0 && sizeof(T) == sizeof(float)) {
-    // float64 refinement: res = rhs - S x (float64 accumulation); solve S dx = res; x += dx
+    // float64 refinement: res = rhs - S x with float64 accumulation; while |res| is above
+    // the tolerance (relative to the original |rhs|) and the float32 solve had converged,
+    // solve S dx = res and add dx. With eta-size tolerances this normally takes 0 iterations.
     double* y64 = reinterpret_cast<double*>(scratch + L.x64);
     double* r64 = reinterpret_cast<double*>(scratch + L.r64);
+    double* rref = result + 4;
     for (int it = 0; it < max_ref; ++it) {
       rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
       if (rc) return rc;
-      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, precond, 0, max_it, tol, st, L, scratch);
+      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, 0, max_it, tol, st, L, scratch, rref, result + 3, result + 1);
       if (rc) return rc;
+      count_launch();
+      k_add_refinement<<<1, 1, 0, st>>>(ba, rref);
     }
     rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
     if (rc) return rc;

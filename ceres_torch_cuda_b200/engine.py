@@ -177,8 +177,8 @@ class BAEngine:
         self.precond = torch.zeros((ncq, 81), dtype=T, device=dev)
         self.rhs = torch.zeros((ncq, 9), **f64)
         self.step_cameras = torch.zeros((ncq, 9), **f64)
-        self.pcg = {k: torch.zeros(9 * ncq, dtype=T, device=dev) for k in ("x", "r", "z", "ap")}
-        self.pcg["p"] = torch.zeros(2 * 9 * ncq, dtype=T, device=dev)
+        self.pcg_vec = {k: torch.zeros(9 * ncq, **f64) for k in ("x", "r", "z", "ap")}
+        self.pcg_vec["p"] = torch.zeros(2 * 9 * ncq, **f64)
         self.ctl = torch.zeros(_lib.CTL_BYTES, dtype=torch.uint8, device=dev)
         self.ctl_host = torch.zeros(_lib.CTL_BYTES, dtype=torch.uint8, pin_memory=True)
         self.dense_work: torch.Tensor | None = None
@@ -198,8 +198,8 @@ class BAEngine:
         s.winv, s.winv_ga, s.step_points = _ptr(self.winv), _ptr(self.winv_ga), _ptr(self.step_points)
         s.cam_diag, s.precond, s.rhs, s.step_cameras = (_ptr(self.cam_diag), _ptr(self.precond), _ptr(self.rhs),
                                                         _ptr(self.step_cameras))
-        s.pcg_x, s.pcg_r, s.pcg_z = _ptr(self.pcg["x"]), _ptr(self.pcg["r"]), _ptr(self.pcg["z"])
-        s.pcg_p, s.pcg_ap = _ptr(self.pcg["p"]), _ptr(self.pcg["ap"])
+        s.pcg_x, s.pcg_r, s.pcg_z = _ptr(self.pcg_vec["x"]), _ptr(self.pcg_vec["r"]), _ptr(self.pcg_vec["z"])
+        s.pcg_p, s.pcg_ap = _ptr(self.pcg_vec["p"]), _ptr(self.pcg_vec["ap"])
         s.counters = self.ctl.data_ptr() + _lib.CTL_COUNTERS
         s.stats = self.ctl.data_ptr()
         self._bind_params()

@@ -140,7 +140,7 @@ typedef struct ceres_b200_ba_t {
   double* rhs;                 /* [num_cameras][9] reduced right-hand side */
   double* step_cameras;        /* [num_cameras][9] */
 
-  /* PCG vectors, float or double, [num_cameras][9] each */
+  /* PCG vectors (float64 in both precisions), [num_cameras][9] each */
   void* pcg_x;
   void* pcg_r;
   void* pcg_z;
