@@ -475,6 +475,13 @@ __device__ inline void block9_inverse(double A[81], double inv[81]) {
   }
 }
 
+// Slices in "snake" order: round r of the grid-stride walk runs forward on even
+// rounds and backward on odd ones, so with slices sorted by length every warp
+// gets a mix of long and short tracks.
+__device__ __forceinline__ int snake_slice(int r, int gw, int nw) {
+  return r * nw + ((r & 1) ? nw - 1 - gw : gw);
+}
+
 // ------------------------------------------------------------------------------------
 // Reductions
 // ------------------------------------------------------------------------------------

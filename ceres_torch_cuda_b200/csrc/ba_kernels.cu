@@ -97,7 +97,9 @@ __global__ void __launch_bounds__(kWarpBlock) k_evaluate(ceres_b200_ba_t ba, dou
   double cost = 0.0;
   unsigned err = 0;
   T* __restrict__ jac = reinterpret_cast<T*>(ba.jac);
-  for (int s = gw; s < ba.num_slices; s += nw) {
+  for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
+    const int s = snake_slice(r_, gw, nw);
+    if (s >= ba.num_slices) continue;
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
@@ -145,28 +147,43 @@ __global__ void __launch_bounds__(kWarpBlock) k_point_assemble(ceres_b200_ba_t b
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   T* __restrict__ winv = reinterpret_cast<T*>(ba.winv);
   double gmax = 0.0, gsq = 0.0;
-  for (int s = gw; s < ba.num_slices; s += nw) {
+  for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
+    const int s = snake_slice(r_, gw, nw);
+    if (s >= ba.num_slices) continue;
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
     double W[6] = {0, 0, 0, 0, 0, 0};
     double g[3] = {0, 0, 0};
-    for (int k = 0; k < len; ++k) {
-      const size_t slot = base + 32 * (size_t)k + lane;
-      if (ba.slot_cam[slot] < 0) continue;
-      T jp[6];
-      load_rec_jp(jac, slot, jp);
-      const double2 r = reinterpret_cast<const double2*>(ba.res)[slot];
-      const double a0 = jp[0], a1 = jp[1], a2 = jp[2], b0 = jp[3], b1 = jp[4], b2 = jp[5];
-      W[0] += a0 * a0 + b0 * b0;
-      W[1] += a0 * a1 + b0 * b1;
-      W[2] += a0 * a2 + b0 * b2;
-      W[3] += a1 * a1 + b1 * b1;
-      W[4] += a1 * a2 + b1 * b2;
-      W[5] += a2 * a2 + b2 * b2;
-      g[0] += a0 * r.x + b0 * r.y;
-      g[1] += a1 * r.x + b1 * r.y;
-      g[2] += a2 * r.x + b2 * r.y;
+    // padding slots hold zero Jacobians and zero residuals: they add nothing
+    int k = 0;
+    constexpr int U = 4;
+    for (; k < len; k += U) {
+      T jp[U][6];
+      double2 r[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int kk = min(k + u, len - 1);
+        const size_t slot = base + 32 * (size_t)kk + lane;
+        load_rec_jp(jac, slot, jp[u]);
+        r[u] = reinterpret_cast<const double2*>(ba.res)[slot];
+        if (k + u >= len) r[u] = make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const double w = (k + u < len) ? 1.0 : 0.0;
+        const double a0 = w * jp[u][0], a1 = w * jp[u][1], a2 = w * jp[u][2];
+        const double b0 = w * jp[u][3], b1 = w * jp[u][4], b2 = w * jp[u][5];
+        W[0] += a0 * a0 + b0 * b0;
+        W[1] += a0 * a1 + b0 * b1;
+        W[2] += a0 * a2 + b0 * b2;
+        W[3] += a1 * a1 + b1 * b1;
+        W[4] += a1 * a2 + b1 * b2;
+        W[5] += a2 * a2 + b2 * b2;
+        g[0] += a0 * r[u].x + b0 * r[u].y;
+        g[1] += a1 * r[u].x + b1 * r[u].y;
+        g[2] += a2 * r[u].x + b2 * r[u].y;
+      }
     }
     double inv[6] = {0, 0, 0, 0, 0, 0};
     double wga[3] = {0, 0, 0};
@@ -206,13 +223,11 @@ __device__ __forceinline__ int tri9(int j, int l) {  // upper-triangle index, j 
   return j * 9 - (j * (j - 1)) / 2 + (l - j);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t ba, double inv_radius, double mn,
-                                                               double mx, int jacobi_scaling, int precond,
-                                                               double* partials) {
+// Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
+// into acc_out[c][72] (float64).
+template <typename T, bool kDup>
+__global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba, double* __restrict__ acc_out) {
   __shared__ double sred[kCamAcc * (kCamBlock / 32)];
-  __shared__ double sacc[kCamAcc];
-  __shared__ double sred2[2 * (kCamBlock / 32)];
   const int c = blockIdx.x;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
@@ -261,7 +276,7 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t b
 #pragma unroll
         for (int l = j; l < 9; ++l) acc[tri9(j, l)] += (double)rv[j] * K0[l] + (double)rv[9 + j] * K1[l];
 
-      if (ba.has_duplicate_cameras) {
+      if (kDup) {
         // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
         const int sidx = q >> 5, ln = q & 31;
         const int len = ba.slice_len[sidx];
@@ -275,16 +290,17 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t b
           const double C01 = P0[0] * rk[21] + P0[1] * rk[22] + P0[2] * rk[23];
           const double C10 = P1[0] * rk[18] + P1[1] * rk[19] + P1[2] * rk[20];
           const double C11 = P1[0] * rk[21] + P1[1] * rk[22] + P1[2] * rk[23];
+#pragma unroll
           for (int j = 0; j < 9; ++j) {
             const double t0 = (double)rv[j] * C00 + (double)rv[9 + j] * C10;
             const double t1 = (double)rv[j] * C01 + (double)rv[9 + j] * C11;
+#pragma unroll
             for (int l = j; l < 9; ++l) acc[tri9(j, l)] -= t0 * (double)rk[l] + t1 * (double)rk[9 + l];
           }
         }
       }
     }
   }
-  // block reduction of kCamAcc values
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int i = 0; i < kCamAcc; ++i) {
@@ -293,19 +309,29 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t b
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < nw; ++w) s += sred[i * nw + w];
-    sacc[i] = s;
+    double sum = 0.0;
+    for (int w = 0; w < nw; ++w) sum += sred[i * nw + w];
+    acc_out[(size_t)c * kCamAcc + i] = sum;
   }
-  __syncthreads();
+}
+
+// Phase 2: one thread per camera forms the damping, the reduced rhs, the gradient
+// stats and the preconditioner block from the 72 sums.
+template <typename T>
+__global__ void __launch_bounds__(128) k_camera_finish(ceres_b200_ba_t ba, const double* __restrict__ acc_in,
+                                                      double inv_radius, double mn, double mx, int jacobi_scaling,
+                                                      int precond, double* partials) {
+  __shared__ double sred2[2 * (128 / 32)];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double gmax = 0.0, gsq = 0.0;
-  if (threadIdx.x == 0) {
-    T* __restrict__ pre = reinterpret_cast<T*>(ba.precond);
+  if (c < ba.num_cameras) {
+    const double* sacc = acc_in + (size_t)c * kCamAcc;
+    T* __restrict__ pre = reinterpret_cast<T*>(ba.precond) + 81 * (size_t)c;
     double* dc = ba.cam_diag + 9 * (size_t)c;
     double* rh = ba.rhs + 9 * (size_t)c;
-    if (cconst) {
+    if (ba.cam_const[c]) {
       for (int j = 0; j < 9; ++j) { dc[j] = 0.0; rh[j] = 0.0; }
-      for (int i = 0; i < 81; ++i) pre[81 * (size_t)c + i] = (T)((i % 10 == 0) ? 1.0 : 0.0);
+      for (int i = 0; i < 81; ++i) pre[i] = (T)((i % 10 == 0) ? 1.0 : 0.0);
     } else {
       double S[81], inv[81];
       for (int j = 0; j < 9; ++j) {
@@ -329,11 +355,10 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t b
         for (int j = 0; j < 9; ++j)
           inv[j * 10] = (precond == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(S[j * 10], Eps<T>::v()) : 1.0;
       }
-      for (int i = 0; i < 81; ++i) pre[81 * (size_t)c + i] = (T)inv[i];
+      for (int i = 0; i < 81; ++i) pre[i] = (T)inv[i];
     }
   }
   double v[2] = {gmax, gsq};
-  // only thread 0 holds values; block_reduce of zeros elsewhere is harmless
   block_reduce<2>(v, 1u, sred2);
   const int out[2] = {CERES_B200_STAT_GMAX_C, CERES_B200_STAT_GSQ_C};
   grid_finish<2>(v, 1u, partials, &ba.counters[kCtrCamera], ba.stats, out);
@@ -344,31 +369,64 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_assemble(ceres_b200_ba_t b
 //   t = sum_k Jp_k^T (Jc_k p_c(k)),  s = W^-1 t,  y_c(k) += Jc_k^T (Jc_k p_c(k) - Jp_k s)
 // The accumulation target y is shared memory (per-CTA partial) or global memory.
 // ======================================================================================
+// Observations processed per step of a lane's track walk: their loads are all
+// issued before any is used, so a warp keeps kUnroll records in flight.
+template <typename T> struct Unroll { static constexpr int v = 2; };
+
+template <typename T, typename TP, typename A, bool kCrossP>
+__device__ __forceinline__ void camera_product(const T* rv, const TP* __restrict__ pc, A& u0, A& u1) {
+  u0 = 0;
+  u1 = 0;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    const A pj = kCrossP ? (A)ld_cross(pc + j) : (A)pc[j];
+    u0 += (A)rv[j] * pj;
+    u1 += (A)rv[9 + j] * pj;
+  }
+}
+
 template <typename T, typename TP, typename A, bool kCrossP = false>
 __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int gw,
                                               int nw) {
+  constexpr int U = Unroll<T>::v;
   const int lane = threadIdx.x & 31;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  for (int s = gw; s < ba.num_slices; s += nw) {
+  for (int r = 0; r * nw < ba.num_slices; ++r) {
+    const int s = snake_slice(r, gw, nw);
+    if (s >= ba.num_slices) continue;
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
-    const size_t base = (size_t)ba.slice_base[s];
+    const size_t base = (size_t)ba.slice_base[s] + lane;
+    // padding slots hold zero Jacobians and camera -1; they are read like any slot
+    // (camera 0 stands in for the address) and add nothing
     A t0 = 0, t1 = 0, t2 = 0;
-    for (int k = 0; k < len; ++k) {
-      const size_t slot = base + 32 * (size_t)k + lane;
+    int k = 0;
+    for (; k + U <= len; k += U) {
+      int c[U];
+      T rv[U][kRec];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const size_t slot = base + 32 * (size_t)(k + u);
+        c[u] = ba.slot_cam[slot];
+        load_rec(jac, slot, rv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        A u0, u1;
+        camera_product<T, TP, A, kCrossP>(rv[u], pvec + 9 * (size_t)max(c[u], 0), u0, u1);
+        t0 += (A)rv[u][18] * u0 + (A)rv[u][21] * u1;
+        t1 += (A)rv[u][19] * u0 + (A)rv[u][22] * u1;
+        t2 += (A)rv[u][20] * u0 + (A)rv[u][23] * u1;
+      }
+    }
+    for (; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k;
       const int c = ba.slot_cam[slot];
-      if (c < 0) continue;
       T rv[kRec];
       load_rec(jac, slot, rv);
-      const TP* pc = pvec + 9 * (size_t)c;
-      A u0 = 0, u1 = 0;
-#pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        const A pj = kCrossP ? (A)ld_cross(pc + j) : (A)pc[j];
-        u0 += (A)rv[j] * pj;
-        u1 += (A)rv[9 + j] * pj;
-      }
+      A u0, u1;
+      camera_product<T, TP, A, kCrossP>(rv, pvec + 9 * (size_t)max(c, 0), u0, u1);
       t0 += (A)rv[18] * u0 + (A)rv[21] * u1;
       t1 += (A)rv[19] * u0 + (A)rv[22] * u1;
       t2 += (A)rv[20] * u0 + (A)rv[23] * u1;
@@ -378,20 +436,36 @@ __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const T
     const A s0 = w0 * t0 + w1 * t1 + w2 * t2;
     const A s1 = w1 * t0 + w3 * t1 + w4 * t2;
     const A s2 = w2 * t0 + w4 * t1 + w5 * t2;
-    for (int k = 0; k < len; ++k) {
-      const size_t slot = base + 32 * (size_t)k + lane;
+    k = 0;
+    for (; k + U <= len; k += U) {
+      int c[U];
+      T rv[U][kRec];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const size_t slot = base + 32 * (size_t)(k + u);
+        c[u] = ba.slot_cam[slot];
+        load_rec(jac, slot, rv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (c[u] < 0) continue;
+        A u0, u1;
+        camera_product<T, TP, A, kCrossP>(rv[u], pvec + 9 * (size_t)c[u], u0, u1);
+        const A v0 = u0 - ((A)rv[u][18] * s0 + (A)rv[u][19] * s1 + (A)rv[u][20] * s2);
+        const A v1 = u1 - ((A)rv[u][21] * s0 + (A)rv[u][22] * s1 + (A)rv[u][23] * s2);
+        A* yc = y + 9 * (size_t)c[u];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[u][j] * v0 + (A)rv[u][9 + j] * v1);
+      }
+    }
+    for (; k < len; ++k) {
+      const size_t slot = base + 32 * (size_t)k;
       const int c = ba.slot_cam[slot];
       if (c < 0) continue;
       T rv[kRec];
       load_rec(jac, slot, rv);
-      const TP* pc = pvec + 9 * (size_t)c;
-      A u0 = 0, u1 = 0;
-#pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        const A pj = kCrossP ? (A)ld_cross(pc + j) : (A)pc[j];
-        u0 += (A)rv[j] * pj;
-        u1 += (A)rv[9 + j] * pj;
-      }
+      A u0, u1;
+      camera_product<T, TP, A, kCrossP>(rv, pvec + 9 * (size_t)c, u0, u1);
       const A v0 = u0 - ((A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2);
       const A v1 = u1 - ((A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2);
       A* yc = y + 9 * (size_t)c;
@@ -437,10 +511,12 @@ struct PcgArgs {
   double* part_c;      // [G][2]
   double* result;      // [4]: iterations, success, rnorm, rhs_norm
   const double* norm_ref;  // when set: the tolerance is relative to *norm_ref, not |rhs|
-  const double* gate;      // when set and *gate == 0: do nothing (refinement after a failed solve)
+  const double* gate;      // when set and *gate == 0: do nothing
+  int stall_window;        // > 0: stop when |r| has not dropped below 0.99 of its best for this many iterations
 };
 
 constexpr int kPcgBlock = 512;
+constexpr int kStallWindow = 20;  // float32 PCG: iterations without a 1% residual drop before it stops
 
 template <typename T>
 __device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const double* __restrict__ r,
@@ -528,6 +604,8 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   int iterations = 0;
   bool success = false;
   double rnorm = sqrt(rr);
+  double rbest = rnorm;
+  int last_improvement = 0;
   double beta = 0.0;
   int cur = 0;
   if (!(a.min_iterations <= 0 && rnorm <= a.tolerance * rhs_norm)) {
@@ -636,6 +714,12 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
         break;
       }
       if (fabs(rz_old) <= a.eps) break;
+      if (a.stall_window > 0) {
+        // float32 products: the recurrence residual stops shrinking at the rounding floor;
+        // the float64 refinement pass then judges the iterate by its true residual
+        if (rnorm < 0.99 * rbest) { rbest = rnorm; last_improvement = iterations; }
+        else if (iterations - last_improvement >= a.stall_window) break;
+      }
       beta = rz_new / rz_old;
       rz_old = rz_new;
     }
@@ -691,15 +775,37 @@ __global__ void __launch_bounds__(kWarpBlock) k_step(ceres_b200_ba_t ba, double*
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
   double cand = 0.0, model = 0.0, sq = 0.0, nonfinite = 0.0, state = 0.0;
   unsigned err = 0;
-  for (int s = gw; s < ba.num_slices; s += nw) {
+  for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
+    const int s = snake_slice(r_, gw, nw);
+    if (s >= ba.num_slices) continue;
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
     double t[3] = {0, 0, 0};
-    for (int k = 0; k < len; ++k) {
+    // padding slots have zero Jacobians: read them with camera 0 as the address
+    int k = 0;
+    for (; k + 2 <= len; k += 2) {
+      int c[2];
+      T rv[2][kRec];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const size_t slot = base + 32 * (size_t)(k + u) + lane;
+        c[u] = max(ba.slot_cam[slot], 0);
+        load_rec(jac, slot, rv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const double* dc = ba.step_cameras + 9 * (size_t)c[u];
+        double u0 = 0.0, u1 = 0.0;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) { u0 += (double)rv[u][j] * dc[j]; u1 += (double)rv[u][9 + j] * dc[j]; }
+#pragma unroll
+        for (int m = 0; m < 3; ++m) t[m] += (double)rv[u][18 + m] * u0 + (double)rv[u][21 + m] * u1;
+      }
+    }
+    for (; k < len; ++k) {
       const size_t slot = base + 32 * (size_t)k + lane;
-      const int c = ba.slot_cam[slot];
-      if (c < 0) continue;
+      const int c = max(ba.slot_cam[slot], 0);
       T rv[kRec];
       load_rec(jac, slot, rv);
       const double* dc = ba.step_cameras + 9 * (size_t)c;
@@ -802,7 +908,9 @@ __global__ void __launch_bounds__(kWarpBlock) k_schur_explicit(ceres_b200_ba_t b
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  for (int s = gw; s < ba.num_slices; s += nw) {
+  for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
+    const int s = snake_slice(r_, gw, nw);
+    if (s >= ba.num_slices) continue;
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
@@ -984,7 +1092,7 @@ struct PcgLayout {
   int cams_per_cta = 0;
   int smem_vectors = 0;
   size_t dyn_smem = 0;
-  size_t aux = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0, total = 0;
+  size_t aux = 0, cam_acc = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0, total = 0;
 };
 
 template <typename T>
@@ -1009,6 +1117,8 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   size_t off = red_area_bytes(ba, d);
   L.aux = off;
   off += 256;
+  L.cam_acc = off;
+  off += ((size_t)(ba.num_cameras > 0 ? ba.num_cameras : 1) * kCamAcc * sizeof(double) + 255) & ~(size_t)255;
   L.part_y = off;
   off += L.smem_vectors ? (size_t)L.grid * n * sizeof(T) : 0;
   off = (off + 255) & ~(size_t)255;
@@ -1038,7 +1148,7 @@ int scratch_bytes_impl(const ceres_b200_ba_t& ba, size_t& bytes) {
 template <typename T>
 int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int accumulate, int min_it, int max_it,
                double tol, cudaStream_t st, const PcgLayout& L, char* scratch, double* result, const double* norm_ref,
-               const double* gate) {
+               const double* gate, int stall_window) {
   PcgArgs a;
   a.rhs = rhs;
   a.x_out = x_out;
@@ -1056,6 +1166,7 @@ int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int 
   a.result = result;
   a.norm_ref = norm_ref;
   a.gate = gate;
+  a.stall_window = stall_window;
   // barrier words start at zero for every launch
   CB_TRACE("pcg: memset barrier words");
   if (cudaMemsetAsync(&ba.counters[kCtrBarCount], 0, 3 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
@@ -1100,21 +1211,26 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
   if (n == 0) return CERES_B200_OK;
   (void)precond;
   double* result = reinterpret_cast<double*>(scratch + L.result);
-  rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, min_it, max_it, tol, st, L, scratch, result, nullptr, nullptr);
+  const bool refine = max_ref > 0 && sizeof(T) == sizeof(float);
+  const int stall = refine ? kStallWindow : 0;
+  rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, min_it, max_it, tol, st, L, scratch, result, nullptr, nullptr,
+                     stall);
   if (rc) return rc;
   count_launch();
   k_copy_result<<<1, 1, 0, st>>>(ba, result, -1.0);
-  if (max_ref > 0 && sizeof(T) == sizeof(float)) {
+  if (refine) {
     // float64 refinement: res = rhs - S x with float64 accumulation; while |res| is above
-    // the tolerance (relative to the original |rhs|) and the float32 solve had converged,
-    // solve S dx = res and add dx. With eta-size tolerances this normally takes 0 iterations.
+    // the tolerance (relative to the original |rhs|), solve S dx = res in float32 and add
+    // dx. With eta-size tolerances this normally takes 0 iterations; it matters when the
+    // float32 recurrence stalled at its rounding floor.
     double* y64 = reinterpret_cast<double*>(scratch + L.x64);
     double* r64 = reinterpret_cast<double*>(scratch + L.r64);
     double* rref = result + 4;
     for (int it = 0; it < max_ref; ++it) {
       rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
       if (rc) return rc;
-      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, 0, max_it, tol, st, L, scratch, rref, result + 3, result + 1);
+      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, 0, max_it, tol, st, L, scratch, rref, result + 3, nullptr,
+                         stall);
       if (rc) return rc;
       count_launch();
       k_add_refinement<<<1, 1, 0, st>>>(ba, rref);
@@ -1190,16 +1306,27 @@ int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, doub
   if (preconditioner < CERES_B200_PRECOND_IDENTITY || preconditioner > CERES_B200_PRECOND_SCHUR_JACOBI)
     return CERES_B200_EINVAL;
   if (ba->num_cameras == 0) return CERES_B200_OK;
+  PcgLayout L;
+  const int lrc = ba->precision == CERES_B200_FP32 ? pcg_layout<float>(*ba, L) : pcg_layout<double>(*ba, L);
+  if (lrc) return lrc;
+  if ((size_t)ba->scratch_bytes < L.total) return CERES_B200_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   const double inv_radius = 1.0 / fmax(radius, kEps64);
   double* partials = reinterpret_cast<double*>(ba->scratch);
-  count_launch();
-  if (ba->precision == CERES_B200_FP32)
-    k_camera_assemble<float><<<ba->num_cameras, kCamBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal,
-                                                                    jacobi_scaling, preconditioner, partials);
-  else
-    k_camera_assemble<double><<<ba->num_cameras, kCamBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal,
-                                                                     jacobi_scaling, preconditioner, partials);
+  double* acc = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + L.cam_acc);
+  const int nc = ba->num_cameras;
+  count_launch(2);
+  if (ba->precision == CERES_B200_FP32) {
+    if (ba->has_duplicate_cameras) k_camera_reduce<float, true><<<nc, kCamBlock, 0, st>>>(*ba, acc);
+    else k_camera_reduce<float, false><<<nc, kCamBlock, 0, st>>>(*ba, acc);
+    k_camera_finish<float><<<(nc + 127) / 128, 128, 0, st>>>(*ba, acc, inv_radius, min_diagonal, max_diagonal,
+                                                               jacobi_scaling, preconditioner, partials);
+  } else {
+    if (ba->has_duplicate_cameras) k_camera_reduce<double, true><<<nc, kCamBlock, 0, st>>>(*ba, acc);
+    else k_camera_reduce<double, false><<<nc, kCamBlock, 0, st>>>(*ba, acc);
+    k_camera_finish<double><<<(nc + 127) / 128, 128, 0, st>>>(*ba, acc, inv_radius, min_diagonal, max_diagonal,
+                                                                jacobi_scaling, preconditioner, partials);
+  }
   return check_launch();
 }
 

@@ -398,11 +398,12 @@ def linear_solver_kind(options: SolverOptions) -> str:
 
 def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, start: float,
            num_active_columns: int, max_refinements: int = 1, target_cost: float | None = None,
-           on_state=None) -> LMResult:
+           stop_at_target: bool = False, on_state=None) -> LMResult:
     """The trust-region loop. ``summary`` arrives with the preprocessing fields set.
 
     ``target_cost``: when given, the wall time at which the best cost first
-    drops to or below it is returned as ``time_to_tolerance``.
+    drops to or below it is returned as ``time_to_tolerance``; with
+    ``stop_at_target`` the solve ends there (USER_SUCCESS, "Target cost reached.").
     ``on_state(engine, which)``: copies device parameters to the caller's
     tensors (used for callbacks that look at the parameters).
     """
@@ -553,12 +554,18 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
                     pass  # best buffers already hold the best state
                 best_is_current = False
                 it.step_is_nonmonotonic = candidate_cost > best_cost
-            if target_cost is not None and ttt is None and best_cost <= target_cost:
+            reached = target_cost is not None and ttt is None and best_cost <= target_cost
+            if reached:
                 ttt = time.perf_counter() - start
             summary.final_cost = best_cost
             radius = lm.accepted(rho)
             it.trust_region_radius = radius
             it.step_is_successful = True
+            if reached and stop_at_target:
+                summary.iterations.append(it)
+                summary.termination_type = TerminationType.USER_SUCCESS
+                summary.message = "Target cost reached."
+                return finalize()
         else:
             summary.num_unsuccessful_steps += 1
             radius = lm.rejected()

@@ -59,12 +59,12 @@ def _check_supported(options: SolverOptions) -> None:
 
 
 def solve(options: SolverOptions, problem, *, precision: str | None = None, max_refinements: int = 1,
-          target_cost: float | None = None, return_engine: bool = False):
+          target_cost: float | None = None, stop_at_target: bool = False, return_engine: bool = False):
     """Solve ``problem`` in place and return the SolverSummary.
 
     ``precision`` overrides the registered precision ("fp64" or "mixed").
     ``target_cost`` records the wall time at which the best cost first reaches it
-    (``summary.time_to_tolerance_in_seconds``).
+    (``summary.time_to_tolerance_in_seconds``); ``stop_at_target`` ends the solve there.
     """
     options.validate()
     _check_supported(options)
@@ -110,7 +110,8 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
         _store(problem, extracted, c, p)
 
     result = run_lm(engine, options, summary, start=start, num_active_columns=n_active,
-                    max_refinements=max_refinements, target_cost=target_cost, on_state=on_state)
+                    max_refinements=max_refinements, target_cost=target_cost, stop_at_target=stop_at_target,
+                    on_state=on_state)
     c, p = engine.get_parameters("current")
     _store(problem, extracted, c, p)
     torch.cuda.current_stream(engine.device).synchronize()
