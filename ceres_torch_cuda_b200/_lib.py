@@ -16,7 +16,7 @@ c_int64 = ctypes.c_int64
 c_double = ctypes.c_double
 c_void_p = ctypes.c_void_p
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 EINVAL = -1
@@ -61,7 +61,7 @@ class BAStruct(ctypes.Structure):
         ("cam_offsets", c_void_p), ("cam_entries", c_void_p), ("cam_const", c_void_p), ("pt_const", c_void_p),
         ("cameras", c_void_p), ("points", c_void_p), ("cand_cameras", c_void_p), ("cand_points", c_void_p),
         ("jac", c_void_p), ("res", c_void_p),
-        ("winv", c_void_p), ("winv_ga", c_void_p), ("step_points", c_void_p),
+        ("point_raw", c_void_p), ("winv", c_void_p), ("winv_ga", c_void_p), ("step_points", c_void_p),
         ("cam_diag", c_void_p), ("precond", c_void_p), ("rhs", c_void_p), ("step_cameras", c_void_p),
         ("pcg_x", c_void_p), ("pcg_r", c_void_p), ("pcg_z", c_void_p), ("pcg_p", c_void_p), ("pcg_ap", c_void_p),
         ("scratch", c_void_p), ("scratch_bytes", c_int64),

@@ -519,12 +519,14 @@ __device__ __forceinline__ void block_reduce(double v[NV], unsigned is_max_mask,
   __syncthreads();
 }
 
-// Deterministic grid reduction: each CTA's thread 0 posts NV partials; the last
-// CTA to arrive folds them in CTA order and writes stats[out_idx[i]] (or ORs/adds
-// into it when accumulate). counter returns to zero afterwards.
+// Deterministic grid reduction: each CTA's thread 0 posts NV partials; the last CTA
+// to arrive folds them (thread t takes partials t, t + blockDim, ...; then a fixed
+// block reduction) and writes stats[out_idx[i]]. counter returns to zero afterwards.
+// smem must hold NV * (blockDim.x / 32) doubles.
 template <int NV>
 __device__ __forceinline__ void grid_finish(const double v[NV], unsigned is_max_mask, double* partials,
-                                            unsigned* counter, double* stats, const int out_idx[NV]) {
+                                            unsigned* counter, double* stats, const int out_idx[NV],
+                                            double* smem) {
   __shared__ bool last;
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -534,17 +536,22 @@ __device__ __forceinline__ void grid_finish(const double v[NV], unsigned is_max_
     last = (ticket == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
+  if (!last) return;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
 #pragma unroll
     for (int i = 0; i < NV; ++i) {
-      double acc = ((is_max_mask >> i) & 1u) ? 0.0 : 0.0;
-      for (unsigned b = 0; b < gridDim.x; ++b) {
-        const double x = *((volatile double*)&partials[(size_t)b * NV + i]);
-        acc = ((is_max_mask >> i) & 1u) ? fmax(acc, x) : acc + x;
-      }
-      stats[out_idx[i]] = acc;
+      const double x = __ldcg(&partials[(size_t)b * NV + i]);
+      acc[i] = ((is_max_mask >> i) & 1u) ? fmax(acc[i], x) : acc[i] + x;
     }
+  }
+  block_reduce<NV>(acc, is_max_mask, smem);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) stats[out_idx[i]] = acc[i];
     *counter = 0u;
     __threadfence();
   }
@@ -565,9 +572,10 @@ struct GridBarrier {
 
 __device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
   __shared__ int ok;
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
+    // the CTA's writes (ordered before thread 0 by the bar.sync) are released at device scope
+    cuda::atomic_thread_fence(cuda::memory_order_release, cuda::thread_scope_device);
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(*gb.generation);
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(*gb.count);
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> flg(*gb.flag);
@@ -593,7 +601,7 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
         }
       }
     }
-    __threadfence();
+    cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
     ok = good;
   }
   __syncthreads();

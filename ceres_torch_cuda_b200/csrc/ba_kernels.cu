@@ -105,6 +105,10 @@ __global__ void __launch_bounds__(kWarpBlock) k_evaluate(ceres_b200_ba_t ba, dou
     const size_t base = (size_t)ba.slice_base[s];
     const double X[3] = {ba.points[3 * (size_t)q], ba.points[3 * (size_t)q + 1], ba.points[3 * (size_t)q + 2]};
     const bool pconst = ba.pt_const[q] != 0;
+    // point sums J_p^T J_p (6) and J_p^T r (3) of this lane's track, from the stored
+    // (precision-T) Jacobian, so the point side of the Schur system needs no pass over
+    // the observations
+    double W[6] = {0, 0, 0, 0, 0, 0}, g[3] = {0, 0, 0};
     for (int k = 0; k < len; ++k) {
       const size_t slot = base + 32 * (size_t)k + lane;
       const int c = ba.slot_cam[slot];
@@ -124,14 +128,32 @@ __global__ void __launch_bounds__(kWarpBlock) k_evaluate(ceres_b200_ba_t ba, dou
           for (int j = 0; j < 3; ++j) o.jp[0][j] = o.jp[1][j] = 0.0;
         }
         store_rec(jac, slot, o);
+        double a[3], b[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) { a[m] = (double)(T)o.jp[0][m]; b[m] = (double)(T)o.jp[1][m]; }
+        W[0] += a[0] * a[0] + b[0] * b[0];
+        W[1] += a[0] * a[1] + b[0] * b[1];
+        W[2] += a[0] * a[2] + b[0] * b[2];
+        W[3] += a[1] * a[1] + b[1] * b[1];
+        W[4] += a[1] * a[2] + b[1] * b[2];
+        W[5] += a[2] * a[2] + b[2] * b[2];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) g[m] += a[m] * o.r[0] + b[m] * o.r[1];
       }
+    }
+    if (kJac) {
+      double* pr = ba.point_raw + 9 * (size_t)q;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) pr[i] = W[i];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) pr[6 + i] = g[i];
     }
   }
   if (err) atomicOr(&ba.counters[kCtrError], err);
   double v[1] = {cost};
   block_reduce<1>(v, 0u, red);
   const int out[1] = {CERES_B200_STAT_COST};
-  grid_finish<1>(v, 0u, partials, &ba.counters[kCtrEval], ba.stats, out);
+  grid_finish<1>(v, 0u, partials, &ba.counters[kCtrEval], ba.stats, out, red);
 }
 
 // ======================================================================================
@@ -141,50 +163,15 @@ template <typename T>
 __global__ void __launch_bounds__(kWarpBlock) k_point_assemble(ceres_b200_ba_t ba, double inv_radius, double mn,
                                                                double mx, int jacobi_scaling, double* partials) {
   __shared__ double red[2 * (kWarpBlock / 32)];
-  const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   T* __restrict__ winv = reinterpret_cast<T*>(ba.winv);
   double gmax = 0.0, gsq = 0.0;
-  for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
-    const int s = snake_slice(r_, gw, nw);
-    if (s >= ba.num_slices) continue;
-    const int q = s * 32 + lane;
-    const int len = ba.slice_len[s];
-    const size_t base = (size_t)ba.slice_base[s];
-    double W[6] = {0, 0, 0, 0, 0, 0};
-    double g[3] = {0, 0, 0};
-    // padding slots hold zero Jacobians and zero residuals: they add nothing
-    int k = 0;
-    constexpr int U = 4;
-    for (; k < len; k += U) {
-      T jp[U][6];
-      double2 r[U];
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ba.num_points; q += gridDim.x * blockDim.x) {
+    const double* pr = ba.point_raw + 9 * (size_t)q;
+    double W[6], g[3];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int kk = min(k + u, len - 1);
-        const size_t slot = base + 32 * (size_t)kk + lane;
-        load_rec_jp(jac, slot, jp[u]);
-        r[u] = reinterpret_cast<const double2*>(ba.res)[slot];
-        if (k + u >= len) r[u] = make_double2(0.0, 0.0);
-      }
+    for (int i = 0; i < 6; ++i) W[i] = pr[i];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const double w = (k + u < len) ? 1.0 : 0.0;
-        const double a0 = w * jp[u][0], a1 = w * jp[u][1], a2 = w * jp[u][2];
-        const double b0 = w * jp[u][3], b1 = w * jp[u][4], b2 = w * jp[u][5];
-        W[0] += a0 * a0 + b0 * b0;
-        W[1] += a0 * a1 + b0 * b1;
-        W[2] += a0 * a2 + b0 * b2;
-        W[3] += a1 * a1 + b1 * b1;
-        W[4] += a1 * a2 + b1 * b2;
-        W[5] += a2 * a2 + b2 * b2;
-        g[0] += a0 * r[u].x + b0 * r[u].y;
-        g[1] += a1 * r[u].x + b1 * r[u].y;
-        g[2] += a2 * r[u].x + b2 * r[u].y;
-      }
-    }
+    for (int i = 0; i < 3; ++i) g[i] = pr[6 + i];
     double inv[6] = {0, 0, 0, 0, 0, 0};
     double wga[3] = {0, 0, 0};
     if (!ba.pt_const[q]) {
@@ -208,7 +195,7 @@ __global__ void __launch_bounds__(kWarpBlock) k_point_assemble(ceres_b200_ba_t b
   double v[2] = {gmax, gsq};
   block_reduce<2>(v, 1u, red);
   const int out[2] = {CERES_B200_STAT_GMAX_P, CERES_B200_STAT_GSQ_P};
-  grid_finish<2>(v, 1u, partials, &ba.counters[kCtrPoint], ba.stats, out);
+  grid_finish<2>(v, 1u, partials, &ba.counters[kCtrPoint], ba.stats, out, red);
 }
 
 // ======================================================================================
@@ -361,7 +348,7 @@ __global__ void __launch_bounds__(128) k_camera_finish(ceres_b200_ba_t ba, const
   double v[2] = {gmax, gsq};
   block_reduce<2>(v, 1u, sred2);
   const int out[2] = {CERES_B200_STAT_GMAX_C, CERES_B200_STAT_GSQ_C};
-  grid_finish<2>(v, 1u, partials, &ba.counters[kCtrCamera], ba.stats, out);
+  grid_finish<2>(v, 1u, partials, &ba.counters[kCtrCamera], ba.stats, out, sred2);
 }
 
 // ======================================================================================
@@ -478,14 +465,16 @@ __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const T
 // y = S x with float64 accumulation (global atomics), for tests and refinement.
 template <typename T>
 __global__ void __launch_bounds__(kWarpBlock) k_matvec_points(ceres_b200_ba_t ba, const double* __restrict__ x,
-                                                              double* y) {
+                                                              double* y, const double* gate) {
+  if (gate != nullptr && *gate != 0.0) return;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   matvec_slices<T, double, double>(ba, x, y, gw, nw);
 }
 
 __global__ void k_matvec_diag(ceres_b200_ba_t ba, const double* __restrict__ x, double* y, const double* __restrict__ rhs,
-                              double* out_res) {
+                              double* out_res, const double* gate) {
+  if (gate != nullptr && *gate != 0.0) return;
   const int n = 9 * ba.num_cameras;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const double v = y[j] + ba.cam_diag[j] * x[j];
@@ -511,7 +500,7 @@ struct PcgArgs {
   double* part_c;      // [G][2]
   double* result;      // [4]: iterations, success, rnorm, rhs_norm
   const double* norm_ref;  // when set: the tolerance is relative to *norm_ref, not |rhs|
-  const double* gate;      // when set and *gate == 0: do nothing
+  const double* gate;      // when set and *gate != 0 (the solve before succeeded): do nothing
   int stall_window;        // > 0: stop when |r| has not dropped below 0.99 of its best for this many iterations
 };
 
@@ -535,11 +524,36 @@ __device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const 
   }
 }
 
+// Sum of the G per-CTA partials part[g * stride + off] (NV values), computed by the
+// whole CTA (thread g loads partial g) and broadcast to every thread. Every CTA
+// folds the same values in the same order, so all CTAs agree bit for bit.
+template <int NV>
+__device__ __forceinline__ void cta_sum_partials(const double* part, int G, int stride, double out[NV],
+                                                 double* red, double* bcast) {
+  double v[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = 0.0;
+  for (int g = threadIdx.x; g < G; g += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] += ld_cross(part + (size_t)g * stride + i);
+  }
+  block_reduce<NV>(v, 0u, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) bcast[i] = v[i];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NV; ++i) out[i] = bcast[i];
+  __syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[2 * (kPcgBlock / 32)];
   __shared__ double sred[kPcgBlock];
+  __shared__ double bcast[4];
   const int n = a.n;
   T* ps = reinterpret_cast<T*>(smem_raw);
   T* ys = ps + ((n + 3) & ~3);
@@ -560,8 +574,8 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (G * blockDim.x) >> 5;
 
-  if (a.gate != nullptr && *a.gate == 0.0) {
-    // refinement after a solve that did not converge: leave x as it is
+  if (a.gate != nullptr && *a.gate != 0.0) {
+    // refinement after a solve that met its tolerance: nothing to do
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.result[0] = 0.0; a.result[1] = 0.0; a.result[2] = 0.0; a.result[3] = 0.0;
     }
@@ -587,8 +601,13 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     if (threadIdx.x == 0) { a.part_c[2 * blockIdx.x] = v[0]; a.part_c[2 * blockIdx.x + 1] = v[1]; }
   }
   if (!grid_sync(gb)) return;
-  double rz_old = 0.0, rr = 0.0;
-  for (int g = 0; g < G; ++g) { rz_old += ld_cross(a.part_c + 2 * g); rr += ld_cross(a.part_c + 2 * g + 1); }
+  double rz_old, rr;
+  {
+    double t2[2];
+    cta_sum_partials<2>(a.part_c, G, 2, t2, red, bcast);
+    rz_old = t2[0];
+    rr = t2[1];
+  }
   // the rhs norm is taken in float64 from the float64 rhs
   double rhs_norm;
   {
@@ -597,9 +616,9 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     block_reduce<1>(v, 0u, red);
     if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
     if (!grid_sync(gb)) return;
-    double t = 0.0;
-    for (int g = 0; g < G; ++g) t += ld_cross(a.part_b + g);
-    rhs_norm = fmax(a.norm_ref != nullptr ? *a.norm_ref : sqrt(t), a.eps);
+    double t[1];
+    cta_sum_partials<1>(a.part_b, G, 1, t, red, bcast);
+    rhs_norm = fmax(a.norm_ref != nullptr ? *a.norm_ref : sqrt(t[0]), a.eps);
   }
   int iterations = 0;
   bool success = false;
@@ -615,6 +634,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
       double* Pold = Pbuf + (size_t)cur * n;
       double* Pnew = Pbuf + (size_t)nxt * n;
       if (a.smem_vectors) {
+#pragma unroll 4
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
           const double pv = (k == 0) ? ld_cross(Z + j) : ld_cross(Z + j) + beta * ld_cross(Pold + j);
           ps[j] = (T)pv;
@@ -647,6 +667,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
           const int t = threadIdx.x;
           if (t < m * S) {
             const int jj = j0 + t % m;
+#pragma unroll 4
             for (int g = t / m; g < G; g += S) acc += (double)ld_cross(part_y + (size_t)g * n + jj);
           }
           sred[t] = acc;
@@ -678,8 +699,12 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
         if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
       }
       if (!grid_sync(gb)) return;
-      double denom = 0.0;
-      for (int g = 0; g < G; ++g) denom += ld_cross(a.part_b + g);
+      double denom;
+      {
+        double t1[1];
+        cta_sum_partials<1>(a.part_b, G, 1, t1, red, bcast);
+        denom = t1[0];
+      }
       if (fabs(denom) <= a.eps) {
         success = rnorm <= a.tolerance * rhs_norm;
         break;
@@ -704,9 +729,13 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
         if (threadIdx.x == 0) { a.part_c[2 * blockIdx.x] = v[0]; a.part_c[2 * blockIdx.x + 1] = v[1]; }
       }
       if (!grid_sync(gb)) return;
-      double rz_new = 0.0;
-      rr = 0.0;
-      for (int g = 0; g < G; ++g) { rz_new += ld_cross(a.part_c + 2 * g); rr += ld_cross(a.part_c + 2 * g + 1); }
+      double rz_new;
+      {
+        double t2[2];
+        cta_sum_partials<2>(a.part_c, G, 2, t2, red, bcast);
+        rz_new = t2[0];
+        rr = t2[1];
+      }
       rnorm = sqrt(rr);
       iterations = k + 1;
       if (iterations >= a.min_iterations && rnorm <= a.tolerance * rhs_norm) {
@@ -761,7 +790,7 @@ __global__ void k_camera_step(ceres_b200_ba_t ba, double* partials) {
   double v[3] = {sq, nonfinite, state};
   block_reduce<3>(v, 0u, red);
   const int out[3] = {CERES_B200_STAT_STEP_SQ_C, CERES_B200_STAT_NONFINITE, CERES_B200_STAT_CAND_STATE_SQ_C};
-  grid_finish<3>(v, 0u, partials, &ba.counters[kCtrCamStep], ba.stats, out);
+  grid_finish<3>(v, 0u, partials, &ba.counters[kCtrCamStep], ba.stats, out, red);
 }
 
 template <typename T>
@@ -865,10 +894,16 @@ __global__ void __launch_bounds__(kWarpBlock) k_step(ceres_b200_ba_t ba, double*
   const int out[5] = {CERES_B200_STAT_CAND_COST, CERES_B200_STAT_MODEL, CERES_B200_STAT_STEP_SQ_P,
                       CERES_B200_STAT_NONFINITE, CERES_B200_STAT_CAND_STATE_SQ_P};
   // the camera step kernel's non-finite count is added afterwards (k_add_nonfinite)
-  grid_finish<5>(v, 0u, partials, &ba.counters[kCtrStep], ba.stats, out);
+  grid_finish<5>(v, 0u, partials, &ba.counters[kCtrStep], ba.stats, out, red);
 }
 
-__global__ void k_norm_into(const double* __restrict__ v, int n, double* out) {
+__global__ void k_zero_gated(double* __restrict__ y, int n, const double* gate) {
+  if (gate != nullptr && *gate != 0.0) return;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) y[j] = 0.0;
+}
+
+__global__ void k_norm_into(const double* __restrict__ v, int n, double* out, const double* gate) {
+  if (gate != nullptr && *gate != 0.0) return;
   __shared__ double red[8];
   double a[1] = {0.0};
   for (int j = threadIdx.x; j < n; j += blockDim.x) a[0] += v[j] * v[j];
@@ -1187,14 +1222,20 @@ int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int 
 
 // y = S x (float64 accumulation; the Jacobian is read in its stored precision T).
 // When rhs and res are given, res = rhs - y as well.
+// ``gate``: when set and *gate != 0 every kernel returns at once (y is then stale).
 template <typename T>
-int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, const double* rhs, double* res, cudaStream_t st) {
+int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, const double* rhs, double* res, cudaStream_t st,
+             const double* gate = nullptr) {
   const DevInfo d = device_info();
   const int n = 9 * ba.num_cameras;
-  if (cudaMemsetAsync(y, 0, (size_t)n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
-  if (ba.num_slices > 0) { count_launch(); k_matvec_points<T><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, x, y); }
   count_launch();
-  k_matvec_diag<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(ba, x, y, rhs, res);
+  k_zero_gated<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(y, n, gate);
+  if (ba.num_slices > 0) {
+    count_launch();
+    k_matvec_points<T><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, x, y, gate);
+  }
+  count_launch();
+  k_matvec_diag<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(ba, x, y, rhs, res, gate);
   return check_launch();
 }
 
@@ -1226,19 +1267,22 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
     double* y64 = reinterpret_cast<double*>(scratch + L.x64);
     double* r64 = reinterpret_cast<double*>(scratch + L.r64);
     double* rref = result + 4;
+    // every refinement kernel is gated on the float32 solve's success flag: when it met
+    // the tolerance the refinement launches return at once
+    const double* gate = result + 1;
     for (int it = 0; it < max_ref; ++it) {
-      rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
+      rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st, gate);
       if (rc) return rc;
-      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, 0, max_it, tol, st, L, scratch, rref, result + 3, nullptr,
+      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, 0, max_it, tol, st, L, scratch, rref, result + 3, gate,
                          stall);
       if (rc) return rc;
       count_launch();
       k_add_refinement<<<1, 1, 0, st>>>(ba, rref);
     }
-    rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st);
+    rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st, gate);
     if (rc) return rc;
     count_launch();
-    k_norm_into<<<1, 256, 0, st>>>(r64, n, ba.stats + CERES_B200_STAT_REFINE_RNORM);
+    k_norm_into<<<1, 256, 0, st>>>(r64, n, ba.stats + CERES_B200_STAT_REFINE_RNORM, gate);
   }
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(ba);
@@ -1265,7 +1309,7 @@ int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out) {
 }
 
 int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* stream) {
-  if (!valid(ba) || !ba->scratch) return CERES_B200_EINVAL;
+  if (!valid(ba) || !ba->scratch || (with_jacobian && !ba->point_raw)) return CERES_B200_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   const DevInfo d = device_info();
   const int grid = slice_grid(*ba, d);
@@ -1284,12 +1328,14 @@ int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* s
 
 int ceres_b200_ba_point_assemble(const ceres_b200_ba_t* ba, double radius, double min_diagonal, double max_diagonal,
                                  int jacobi_scaling, void* stream) {
-  if (!valid(ba) || !ba->scratch || !ba->winv || !ba->winv_ga) return CERES_B200_EINVAL;
+  if (!valid(ba) || !ba->scratch || !ba->winv || !ba->winv_ga || !ba->point_raw) return CERES_B200_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   const DevInfo d = device_info();
   const double inv_radius = 1.0 / fmax(radius, kEps64);
   double* partials = reinterpret_cast<double*>(ba->scratch);
-  const int grid = slice_grid(*ba, d);
+  int grid = (ba->num_points + kWarpBlock - 1) / kWarpBlock;
+  if (grid > d.sms * 8) grid = d.sms * 8;
+  if (grid < 1) grid = 1;
   count_launch();
   if (ba->precision == CERES_B200_FP32)
     k_point_assemble<float><<<grid, kWarpBlock, 0, st>>>(*ba, inv_radius, min_diagonal, max_diagonal, jacobi_scaling,

@@ -170,6 +170,7 @@ class BAEngine:
         self.best_points = torch.zeros((npq, 3), **f64)
         self.jac = torch.zeros((nslot, 24), dtype=T, device=dev)
         self.res = torch.zeros((nslot, 2), **f64)
+        self.point_raw = torch.zeros((npq, 9), **f64)
         self.winv = torch.zeros((npq, 6), dtype=T, device=dev)
         self.winv_ga = torch.zeros((npq, 3), **f64)
         self.step_points = torch.zeros((npq, 3), **f64)
@@ -195,6 +196,7 @@ class BAEngine:
         s.cam_offsets, s.cam_entries = _ptr(L.cam_offsets), _ptr(L.cam_entries)
         s.cam_const, s.pt_const = _ptr(self.cam_const), _ptr(self.pt_const)
         s.jac, s.res = _ptr(self.jac), _ptr(self.res)
+        s.point_raw = _ptr(self.point_raw)
         s.winv, s.winv_ga, s.step_points = _ptr(self.winv), _ptr(self.winv_ga), _ptr(self.step_points)
         s.cam_diag, s.precond, s.rhs, s.step_cameras = (_ptr(self.cam_diag), _ptr(self.precond), _ptr(self.rhs),
                                                         _ptr(self.step_cameras))
@@ -248,10 +250,34 @@ class BAEngine:
     def _stream(self) -> int:
         return torch.cuda.current_stream(self.device).cuda_stream
 
+    def enable_profiling(self) -> dict:
+        """Record CUDA events around every library call (no extra synchronisation);
+        ``profile_report()`` sums the device time per entry point."""
+        self._events = []
+        return self._events
+
+    def profile_report(self) -> dict:
+        torch.cuda.current_stream(self.device).synchronize()
+        out: dict = {}
+        for name, a, b in getattr(self, "_events", []):
+            ms = a.elapsed_time(b)
+            t = out.setdefault(name, [0, 0.0])
+            t[0] += 1
+            t[1] += ms
+        return {k: {"calls": v[0], "ms": v[1]} for k, v in out.items()}
+
     def _call(self, name: str, *args) -> None:
         fn = getattr(self.lib, name)
+        events = getattr(self, "_events", None)
+        if events is not None:
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
         with torch.cuda.device(self.device):
             _lib.check(fn(ctypes.byref(self.struct), *args, self._stream()), name)
+        if events is not None:
+            b.record()
+            events.append((name, a, b))
 
     def evaluate(self, with_jacobian: bool = True) -> None:
         self._call("ceres_b200_ba_evaluate", int(with_jacobian))

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define CERES_B200_ABI_VERSION 1
+#define CERES_B200_ABI_VERSION 2
 
 /* status codes */
 #define CERES_B200_OK 0
@@ -130,6 +130,7 @@ typedef struct ceres_b200_ba_t {
   double* res;                 /* [num_slots][2] corrected residuals */
 
   /* point-side Schur pieces */
+  double* point_raw;           /* [num_points][9] J_p^T J_p (symmetric, 6) and J_p^T r (3), written by evaluate */
   void* winv;                  /* [num_points][6] (W + D_p)^-1, symmetric, float or double */
   double* winv_ga;             /* [num_points][3] W^-1 g_a with g_a = -J_p^T r */
   double* step_points;         /* [num_points][3] */
@@ -168,7 +169,7 @@ int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out);
 
 /*
  * Residuals, Jacobian and robust correction at ba->cameras / ba->points.
- * Writes ba->res, ba->jac (when with_jacobian) and stats[COST].
+ * Writes ba->res, ba->jac and ba->point_raw (when with_jacobian) and stats[COST].
  * Replaces Problem.evaluate (problem.py:377-413, :486-520), the autodiff
  * Jacobian of the Snavely residual (costs.py:31-44 over
  * examples/simple_bundle_adjuster.py:73-79, rotation.py:104-110, :211-222)
@@ -177,8 +178,9 @@ int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out);
 int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* stream);
 
 /*
- * Point side of the Schur system for a trust-region radius: Jacobi damping
- * D_p (linear.py:539-551), W_p = J_p^T J_p + D_p inverted per point
+ * Point side of the Schur system for a trust-region radius, from the point
+ * sums of the last evaluation: Jacobi damping D_p (linear.py:539-551),
+ * W_p = J_p^T J_p + D_p inverted per point
  * (linear.py:808 on the block-diagonal Haa), W^-1 g_a, and the point
  * gradient stats. Replaces the Haa part of linear.py:794-839.
  */
