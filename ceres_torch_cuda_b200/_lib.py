@@ -78,6 +78,7 @@ SIGNATURES = {
     "ceres_b200_launch_count": (ctypes.c_uint64, []),
     "ceres_b200_scratch_bytes": (c_int32, [_P, ctypes.POINTER(c_int64)]),
     "ceres_b200_ba_evaluate": (c_int32, [_P, c_int32, c_void_p]),
+    "ceres_b200_ba_evaluate_noalloc": (c_int32, [_P, c_int32, c_void_p]),
     "ceres_b200_ba_point_assemble": (c_int32, [_P, c_double, c_double, c_double, c_int32, c_void_p]),
     "ceres_b200_ba_camera_assemble": (c_int32, [_P, c_double, c_double, c_double, c_int32, c_int32, c_void_p]),
     "ceres_b200_ba_pcg": (c_int32, [_P, c_int32, c_int32, c_int32, c_double, c_int32, c_void_p]),

@@ -11,6 +11,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <mutex>
+
 #include "ba_device.cuh"
 
 using namespace cb200;
@@ -1314,6 +1316,78 @@ int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* s
   const DevInfo d = device_info();
   const int grid = slice_grid(*ba, d);
   double* partials = reinterpret_cast<double*>(ba->scratch);
+  if (ba->precision == CERES_B200_FP32) {
+    if (with_jacobian) { count_launch(); k_evaluate<float, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    else { count_launch(); k_evaluate<float, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+  } else {
+    if (with_jacobian) { count_launch(); k_evaluate<double, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    else { count_launch(); k_evaluate<double, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+  }
+  count_launch();
+  k_copy_error<<<1, 1, 0, st>>>(*ba);
+  return check_launch();
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------------------------------------
+// Evaluation without caller-provided scratch (ceres_b200_ba_evaluate_noalloc)
+// --------------------------------------------------------------------------------------
+namespace {
+
+// Per-CTA cost partials of the evaluator for callers that cannot hand us a scratch
+// buffer. It lives in the library image: every GPU that loads the library holds these
+// 256 KB until the process exits. All calls on a device share it.
+constexpr int kNoAllocPartials = 32768;  // float64 slots: one per evaluation CTA
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocPartials];
+
+// Device address of g_noalloc_partials, looked up once per device. In host code the
+// symbol's name is only a host-side stand-in, so kernels are given this address.
+double* noalloc_partials(int device, int* rc) {
+  static std::mutex mu;
+  static double* addr[64] = {nullptr};
+  *rc = CERES_B200_OK;
+  if (device < 0 || device >= 64) {
+    *rc = CERES_B200_EINVAL;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[device] == nullptr) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
+    if (e != cudaSuccess || ptr == nullptr) {
+      fprintf(stderr, "ceres_b200: cudaGetSymbolAddress for the static evaluation scratch failed: %s\n",
+              cudaGetErrorString(e));
+      *rc = CERES_B200_ECUDA;
+      return nullptr;
+    }
+    addr[device] = static_cast<double*>(ptr);
+  }
+  return addr[device];
+}
+
+}  // namespace
+
+extern "C" {
+
+int ceres_b200_ba_evaluate_noalloc(const ceres_b200_ba_t* ba, int with_jacobian, void* stream) {
+  if (!valid(ba) || (with_jacobian && !ba->point_raw)) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CERES_B200_ECUDA;
+  const DevInfo d = device_info();
+  const int grid = slice_grid(*ba, d);
+  if (grid > kNoAllocPartials) {
+    fprintf(stderr,
+            "ceres_b200: ceres_b200_ba_evaluate_noalloc needs %d reduction slots, above its static capacity of %d\n",
+            grid, kNoAllocPartials);
+    return CERES_B200_ETOOBIG;
+  }
+  int rc = CERES_B200_OK;
+  double* partials = noalloc_partials(dev, &rc);
+  if (rc) return rc;
+  // every CTA writes its own slot before the last one folds them, so the shared array
+  // needs no clearing between calls; the ticket counter is the caller's (counters[])
   if (ba->precision == CERES_B200_FP32) {
     if (with_jacobian) { count_launch(); k_evaluate<float, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
     else { count_launch(); k_evaluate<float, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }

@@ -178,6 +178,21 @@ int ceres_b200_scratch_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out);
 int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* stream);
 
 /*
+ * The same evaluation as ceres_b200_ba_evaluate for callers that cannot allocate
+ * device memory - for example a host runtime whose device memory is owned by
+ * another allocator, or one that forbids allocation after start-up - and so have
+ * no scratch buffer to put in ba->scratch (it is ignored here). The per-CTA cost
+ * partials go to a static 256 KB array inside the library (32768 float64 slots,
+ * one per evaluation CTA; each loaded GPU keeps it until the process exits). The
+ * first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. Sizes
+ * that need more slots return CERES_B200_ETOOBIG. Calls share the array: two
+ * calls that overlap on the GPU race. No memory is allocated or freed.
+ * This entry point has no counterpart in the reference.
+ */
+int ceres_b200_ba_evaluate_noalloc(const ceres_b200_ba_t* ba, int with_jacobian, void* stream);
+
+/*
  * Point side of the Schur system for a trust-region radius, from the point
  * sums of the last evaluation: Jacobi damping D_p (linear.py:539-551),
  * W_p = J_p^T J_p + D_p inverted per point
