@@ -59,12 +59,16 @@ def _check_supported(options: SolverOptions) -> None:
 
 
 def solve(options: SolverOptions, problem, *, precision: str | None = None, max_refinements: int = 1,
-          target_cost: float | None = None, stop_at_target: bool = False, return_engine: bool = False):
+          target_cost: float | None = None, stop_at_target: bool = False, return_engine: bool = False,
+          profile: bool = False):
     """Solve ``problem`` in place and return the SolverSummary.
 
     ``precision`` overrides the registered precision ("fp64" or "mixed").
     ``target_cost`` records the wall time at which the best cost first reaches it
     (``summary.time_to_tolerance_in_seconds``); ``stop_at_target`` ends the solve there.
+    ``profile`` brackets every library call with CUDA events (no extra
+    synchronisation) and puts the per-entry-point device times in
+    ``summary.kernel_profile``.
     """
     options.validate()
     _check_supported(options)
@@ -103,6 +107,8 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
     engine = BAEngine(cams, pts, obs, ci, pi, loss=loss, camera_constant=cam_const, point_constant=pt_const,
                       precision=prec)
     n_active = summary.num_effective_parameters
+    if profile:
+        engine.enable_profiling()
     summary.preprocessor_time_in_seconds = time.perf_counter() - start
 
     def on_state(eng, which):
@@ -118,6 +124,8 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
     summary.total_time_in_seconds = time.perf_counter() - start
     summary.time_to_tolerance_in_seconds = result.time_to_tolerance
     summary.precision = prec
+    if profile:
+        summary.kernel_profile = engine.profile_report()
     if return_engine:
         return summary, engine
     return summary

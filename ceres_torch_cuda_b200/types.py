@@ -271,6 +271,7 @@ class SolverSummary:
     # cost was given, the wall time until the best cost first reached it
     precision: str = "fp64"
     time_to_tolerance_in_seconds: float | None = None
+    kernel_profile: dict | None = None
 
     def IsSolutionUsable(self) -> bool:  # noqa: N802 - ceres-torch API name
         return self.termination_type in (TerminationType.CONVERGENCE, TerminationType.NO_CONVERGENCE,
