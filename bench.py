@@ -255,6 +255,7 @@ def run_ours(args):
     launches0 = lib.ceres_b200_launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")  # ncu --nvtx --nvtx-include "timed]" selects these launches
     ev0.record()
     ttts, summaries = [], []
     for _ in range(args.steps):
@@ -262,6 +263,7 @@ def run_ours(args):
         ttts.append(t)
         summaries.append(s)
     ev1.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -324,12 +326,16 @@ def run_ours(args):
                      "iterations_to_minimum": len(s64.iterations),
                      "iterations_to_tol": len(fp64_runs[-1][0].iterations)},
             "mixed": {"iterations_to_tol": len(summaries[-1].iterations),
+                      "time_to_tol_steps_s": ttts,
+                      "iterations_to_tol_steps": [len(s.iterations) for s in summaries],
+                      "e2e_steps_s": e2e_vals,
                       "best_cost": summaries[-1].final_cost,
                       "rel_err_vs_fp64_minimum": (summaries[-1].final_cost - cstar) / cstar,
                       "speedup_vs_fp64_ttt": (fp64_ttt / value) if value > 0 else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": TRAFFIC_PER_PCG_ITERATION * pcg["iterations_per_launch"]
-                         if TRAFFIC_PER_PCG_ITERATION else None,
+                         "traffic": pcg_traffic_per_launch(data.num_observations, pcg["iterations_per_launch"]),
+                         "traffic_note": "ncu DRAM bytes of a 1.5M-observation capture scaled by observations "
+                                         "and PCG iterations per launch",
                          "kernel": "k_pcg (implicit-Schur PCG, per launch; bytes and time over the timed solves)",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"},
             "kernels_timed_region": live,
@@ -347,10 +353,17 @@ def run_ours(args):
     return 0
 
 
-# DRAM bytes (read + write) of one PCG iteration on the 6M-observation workload,
-# from the ncu capture summarised in profiles/ (a 1.5M-observation capture scaled by
-# the observation count); None until a capture exists.
-TRAFFIC_PER_PCG_ITERATION = None
+# DRAM traffic of the PCG kernel from one ncu capture (profiles/k_pcg_kernel_pass_ring_1.5M_obs.md):
+# k_pcg<float>, 10 iterations on the 1,503,061-observation problem (bench.py --kernel-pass
+# --scale 0.25), dram__bytes_read.sum + dram__bytes_write.sum = 1726.3 MB + 79.2 MB.
+# Traffic grows with the observations (the Jacobian store is re-read every iteration), so
+# a launch on the full workload is credited that traffic per iteration and observation.
+PCG_CAPTURE = {"observations": 1503061, "iterations": 10, "dram_bytes": 1726.291e6 + 79.1936e6}
+
+
+def pcg_traffic_per_launch(observations: int, iterations_per_launch: float) -> float:
+    per_it_obs = PCG_CAPTURE["dram_bytes"] / PCG_CAPTURE["iterations"] / PCG_CAPTURE["observations"]
+    return per_it_obs * observations * iterations_per_launch
 
 
 def live_kernel_table(summaries, prof) -> dict:
@@ -438,6 +451,33 @@ def profile_kernels(tc, eng, opts) -> dict:
             "pcg_bytes_per_iteration": no * rec + slots * 4 + npq * 6 * jb}
 
 
+def run_kernel_pass(args):
+    """The kernels of one LM iteration (evaluate, point and camera assembly, a
+    10-iteration PCG, step), twice, on the workload at ``--scale``: the launch
+    sequence profiler captures are taken on. Prints one JSON line."""
+    import torch
+
+    import ceres_torch_cuda_b200 as tc
+
+    data = make_workload(args)
+    dev = torch.device("cuda", 0)
+    t = lambda a, dt=torch.float64: torch.as_tensor(a).to(dev, dt)  # noqa: E731
+    eng = tc.BAEngine(t(data.cameras), t(data.points), t(data.observations), t(data.camera_index, torch.int64),
+                      t(data.point_index, torch.int64), loss=loss_of(tc, data), precision=args.precision)
+    opts = solver_options(tc, data, tight=False)
+    for _ in range(2):
+        eng.evaluate(True)
+        eng.assemble(1e3, opts, 2)
+        eng.pcg(2, 10, 10, 0.0, 0)
+        eng.step()
+        eng.read_stats()
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_pass": data.description, "precision": args.precision,
+                      "observations": data.num_observations, "slots": eng.layout.num_slots,
+                      "jacobian_bytes": eng.jac.numel() * eng.jac.element_size()}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -447,7 +487,12 @@ def main():
     ap.add_argument("--config", type=int, default=2, choices=[0, 1, 2])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-pass", action="store_true",
+                    help="run one LM iteration's kernels twice (for profiler captures) and exit")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
+    if args.kernel_pass:
+        return run_kernel_pass(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -129,63 +129,67 @@ __device__ inline void loss_eval(const LossSpec& L, double s, double& r0, double
 // applied as X + w uv + u x uv with uv = 2 u x X (rotation.py:211-214). The
 // derivative follows the same chain, including the normalisation, so it equals
 // what autograd produces on the reference (costs.py:31-44), up to rounding.
-struct Proj {
+// Residual (float64) and Jacobian rows in J: float64, or float32 for the float32
+// Jacobian store, whose entries carry float32 rounding anyway.
+template <typename J>
+struct ProjT {
   double r[2];
-  double jc[2][9];
-  double jp[2][3];
+  J jc[2][9];
+  J jp[2][3];
 };
+using Proj = ProjT<double>;
 
-__device__ __forceinline__ void cross3(const double a[3], const double b[3], double o[3]) {
+template <typename V>
+__device__ __forceinline__ void cross3(const V a[3], const V b[3], V o[3]) {
   o[0] = a[1] * b[2] - a[2] * b[1];
   o[1] = a[2] * b[0] - a[0] * b[2];
   o[2] = a[0] * b[1] - a[1] * b[0];
 }
 
+// The camera-only part of the projection: the unit quaternion (w, u) of the
+// angle-axis aa and, for the Jacobian, its derivative dqn = d(w, u)/d(aa) (4 x 3),
+// including the normalisation. It depends on the 3 rotation parameters alone, so
+// the kernels compute it once per camera (k_camera_frames) and every observation of
+// the camera reads it back.
+struct CamRot {
+  double w;
+  double u[3];
+  double dqn[4][3];
+};
+
 template <bool kJac>
-__device__ __forceinline__ void snavely(const double* __restrict__ cam, const double X[3], double ox, double oy,
-                                        Proj& o) {
-  const double aa[3] = {cam[0], cam[1], cam[2]};
+__device__ __forceinline__ void camera_rotation(const double aa[3], CamRot& R) {
   const double th2 = aa[0] * aa[0] + aa[1] * aa[1] + aa[2] * aa[2];
   const double theta = sqrt(th2);
   const double half = theta * 0.5;
   const bool small = theta <= kEps64;
   double sh, ch;
   sincos(half, &sh, &ch);
-  const double safe_theta = small ? 1.0 : theta;
-  const double k = small ? 0.5 - theta * theta / 48.0 : sh / safe_theta;
+  // one reciprocal per divisor, reused below (a float64 division is a long
+  // instruction sequence; the products differ from the quotients by at most an ulp)
+  const double inv_theta = small ? 1.0 : 1.0 / theta;
+  const double k = small ? 0.5 - theta * theta * (1.0 / 48.0) : sh * inv_theta;
   double q[4] = {ch, k * aa[0], k * aa[1], k * aa[2]};
   double qn2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
   double n = sqrt(qn2);
   const bool clamped = n < kTiny64;
   if (clamped) n = kTiny64;
-  const double w = q[0] / n;
-  const double u[3] = {q[1] / n, q[2] / n, q[3] / n};
-  double c1[3];
-  cross3(u, X, c1);
-  const double uv[3] = {c1[0] * 2.0, c1[1] * 2.0, c1[2] * 2.0};
-  double c2[3];
-  cross3(u, uv, c2);
-  double p[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) p[i] = (X[i] + w * uv[i] + c2[i]) + cam[3 + i];
-  const double xp = -p[0] / p[2];
-  const double yp = -p[1] / p[2];
-  const double r2 = xp * xp + yp * yp;
-  const double k1 = cam[7], k2 = cam[8], f = cam[6];
-  const double dist = 1.0 + r2 * (k1 + k2 * r2);
-  const double fd = f * dist;
-  o.r[0] = fd * xp - ox;
-  o.r[1] = fd * yp - oy;
+  const double inv_n = 1.0 / n;
+  R.w = q[0] * inv_n;
+  R.u[0] = q[1] * inv_n;
+  R.u[1] = q[2] * inv_n;
+  R.u[2] = q[3] * inv_n;
   if (!kJac) return;
 
   // d q_raw / d aa  (4 x 3)
   double dth[3];
   if (theta > 0.0) {
-    dth[0] = aa[0] / theta; dth[1] = aa[1] / theta; dth[2] = aa[2] / theta;
+    const double it = small ? 1.0 / theta : inv_theta;
+    dth[0] = aa[0] * it; dth[1] = aa[1] * it; dth[2] = aa[2] * it;
   } else {
     dth[0] = dth[1] = dth[2] = 0.0;  // torch.linalg.norm's subgradient at 0
   }
-  const double dk_dth = small ? -(2.0 * theta) / 48.0 : (ch * 0.5 * theta - sh) / (theta * theta);
+  const double dk_dth = small ? -(2.0 * theta) * (1.0 / 48.0) : (ch * 0.5 * theta - sh) * (inv_theta * inv_theta);
   double dq[4][3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
@@ -195,75 +199,158 @@ __device__ __forceinline__ void snavely(const double* __restrict__ cam, const do
     for (int i = 0; i < 3; ++i) dq[1 + i][j] = (i == j ? k : 0.0) + aa[i] * dkj;
   }
   // normalisation: dqn = (dq - qn (qn . dq)) / n
-  double dqn[4][3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     if (clamped) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) dqn[i][j] = dq[i][j] / n;
+      for (int i = 0; i < 4; ++i) R.dqn[i][j] = dq[i][j] * inv_n;
     } else {
-      const double qn_dot = (w * dq[0][j] + u[0] * dq[1][j] + u[1] * dq[2][j] + u[2] * dq[3][j]);
-      dqn[0][j] = (dq[0][j] - w * qn_dot) / n;
+      const double qn_dot = (R.w * dq[0][j] + R.u[0] * dq[1][j] + R.u[1] * dq[2][j] + R.u[2] * dq[3][j]);
+      R.dqn[0][j] = (dq[0][j] - R.w * qn_dot) * inv_n;
 #pragma unroll
-      for (int i = 0; i < 3; ++i) dqn[1 + i][j] = (dq[1 + i][j] - u[i] * qn_dot) / n;
+      for (int i = 0; i < 3; ++i) R.dqn[1 + i][j] = (dq[1 + i][j] - R.u[i] * qn_dot) * inv_n;
     }
   }
-  // dp/daa: d(X + w uv + u x uv) = dw uv + w duv + du x uv + u x duv, duv = 2 du x X
-  double dpa[3][3];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const double du[3] = {dqn[1][j], dqn[2][j], dqn[3][j]};
-    double t1[3];
-    cross3(du, X, t1);
-    const double duv[3] = {2.0 * t1[0], 2.0 * t1[1], 2.0 * t1[2]};
-    double t2[3], t3[3];
-    cross3(du, uv, t2);
-    cross3(u, duv, t3);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) dpa[i][j] = dqn[0][j] * uv[i] + w * duv[i] + t2[i] + t3[i];
-  }
-  // dp/dX = I + 2 w [u]x + 2 [u]x^2, [u]x^2 = u u^T - (u.u) I
-  const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-  double M[3][3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) M[i][j] = 2.0 * u[i] * u[j] + (i == j ? 1.0 - 2.0 * uu : 0.0);
-  M[0][1] -= 2.0 * w * u[2]; M[0][2] += 2.0 * w * u[1];
-  M[1][0] += 2.0 * w * u[2]; M[1][2] -= 2.0 * w * u[0];
-  M[2][0] -= 2.0 * w * u[1]; M[2][1] += 2.0 * w * u[0];
+}
 
-  // projection
+// The observation part: residual (and Jacobian) of point X seen by a camera with
+// rotation R and parameters tail = cam[3..8] (translation, f, k1, k2). The residual
+// is float64; the Jacobian is computed in J from the float64 intermediates.
+template <bool kJac, typename J = double>
+__device__ __forceinline__ void snavely_project(const CamRot& R, const double tail[6], const double X[3], double ox,
+                                                double oy, ProjT<J>& o) {
+  const double w = R.w;
+  const double* u = R.u;
+  double c1[3];
+  cross3(u, X, c1);
+  const double uv[3] = {c1[0] * 2.0, c1[1] * 2.0, c1[2] * 2.0};
+  double c2[3];
+  cross3(u, uv, c2);
+  double p[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) p[i] = (X[i] + w * uv[i] + c2[i]) + tail[i];
   const double inv_p2 = 1.0 / p[2];
-  const double dxp[3] = {-inv_p2, 0.0, -xp * inv_p2};
-  const double dyp[3] = {0.0, -inv_p2, -yp * inv_p2};
-  const double g = k1 + 2.0 * k2 * r2;
-  const double dd_dx = 2.0 * xp * g, dd_dy = 2.0 * yp * g;
-  const double A00 = f * (dist + xp * dd_dx), A01 = f * xp * dd_dy;
-  const double A10 = f * yp * dd_dx, A11 = f * (dist + yp * dd_dy);
-  double Dp[2][3];
-#pragma unroll
-  for (int m = 0; m < 3; ++m) {
-    Dp[0][m] = A00 * dxp[m] + A01 * dyp[m];
-    Dp[1][m] = A10 * dxp[m] + A11 * dyp[m];
-  }
-#pragma unroll
-  for (int rrow = 0; rrow < 2; ++rrow) {
+  const double xp = -p[0] * inv_p2;
+  const double yp = -p[1] * inv_p2;
+  const double r2 = xp * xp + yp * yp;
+  const double k1 = tail[4], k2 = tail[5], f = tail[3];
+  const double dist = 1.0 + r2 * (k1 + k2 * r2);
+  const double fd = f * dist;
+  o.r[0] = fd * xp - ox;
+  o.r[1] = fd * yp - oy;
+  if constexpr (kJac) {
+    const J wj = (J)w;
+    const J uj[3] = {(J)u[0], (J)u[1], (J)u[2]};
+    const J Xj[3] = {(J)X[0], (J)X[1], (J)X[2]};
+    const J uvj[3] = {(J)uv[0], (J)uv[1], (J)uv[2]};
+    // dp/daa: d(X + w uv + u x uv) = dw uv + w duv + du x uv + u x duv, duv = 2 du x X
+    J dpa[3][3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      o.jc[rrow][j] = Dp[rrow][0] * dpa[0][j] + Dp[rrow][1] * dpa[1][j] + Dp[rrow][2] * dpa[2][j];
-      o.jc[rrow][3 + j] = Dp[rrow][j];
-      o.jp[rrow][j] = Dp[rrow][0] * M[0][j] + Dp[rrow][1] * M[1][j] + Dp[rrow][2] * M[2][j];
+      const J du[3] = {(J)R.dqn[1][j], (J)R.dqn[2][j], (J)R.dqn[3][j]};
+      J t1[3];
+      cross3(du, Xj, t1);
+      const J duv[3] = {(J)2 * t1[0], (J)2 * t1[1], (J)2 * t1[2]};
+      J t2[3], t3[3];
+      cross3(du, uvj, t2);
+      cross3(uj, duv, t3);
+      const J dw = (J)R.dqn[0][j];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) dpa[i][j] = dw * uvj[i] + wj * duv[i] + t2[i] + t3[i];
+    }
+    // dp/dX = I + 2 w [u]x + 2 [u]x^2, [u]x^2 = u u^T - (u.u) I
+    const J uu = uj[0] * uj[0] + uj[1] * uj[1] + uj[2] * uj[2];
+    J M[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) M[i][j] = (J)2 * uj[i] * uj[j] + (i == j ? (J)1 - (J)2 * uu : (J)0);
+    M[0][1] -= (J)2 * wj * uj[2]; M[0][2] += (J)2 * wj * uj[1];
+    M[1][0] += (J)2 * wj * uj[2]; M[1][2] -= (J)2 * wj * uj[0];
+    M[2][0] -= (J)2 * wj * uj[1]; M[2][1] += (J)2 * wj * uj[0];
+
+    // projection
+    const J ip = (J)inv_p2, xq = (J)xp, yq = (J)yp, r2q = (J)r2, fq = (J)f, k1q = (J)k1, k2q = (J)k2;
+    const J distq = (J)dist;
+    const J dxp[3] = {-ip, (J)0, -xq * ip};
+    const J dyp[3] = {(J)0, -ip, -yq * ip};
+    const J g = k1q + (J)2 * k2q * r2q;
+    const J dd_dx = (J)2 * xq * g, dd_dy = (J)2 * yq * g;
+    const J A00 = fq * (distq + xq * dd_dx), A01 = fq * xq * dd_dy;
+    const J A10 = fq * yq * dd_dx, A11 = fq * (distq + yq * dd_dy);
+    J Dp[2][3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      Dp[0][m] = A00 * dxp[m] + A01 * dyp[m];
+      Dp[1][m] = A10 * dxp[m] + A11 * dyp[m];
+    }
+#pragma unroll
+    for (int rrow = 0; rrow < 2; ++rrow) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        o.jc[rrow][j] = Dp[rrow][0] * dpa[0][j] + Dp[rrow][1] * dpa[1][j] + Dp[rrow][2] * dpa[2][j];
+        o.jc[rrow][3 + j] = Dp[rrow][j];
+        o.jp[rrow][j] = Dp[rrow][0] * M[0][j] + Dp[rrow][1] * M[1][j] + Dp[rrow][2] * M[2][j];
+      }
+    }
+    o.jc[0][6] = distq * xq; o.jc[1][6] = distq * yq;
+    o.jc[0][7] = fq * r2q * xq; o.jc[1][7] = fq * r2q * yq;
+    o.jc[0][8] = fq * r2q * r2q * xq; o.jc[1][8] = fq * r2q * r2q * yq;
+  }
+}
+
+template <bool kJac>
+__device__ __forceinline__ void snavely(const double* __restrict__ cam, const double X[3], double ox, double oy,
+                                        Proj& o) {
+  const double aa[3] = {cam[0], cam[1], cam[2]};
+  CamRot R;
+  camera_rotation<kJac>(aa, R);
+  const double tail[6] = {cam[3], cam[4], cam[5], cam[6], cam[7], cam[8]};
+  snavely_project<kJac>(R, tail, X, ox, oy, o);
+}
+
+// Camera frame record: 24 float64 per camera, [0] w, [1..3] u, [4..15] dqn (row-major
+// 4 x 3), [16..21] cam[3..8], [22..23] zero.
+constexpr int kFrame = 24;
+
+template <bool kJac>
+__device__ __forceinline__ void frame_store(double* __restrict__ f, const CamRot& R, const double* __restrict__ cam) {
+  f[0] = R.w; f[1] = R.u[0]; f[2] = R.u[1]; f[3] = R.u[2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) f[4 + 3 * i + j] = kJac ? R.dqn[i][j] : 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) f[16 + i] = cam[3 + i];
+  f[22] = 0.0; f[23] = 0.0;
+}
+
+template <bool kJac>
+__device__ __forceinline__ void frame_load(const double* __restrict__ f, CamRot& R, double tail[6]) {
+  const double2* f2 = reinterpret_cast<const double2*>(f);
+  double2 v = f2[0];
+  R.w = v.x; R.u[0] = v.y;
+  v = f2[1];
+  R.u[1] = v.x; R.u[2] = v.y;
+  if (kJac) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      v = f2[2 + i];
+      R.dqn[(2 * i) / 3][(2 * i) % 3] = v.x;
+      R.dqn[(2 * i + 1) / 3][(2 * i + 1) % 3] = v.y;
     }
   }
-  o.jc[0][6] = dist * xp; o.jc[1][6] = dist * yp;
-  o.jc[0][7] = f * r2 * xp; o.jc[1][7] = f * r2 * yp;
-  o.jc[0][8] = f * r2 * r2 * xp; o.jc[1][8] = f * r2 * r2 * yp;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    v = f2[8 + i];
+    tail[2 * i] = v.x;
+    tail[2 * i + 1] = v.y;
+  }
 }
 
 // Ceres corrector (losses.py:158-193) applied in place. Returns 0.5 rho0.
-template <bool kJac>
-__device__ __forceinline__ double robustify(const LossSpec& L, Proj& o, unsigned& err) {
+template <bool kJac, typename J = double>
+__device__ __forceinline__ double robustify(const LossSpec& L, ProjT<J>& o, unsigned& err) {
   const double s = o.r[0] * o.r[0] + o.r[1] * o.r[1];
   double r0, r1, r2;
   loss_eval(L, s, r0, r1, r2);
@@ -276,26 +363,28 @@ __device__ __forceinline__ double robustify(const LossSpec& L, Proj& o, unsigned
     alpha_s = alpha / s;
   }
   if (kJac) {
+    const J sq = (J)sqrt_rho1;
     if (alpha_s == 0.0) {
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
 #pragma unroll
-        for (int j = 0; j < 9; ++j) o.jc[i][j] *= sqrt_rho1;
+        for (int j = 0; j < 9; ++j) o.jc[i][j] *= sq;
 #pragma unroll
-        for (int j = 0; j < 3; ++j) o.jp[i][j] *= sqrt_rho1;
+        for (int j = 0; j < 3; ++j) o.jp[i][j] *= sq;
       }
     } else {
+      const J as = (J)alpha_s, ra = (J)o.r[0], rb = (J)o.r[1];
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
-        const double rTj = o.r[0] * o.jc[0][j] + o.r[1] * o.jc[1][j];
-        o.jc[0][j] = sqrt_rho1 * (o.jc[0][j] - alpha_s * o.r[0] * rTj);
-        o.jc[1][j] = sqrt_rho1 * (o.jc[1][j] - alpha_s * o.r[1] * rTj);
+        const J rTj = ra * o.jc[0][j] + rb * o.jc[1][j];
+        o.jc[0][j] = sq * (o.jc[0][j] - as * ra * rTj);
+        o.jc[1][j] = sq * (o.jc[1][j] - as * rb * rTj);
       }
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const double rTj = o.r[0] * o.jp[0][j] + o.r[1] * o.jp[1][j];
-        o.jp[0][j] = sqrt_rho1 * (o.jp[0][j] - alpha_s * o.r[0] * rTj);
-        o.jp[1][j] = sqrt_rho1 * (o.jp[1][j] - alpha_s * o.r[1] * rTj);
+        const J rTj = ra * o.jp[0][j] + rb * o.jp[1][j];
+        o.jp[0][j] = sq * (o.jp[0][j] - as * ra * rTj);
+        o.jp[1][j] = sq * (o.jp[1][j] - as * rb * rTj);
       }
     }
   }
@@ -336,7 +425,8 @@ __device__ __forceinline__ void load_rec_jp(const double* __restrict__ base, siz
 #pragma unroll
   for (int i = 0; i < 3; ++i) { const double2 t = __ldg(p + i); v[2 * i] = t.x; v[2 * i + 1] = t.y; }
 }
-__device__ __forceinline__ void store_rec(float* __restrict__ base, size_t slot, const Proj& o) {
+template <typename J>
+__device__ __forceinline__ void store_rec(float* __restrict__ base, size_t slot, const ProjT<J>& o) {
   float4* p = reinterpret_cast<float4*>(base + slot * kRec);
   float v[kRec];
 #pragma unroll

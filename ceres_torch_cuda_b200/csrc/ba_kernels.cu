@@ -46,6 +46,21 @@ constexpr int kCtrEval = 0, kCtrPoint = 1, kCtrCamera = 2, kCtrStep = 3, kCtrCam
 constexpr int kCtrBarCount = 8, kCtrBarGen = 9, kCtrBarFlag = 10, kCtrError = 12;
 
 constexpr int kWarpBlock = 256;  // threads per CTA of the slice-walking kernels
+// Resident CTAs per SM the evaluator and the step kernel are compiled for: a register
+// cap that trades a few spilled registers for twice (evaluator with Jacobian: 128
+// registers, 2 CTAs) or 1.5 times (step: 80 registers, 3 CTAs) the warps in flight;
+// both kernels wait on chains of dependent float64 operations, so more warps hide more
+// of that latency (measured on the 6.0M-observation problem: evaluator 0.62 -> 0.42 ms,
+// step 0.49 -> 0.45 ms).
+#ifndef CERES_B200_EVAL_MIN_BLOCKS
+#define CERES_B200_EVAL_MIN_BLOCKS 2
+#endif
+#ifndef CERES_B200_EVAL_NOJAC_MIN_BLOCKS
+#define CERES_B200_EVAL_NOJAC_MIN_BLOCKS 3
+#endif
+#ifndef CERES_B200_STEP_MIN_BLOCKS
+#define CERES_B200_STEP_MIN_BLOCKS 3
+#endif
 
 struct DevInfo {
   int sms = 0;
@@ -84,13 +99,34 @@ inline size_t red_area_bytes(const ceres_b200_ba_t& ba, const DevInfo& d) {
   return ((size_t)g * kRedSlots * sizeof(double) + 255) & ~(size_t)255;
 }
 
+// Camera frames (kFrame float64 per camera) follow the reduction area in the scratch.
+inline size_t frames_bytes(const ceres_b200_ba_t& ba) {
+  return ((size_t)(ba.num_cameras > 0 ? ba.num_cameras : 1) * kFrame * sizeof(double) + 255) & ~(size_t)255;
+}
+
 }  // namespace
 
 // ======================================================================================
 // Evaluation: residual, Jacobian, corrector
 // ======================================================================================
-template <typename T, bool kJac>
-__global__ void __launch_bounds__(kWarpBlock) k_evaluate(ceres_b200_ba_t ba, double* partials) {
+// Camera frames (the per-camera rotation part of the projection, see CamRot) of
+// cams[nc][9] into frames[nc][kFrame]; one thread per camera.
+template <bool kJac>
+__global__ void k_camera_frames(const double* __restrict__ cams, double* __restrict__ frames, int nc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const double* cam = cams + 9 * (size_t)c;
+  const double aa[3] = {cam[0], cam[1], cam[2]};
+  CamRot R;
+  camera_rotation<kJac>(aa, R);
+  frame_store<kJac>(frames + kFrame * (size_t)c, R, cam);
+}
+
+// kFrames: the cameras' rotation parts come from frames[nc][kFrame] (k_camera_frames
+// of ba.cameras); otherwise every observation computes its camera's rotation.
+template <typename T, bool kJac, bool kFrames>
+__global__ void __launch_bounds__(kWarpBlock, kJac ? CERES_B200_EVAL_MIN_BLOCKS : CERES_B200_EVAL_NOJAC_MIN_BLOCKS)
+k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ frames) {
   __shared__ double red[kWarpBlock / 32];
   const LossSpec L = loss_spec(ba);
   const int lane = threadIdx.x & 31;
@@ -116,8 +152,22 @@ __global__ void __launch_bounds__(kWarpBlock) k_evaluate(ceres_b200_ba_t ba, dou
       const int c = ba.slot_cam[slot];
       if (c < 0) continue;
       const double2 ob = reinterpret_cast<const double2*>(ba.slot_obs)[slot];
+      // Jacobian in float64, rounded to T when stored: a Jacobian computed in float32
+      // arithmetic (errors of ~1e-6 instead of the 6e-8 of rounding) made the mixed
+      // LM solves of the 6.0M-observation problem take 1.3x the iterations
       Proj o;
-      snavely<kJac>(ba.cameras + 9 * (size_t)c, X, ob.x, ob.y, o);
+      CamRot R;
+      double tail[6];
+      if (kFrames) {
+        frame_load<kJac>(frames + kFrame * (size_t)c, R, tail);
+      } else {
+        const double* cam = ba.cameras + 9 * (size_t)c;
+        const double aa[3] = {cam[0], cam[1], cam[2]};
+        camera_rotation<kJac>(aa, R);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) tail[i] = cam[3 + i];
+      }
+      snavely_project<kJac>(R, tail, X, ob.x, ob.y, o);
       cost += robustify<kJac>(L, o, err);
       reinterpret_cast<double2*>(ba.res)[slot] = make_double2(o.r[0], o.r[1]);
       if (kJac) {
@@ -212,58 +262,89 @@ __device__ __forceinline__ int tri9(int j, int l) {  // upper-triangle index, j 
   return j * 9 - (j * (j - 1)) / 2 + (l - j);
 }
 
+// The camera sums are float64 in both precisions. With the float32 store, float32
+// accumulators (168 registers, three CTAs per SM: 0.34 instead of 0.42 ms on the
+// 6.0M-observation problem) made the SCHUR_JACOBI blocks inaccurate enough to change
+// PCG iteration counts: the mixed LM solves then took 71-176 iterations to the target
+// (median 89, 9 runs) instead of 77-94 (median 90).
+
+// One entry of a camera's observation list with the data its update reads.
+template <typename T>
+struct CamObs {
+  int2 ent;  // (slot, sorted point)
+  T rv[kRec];
+  double2 r;
+};
+
+template <typename T>
+__device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ jac, int e,
+                                             CamObs<T>& o) {
+  o.ent = reinterpret_cast<const int2*>(ba.cam_entries)[e];
+  load_rec(jac, (size_t)o.ent.x, o.rv);
+  o.r = reinterpret_cast<const double2*>(ba.res)[o.ent.x];
+}
+
 // Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
 // into acc_out[c][72] (float64).
 template <typename T, bool kDup>
 __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba, double* __restrict__ acc_out) {
+  using A = double;
   __shared__ double sred[kCamAcc * (kCamBlock / 32)];
   const int c = blockIdx.x;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  double acc[kCamAcc];
+  A av[54];      // Schur block (upper triangle, 45), column sums (9)
+  double ag[18]; // gradient (9), reduced rhs (9)
 #pragma unroll
-  for (int i = 0; i < kCamAcc; ++i) acc[i] = 0.0;
+  for (int i = 0; i < 54; ++i) av[i] = (A)0;
+#pragma unroll
+  for (int i = 0; i < 18; ++i) ag[i] = 0.0;
   const bool cconst = ba.cam_const[c] != 0;
   const int e0 = ba.cam_offsets[c], e1 = ba.cam_offsets[c + 1];
   if (!cconst) {
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-      const int2 ent = reinterpret_cast<const int2*>(ba.cam_entries)[e];
-      const size_t slot = (size_t)ent.x;
-      const int q = ent.y;
-      T rv[kRec];
-      load_rec(jac, slot, rv);
-      const double2 r = reinterpret_cast<const double2*>(ba.res)[slot];
-      double wi[6];
+      CamObs<T> cur;
+      cam_obs_load(ba, jac, e, cur);
+      const size_t slot = (size_t)cur.ent.x;
+      const int q = cur.ent.y;
+      const T* rv = cur.rv;
+      const double2 r = cur.r;
+      A wi[6];
 #pragma unroll
-      for (int i = 0; i < 6; ++i) wi[i] = (double)winv[6 * (size_t)q + i];
+      for (int i = 0; i < 6; ++i) wi[i] = (A)winv[6 * (size_t)q + i];
       const double wg[3] = {ba.winv_ga[3 * (size_t)q], ba.winv_ga[3 * (size_t)q + 1], ba.winv_ga[3 * (size_t)q + 2]};
-      double jp0[3], jp1[3];
+      A jp0[3], jp1[3];
 #pragma unroll
-      for (int m = 0; m < 3; ++m) { jp0[m] = rv[18 + m]; jp1[m] = rv[21 + m]; }
+      for (int m = 0; m < 3; ++m) { jp0[m] = (A)rv[18 + m]; jp1[m] = (A)rv[21 + m]; }
       // P = Jp W^-1 (2x3); B = P Jp^T (2x2); a = Jp W^-1 g_a
-      double P0[3], P1[3];
-      sym3_mul(wi, jp0, P0);
-      sym3_mul(wi, jp1, P1);
-      const double B00 = P0[0] * jp0[0] + P0[1] * jp0[1] + P0[2] * jp0[2];
-      const double B01 = P0[0] * jp1[0] + P0[1] * jp1[1] + P0[2] * jp1[2];
-      const double B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
-      const double a0 = jp0[0] * wg[0] + jp0[1] * wg[1] + jp0[2] * wg[2];
-      const double a1 = jp1[0] * wg[0] + jp1[1] * wg[1] + jp1[2] * wg[2];
-      const double M00 = 1.0 - B00, M01 = -B01, M11 = 1.0 - B11;
-      double K0[9], K1[9];
+      A P0[3], P1[3];
+      P0[0] = wi[0] * jp0[0] + wi[1] * jp0[1] + wi[2] * jp0[2];
+      P0[1] = wi[1] * jp0[0] + wi[3] * jp0[1] + wi[4] * jp0[2];
+      P0[2] = wi[2] * jp0[0] + wi[4] * jp0[1] + wi[5] * jp0[2];
+      P1[0] = wi[0] * jp1[0] + wi[1] * jp1[1] + wi[2] * jp1[2];
+      P1[1] = wi[1] * jp1[0] + wi[3] * jp1[1] + wi[4] * jp1[2];
+      P1[2] = wi[2] * jp1[0] + wi[4] * jp1[1] + wi[5] * jp1[2];
+      const A B00 = P0[0] * jp0[0] + P0[1] * jp0[1] + P0[2] * jp0[2];
+      const A B01 = P0[0] * jp1[0] + P0[1] * jp1[1] + P0[2] * jp1[2];
+      const A B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
+      const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
+      const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
+      const A M00 = (A)1 - B00, M01 = -B01, M11 = (A)1 - B11;
+      A K0[9], K1[9];
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
-        const double c0 = rv[j], c1 = rv[9 + j];
+        const A c0 = (A)rv[j], c1 = (A)rv[9 + j];
         K0[j] = M00 * c0 + M01 * c1;
         K1[j] = M01 * c0 + M11 * c1;
-        acc[45 + j] += c0 * c0 + c1 * c1;
-        acc[54 + j] += c0 * r.x + c1 * r.y;
-        acc[63 + j] += c0 * (r.x + a0) + c1 * (r.y + a1);
+        av[45 + j] += c0 * c0 + c1 * c1;
+        const double d0 = (double)rv[j], d1 = (double)rv[9 + j];
+        ag[j] += d0 * r.x + d1 * r.y;
+        ag[9 + j] += d0 * (r.x + a0) + d1 * (r.y + a1);
       }
 #pragma unroll
       for (int j = 0; j < 9; ++j)
 #pragma unroll
-        for (int l = j; l < 9; ++l) acc[tri9(j, l)] += (double)rv[j] * K0[l] + (double)rv[9 + j] * K1[l];
+        for (int l = j; l < 9; ++l) av[tri9(j, l)] += (A)rv[j] * K0[l] + (A)rv[9 + j] * K1[l];
 
       if (kDup) {
         // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
@@ -275,16 +356,16 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
           if (slot2 == slot || ba.slot_cam[slot2] != c) continue;
           T rk[kRec];
           load_rec(jac, slot2, rk);
-          const double C00 = P0[0] * rk[18] + P0[1] * rk[19] + P0[2] * rk[20];
-          const double C01 = P0[0] * rk[21] + P0[1] * rk[22] + P0[2] * rk[23];
-          const double C10 = P1[0] * rk[18] + P1[1] * rk[19] + P1[2] * rk[20];
-          const double C11 = P1[0] * rk[21] + P1[1] * rk[22] + P1[2] * rk[23];
+          const A C00 = P0[0] * (A)rk[18] + P0[1] * (A)rk[19] + P0[2] * (A)rk[20];
+          const A C01 = P0[0] * (A)rk[21] + P0[1] * (A)rk[22] + P0[2] * (A)rk[23];
+          const A C10 = P1[0] * (A)rk[18] + P1[1] * (A)rk[19] + P1[2] * (A)rk[20];
+          const A C11 = P1[0] * (A)rk[21] + P1[1] * (A)rk[22] + P1[2] * (A)rk[23];
 #pragma unroll
           for (int j = 0; j < 9; ++j) {
-            const double t0 = (double)rv[j] * C00 + (double)rv[9 + j] * C10;
-            const double t1 = (double)rv[j] * C01 + (double)rv[9 + j] * C11;
+            const A t0 = (A)rv[j] * C00 + (A)rv[9 + j] * C10;
+            const A t1 = (A)rv[j] * C01 + (A)rv[9 + j] * C11;
 #pragma unroll
-            for (int l = j; l < 9; ++l) acc[tri9(j, l)] -= t0 * (double)rk[l] + t1 * (double)rk[9 + l];
+            for (int l = j; l < 9; ++l) av[tri9(j, l)] -= t0 * (A)rk[l] + t1 * (A)rk[9 + l];
           }
         }
       }
@@ -292,9 +373,14 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-  for (int i = 0; i < kCamAcc; ++i) {
-    const double v = warp_sum(acc[i]);
+  for (int i = 0; i < 54; ++i) {
+    const double v = warp_sum((double)av[i]);
     if (lane == 0) sred[i * nw + wid] = v;
+  }
+#pragma unroll
+  for (int i = 0; i < 18; ++i) {
+    const double v = warp_sum(ag[i]);
+    if (lane == 0) sred[(54 + i) * nw + wid] = v;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x) {
@@ -304,47 +390,111 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
   }
 }
 
-// Phase 2: one thread per camera forms the damping, the reduced rhs, the gradient
-// stats and the preconditioner block from the 72 sums.
+// Phase 2: one warp per camera forms the damping, the reduced rhs, the gradient stats
+// and the preconditioner block from the 72 sums. Lane i < 9 holds row i of the
+// damped Schur block S; the SCHUR_JACOBI inverse is the Cholesky factorisation and
+// the two triangular solves of block9_inverse, spread over the lanes (row i of L on
+// lane i, column c of the inverse on lane c) with the same operation order, so it
+// gives block9_inverse's result. A block that is not positive definite goes to
+// block9_inverse's pivoted Gauss-Jordan on lane 0 (linear.py:1156-1182 falls back
+// from Cholesky to a general solve the same way).
+constexpr int kFinishWarps = 4;  // cameras per CTA
+
 template <typename T>
-__global__ void __launch_bounds__(128) k_camera_finish(ceres_b200_ba_t ba, const double* __restrict__ acc_in,
-                                                      double inv_radius, double mn, double mx, int jacobi_scaling,
-                                                      int precond, double* partials) {
-  __shared__ double sred2[2 * (128 / 32)];
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_ba_t ba, const double* __restrict__ acc_in,
+                                                                     double inv_radius, double mn, double mx,
+                                                                     int jacobi_scaling, int precond, double* partials) {
+  constexpr unsigned kFull = 0xffffffffu;
+  __shared__ double sred2[2 * kFinishWarps];
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kFinishWarps + (threadIdx.x >> 5);
   double gmax = 0.0, gsq = 0.0;
-  if (c < ba.num_cameras) {
+  if (c < ba.num_cameras) {  // uniform in the warp
     const double* sacc = acc_in + (size_t)c * kCamAcc;
     T* __restrict__ pre = reinterpret_cast<T*>(ba.precond) + 81 * (size_t)c;
     double* dc = ba.cam_diag + 9 * (size_t)c;
     double* rh = ba.rhs + 9 * (size_t)c;
     if (ba.cam_const[c]) {
-      for (int j = 0; j < 9; ++j) { dc[j] = 0.0; rh[j] = 0.0; }
-      for (int i = 0; i < 81; ++i) pre[i] = (T)((i % 10 == 0) ? 1.0 : 0.0);
+      if (lane < 9) { dc[lane] = 0.0; rh[lane] = 0.0; }
+      for (int i = lane; i < 81; i += 32) pre[i] = (T)((i % 10 == 0) ? 1.0 : 0.0);
     } else {
-      double S[81], inv[81];
-      for (int j = 0; j < 9; ++j) {
-        const double col = jacobi_scaling ? sacc[45 + j] : 1.0;
-        dc[j] = fmin(fmax(col, mn), mx) * inv_radius;
-        rh[j] = -sacc[63 + j];
-        const double gj = sacc[54 + j];
-        gmax = fmax(gmax, fabs(gj));
-        gsq += gj * gj;
+      const int i = lane < 9 ? lane : 8;  // lanes 9..31 shadow row 8 and store nothing
+      const double col = jacobi_scaling ? sacc[45 + i] : 1.0;
+      const double di = fmin(fmax(col, mn), mx) * inv_radius;
+      if (lane < 9) {
+        dc[i] = di;
+        rh[i] = -sacc[63 + i];
+        const double gi = sacc[54 + i];
+        gmax = fabs(gi);
+        gsq = gi * gi;
       }
-      for (int j = 0; j < 9; ++j)
-        for (int l = j; l < 9; ++l) {
-          const double v = sacc[tri9(j, l)] + (j == l ? dc[j] : 0.0);
-          S[j * 9 + l] = v;
-          S[l * 9 + j] = v;
-        }
+      double a[9];  // row i of S = V + D
+#pragma unroll
+      for (int l = 0; l < 9; ++l) a[l] = sacc[l < i ? tri9(l, i) : tri9(i, l)] + (l == i ? di : 0.0);
       if (precond == CERES_B200_PRECOND_SCHUR_JACOBI) {
-        block9_inverse(S, inv);
-      } else {
-        for (int i = 0; i < 81; ++i) inv[i] = 0.0;
-        for (int j = 0; j < 9; ++j)
-          inv[j * 10] = (precond == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(S[j * 10], Eps<T>::v()) : 1.0;
+        double Lr[9];  // row i of L (entries 0..i)
+        bool pd = true;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+          double Lj[9];
+#pragma unroll
+          for (int k = 0; k < j; ++k) Lj[k] = __shfl_sync(kFull, Lr[k], j);
+          double d = __shfl_sync(kFull, a[j], j);
+#pragma unroll
+          for (int k = 0; k < j; ++k) d -= Lj[k] * Lj[k];
+          if (!(d > 0.0)) { pd = false; break; }  // every lane computed the same d
+          const double ljj = sqrt(d);
+          double sj = a[j];
+#pragma unroll
+          for (int k = 0; k < j; ++k) sj -= Lr[k] * Lj[k];
+          Lr[j] = (i == j) ? ljj : sj / ljj;
+        }
+        if (pd) {
+          double Lf[45];  // packed lower triangle of L: row r, column k at r (r + 1) / 2 + k
+#pragma unroll
+          for (int r = 0; r < 9; ++r)
+#pragma unroll
+            for (int k = 0; k <= r; ++k) Lf[r * (r + 1) / 2 + k] = __shfl_sync(kFull, Lr[k], r);
+          double y[9], x[9];
+#pragma unroll
+          for (int r = 0; r < 9; ++r) {
+            double sv = (r == lane) ? 1.0 : 0.0;
+#pragma unroll
+            for (int k = 0; k < r; ++k) sv -= Lf[r * (r + 1) / 2 + k] * y[k];
+            y[r] = sv / Lf[r * (r + 1) / 2 + r];
+          }
+#pragma unroll
+          for (int r = 8; r >= 0; --r) {
+            double sv = y[r];
+#pragma unroll
+            for (int k = r + 1; k < 9; ++k) sv -= Lf[k * (k + 1) / 2 + r] * x[k];
+            x[r] = sv / Lf[r * (r + 1) / 2 + r];
+          }
+          if (lane < 9) {
+#pragma unroll
+            for (int r = 0; r < 9; ++r) pre[r * 9 + lane] = (T)x[r];
+          }
+        } else if (lane == 0) {
+          double S[81], inv[81];
+          for (int j = 0; j < 9; ++j) {
+            const double dj = fmin(fmax(jacobi_scaling ? sacc[45 + j] : 1.0, mn), mx) * inv_radius;
+            for (int l = j; l < 9; ++l) {
+              const double v = sacc[tri9(j, l)] + (j == l ? dj : 0.0);
+              S[j * 9 + l] = v;
+              S[l * 9 + j] = v;
+            }
+          }
+          block9_inverse(S, inv);
+          for (int k = 0; k < 81; ++k) pre[k] = (T)inv[k];
+        }
+      } else if (lane < 9) {
+        double sii = 0.0;
+#pragma unroll
+        for (int l = 0; l < 9; ++l) sii = (l == i) ? a[l] : sii;
+        const double v = (precond == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(sii, Eps<T>::v()) : 1.0;
+#pragma unroll
+        for (int l = 0; l < 9; ++l) pre[i * 9 + l] = (T)(l == i ? v : 0.0);
       }
-      for (int i = 0; i < 81; ++i) pre[i] = (T)inv[i];
     }
   }
   double v[2] = {gmax, gsq};
@@ -796,7 +946,7 @@ __global__ void k_camera_step(ceres_b200_ba_t ba, double* partials) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kWarpBlock) k_step(ceres_b200_ba_t ba, double* partials) {
+__global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step(ceres_b200_ba_t ba, double* partials, const double* __restrict__ frames) {
   __shared__ double red[5 * (kWarpBlock / 32)];
   const LossSpec L = loss_spec(ba);
   const int lane = threadIdx.x & 31;
@@ -886,7 +1036,10 @@ __global__ void __launch_bounds__(kWarpBlock) k_step(ceres_b200_ba_t ba, double*
       model += 0.5 * (r.x * r.x + r.y * r.y) - 0.5 * (a0 * a0 + a1 * a1);
       const double2 ob = reinterpret_cast<const double2*>(ba.slot_obs)[slot];
       Proj o;
-      snavely<false>(ba.cand_cameras + 9 * (size_t)c, Xc, ob.x, ob.y, o);
+      CamRot R;
+      double tail[6];
+      frame_load<false>(frames + kFrame * (size_t)c, R, tail);  // frames of the candidate cameras
+      snavely_project<false>(R, tail, Xc, ob.x, ob.y, o);
       cand += robustify<false>(L, o, err);
     }
   }
@@ -1129,7 +1282,7 @@ struct PcgLayout {
   int cams_per_cta = 0;
   int smem_vectors = 0;
   size_t dyn_smem = 0;
-  size_t aux = 0, cam_acc = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0, total = 0;
+  size_t frames = 0, aux = 0, cam_acc = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0, total = 0;
 };
 
 template <typename T>
@@ -1152,6 +1305,8 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   const int needed_for_cams = ba.num_cameras > 0 ? ba.num_cameras : 1;
   L.cams_per_cta = (needed_for_cams + L.grid - 1) / L.grid;
   size_t off = red_area_bytes(ba, d);
+  L.frames = off;
+  off += frames_bytes(ba);
   L.aux = off;
   off += 256;
   L.cam_acc = off;
@@ -1314,14 +1469,24 @@ int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* s
   if (!valid(ba) || !ba->scratch || (with_jacobian && !ba->point_raw)) return CERES_B200_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   const DevInfo d = device_info();
+  const size_t red = red_area_bytes(*ba, d);
+  if (ba->scratch_bytes < 0 || (size_t)ba->scratch_bytes < red + frames_bytes(*ba)) return CERES_B200_EINVAL;
   const int grid = slice_grid(*ba, d);
   double* partials = reinterpret_cast<double*>(ba->scratch);
+  double* frames = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + red);
+  const int nc = ba->num_cameras;
+  if (nc > 0) {
+    count_launch();
+    if (with_jacobian) k_camera_frames<true><<<(nc + 127) / 128, 128, 0, st>>>(ba->cameras, frames, nc);
+    else k_camera_frames<false><<<(nc + 127) / 128, 128, 0, st>>>(ba->cameras, frames, nc);
+  }
+  count_launch();
   if (ba->precision == CERES_B200_FP32) {
-    if (with_jacobian) { count_launch(); k_evaluate<float, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
-    else { count_launch(); k_evaluate<float, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    if (with_jacobian) k_evaluate<float, true, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
+    else k_evaluate<float, false, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
   } else {
-    if (with_jacobian) { count_launch(); k_evaluate<double, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
-    else { count_launch(); k_evaluate<double, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    if (with_jacobian) k_evaluate<double, true, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
+    else k_evaluate<double, false, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
   }
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
@@ -1388,12 +1553,14 @@ int ceres_b200_ba_evaluate_noalloc(const ceres_b200_ba_t* ba, int with_jacobian,
   if (rc) return rc;
   // every CTA writes its own slot before the last one folds them, so the shared array
   // needs no clearing between calls; the ticket counter is the caller's (counters[])
+  // no scratch for camera frames here: each observation computes its camera's rotation
+  // (the same arithmetic as the frames, so the results are those of ceres_b200_ba_evaluate)
   if (ba->precision == CERES_B200_FP32) {
-    if (with_jacobian) { count_launch(); k_evaluate<float, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
-    else { count_launch(); k_evaluate<float, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    if (with_jacobian) { count_launch(); k_evaluate<float, true, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
+    else { count_launch(); k_evaluate<float, false, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
   } else {
-    if (with_jacobian) { count_launch(); k_evaluate<double, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
-    else { count_launch(); k_evaluate<double, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+    if (with_jacobian) { count_launch(); k_evaluate<double, true, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
+    else { count_launch(); k_evaluate<double, false, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
   }
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
@@ -1439,13 +1606,13 @@ int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, doub
   if (ba->precision == CERES_B200_FP32) {
     if (ba->has_duplicate_cameras) k_camera_reduce<float, true><<<nc, kCamBlock, 0, st>>>(*ba, acc);
     else k_camera_reduce<float, false><<<nc, kCamBlock, 0, st>>>(*ba, acc);
-    k_camera_finish<float><<<(nc + 127) / 128, 128, 0, st>>>(*ba, acc, inv_radius, min_diagonal, max_diagonal,
-                                                               jacobi_scaling, preconditioner, partials);
+    k_camera_finish<float><<<(nc + kFinishWarps - 1) / kFinishWarps, 32 * kFinishWarps, 0, st>>>(
+        *ba, acc, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, preconditioner, partials);
   } else {
     if (ba->has_duplicate_cameras) k_camera_reduce<double, true><<<nc, kCamBlock, 0, st>>>(*ba, acc);
     else k_camera_reduce<double, false><<<nc, kCamBlock, 0, st>>>(*ba, acc);
-    k_camera_finish<double><<<(nc + 127) / 128, 128, 0, st>>>(*ba, acc, inv_radius, min_diagonal, max_diagonal,
-                                                                jacobi_scaling, preconditioner, partials);
+    k_camera_finish<double><<<(nc + kFinishWarps - 1) / kFinishWarps, 32 * kFinishWarps, 0, st>>>(
+        *ba, acc, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, preconditioner, partials);
   }
   return check_launch();
 }
@@ -1486,9 +1653,15 @@ int ceres_b200_ba_step(const ceres_b200_ba_t* ba, void* stream) {
   b2.stats = cam_stats;
   count_launch();
   k_camera_step<<<cgrid, 256, 0, st>>>(b2, partials);
+  double* frames = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + L.frames);
+  const int nc = ba->num_cameras;
+  if (nc > 0) {
+    count_launch();
+    k_camera_frames<false><<<(nc + 127) / 128, 128, 0, st>>>(ba->cand_cameras, frames, nc);
+  }
   const int grid = slice_grid(*ba, d);
-  if (ba->precision == CERES_B200_FP32) { count_launch(); k_step<float><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
-  else { count_launch(); k_step<double><<<grid, kWarpBlock, 0, st>>>(*ba, partials); }
+  if (ba->precision == CERES_B200_FP32) { count_launch(); k_step<float><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames); }
+  else { count_launch(); k_step<double><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames); }
   // STEP_SQ_C and the camera non-finite count into the shared stats
   count_launch();
   k_add_nonfinite<<<1, 1, 0, st>>>(ba->stats, cam_stats + CERES_B200_STAT_NONFINITE);
