@@ -13,6 +13,7 @@ from .cuda_backends import (CUDA_BACKEND_NAMES, CudaExtensionInfo, cuda_block_sc
                             get_cuda_extension_info, get_torch_cuda_backend_info, load_cuda_extension,
                             register_cuda_extension_backends, register_cuda_sparse_backends,
                             torch_cuda_backend_available, unregister_cuda_sparse_backends)
+from .batch import BatchSolver, build_batch_layout, solve_batch
 from .engine import BAEngine, build_layout
 from .linear import (LinearSolverResult, LinearSolverSummary, OptionalBackendUnavailable, clear_optional_backends,
                      get_optional_backend, register_optional_backend, solve_linear_system,

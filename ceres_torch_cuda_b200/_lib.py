@@ -16,7 +16,7 @@ c_int64 = ctypes.c_int64
 c_double = ctypes.c_double
 c_void_p = ctypes.c_void_p
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 EINVAL = -1
@@ -71,6 +71,46 @@ class BAStruct(ctypes.Structure):
 
 _P = ctypes.POINTER(BAStruct)
 
+# batched solves (ceres_b200_batch_t)
+BATCH_RESULT = 16
+BATCH_TRACE = 10
+(BR_INITIAL_COST, BR_FINAL_COST, BR_RECORDS, BR_TERMINATION, BR_MESSAGE, BR_SUCCESSFUL, BR_UNSUCCESSFUL,
+ BR_JACOBIAN_EVALS, BR_RESIDUAL_EVALS, BR_LINEAR_SOLVES, BR_ERROR, BR_FINAL_GMAX) = range(12)
+(BT_COST, BT_COST_CHANGE, BT_GMAX, BT_GNORM, BT_STEP_NORM, BT_RHO, BT_RADIUS, BT_LINEAR_ITERATIONS,
+ BT_FLAGS) = range(9)
+TERM_CONVERGENCE, TERM_NO_CONVERGENCE, TERM_FAILURE = range(3)
+MESSAGES = ("Gradient tolerance reached.", "Maximum iterations reached.", "Too many invalid trust-region steps.",
+            "Parameter tolerance reached.", "Function tolerance reached.", "Minimum trust-region radius reached.")
+
+
+class BatchStruct(ctypes.Structure):
+    """Mirror of ``ceres_b200_batch_t``."""
+
+    _fields_ = [
+        ("num_problems", c_int32), ("precision", c_int32), ("max_cameras", c_int32),
+        ("has_duplicate_cameras", c_int32), ("loss_kind", c_int32), ("inner_loss_kind", c_int32),
+        ("loss_a", c_double), ("loss_b", c_double), ("loss_scale", c_double),
+        ("inner_a", c_double), ("inner_b", c_double), ("inner_scale", c_double),
+        ("max_num_iterations", c_int32), ("min_linear_solver_iterations", c_int32),
+        ("max_linear_solver_iterations", c_int32), ("preconditioner", c_int32),
+        ("jacobi_scaling", c_int32), ("max_consecutive_invalid_steps", c_int32),
+        ("max_refinements", c_int32), ("max_trace", c_int32),
+        ("function_tolerance", c_double), ("gradient_tolerance", c_double), ("parameter_tolerance", c_double),
+        ("min_relative_decrease", c_double), ("initial_radius", c_double), ("max_radius", c_double),
+        ("min_radius", c_double), ("min_lm_diagonal", c_double), ("max_lm_diagonal", c_double), ("eta", c_double),
+        ("cam_off", c_void_p), ("slice_off", c_void_p),
+        ("slice_base", c_void_p), ("slice_len", c_void_p), ("slot_cam", c_void_p), ("slot_obs", c_void_p),
+        ("cam_offsets", c_void_p), ("cam_entries", c_void_p), ("cam_const", c_void_p), ("pt_const", c_void_p),
+        ("cameras", c_void_p), ("points", c_void_p), ("cand_cameras", c_void_p), ("cand_points", c_void_p),
+        ("jac", c_void_p), ("res", c_void_p), ("point_raw", c_void_p), ("winv", c_void_p), ("winv_ga", c_void_p),
+        ("step_points", c_void_p), ("cam_diag", c_void_p), ("precond", c_void_p), ("rhs", c_void_p),
+        ("step_cameras", c_void_p), ("cam_acc", c_void_p), ("frames", c_void_p), ("pcg", c_void_p),
+        ("result", c_void_p), ("trace", c_void_p), ("queue", c_void_p),
+    ]
+
+
+_PB = ctypes.POINTER(BatchStruct)
+
 # name -> (restype, argtypes); every symbol include/ceres_b200.h declares
 SIGNATURES = {
     "ceres_b200_abi_version": (c_int32, []),
@@ -87,6 +127,8 @@ SIGNATURES = {
     "ceres_b200_dense_schur_bytes": (c_int32, [_P, ctypes.POINTER(c_int64)]),
     "ceres_b200_ba_dense_schur_solve": (c_int32, [_P, c_void_p, c_void_p]),
     "ceres_b200_dense_cholesky_solve": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    "ceres_b200_batch_struct_bytes": (c_int32, []),
+    "ceres_b200_batch_solve": (c_int32, [_PB, c_int32, c_int32, c_void_p]),
 }
 
 _LIB: ctypes.CDLL | None = None
@@ -120,6 +162,8 @@ def load(*, build_if_missing: bool = False) -> ctypes.CDLL:
         raise NativeLibraryError(f"{path} has ABI {lib.ceres_b200_abi_version()}, expected {ABI_VERSION}")
     if lib.ceres_b200_ba_struct_bytes() != ctypes.sizeof(BAStruct):
         raise NativeLibraryError("ceres_b200_ba_t layout differs between the library and this binding")
+    if lib.ceres_b200_batch_struct_bytes() != ctypes.sizeof(BatchStruct):
+        raise NativeLibraryError("ceres_b200_batch_t layout differs between the library and this binding")
     _LIB = lib
     return lib
 

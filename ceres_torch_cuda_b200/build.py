@@ -17,7 +17,7 @@ CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 LIBDIR = PKG / "lib"
 LIBNAME = "libceres_b200.so"
-SOURCES = ["ba_kernels.cu"]
+SOURCES = ["ba_kernels.cu", "ba_batch.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

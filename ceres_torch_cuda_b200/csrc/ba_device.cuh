@@ -31,6 +31,9 @@ __device__ __forceinline__ double softplus(double x) {
   return x > 20.0 ? x : log1p(exp(x));
 }
 
+// The divisions of the formulas are written as products with one reciprocal each
+// (a float64 division is a long instruction sequence on the critical path of the
+// evaluator); the results differ from the quotient forms by an ulp or two.
 __device__ inline void loss_base(int kind, double a, double b, double s, double& r0, double& r1, double& r2) {
   switch (kind) {
     case CERES_B200_LOSS_HUBER: {
@@ -38,35 +41,42 @@ __device__ inline void loss_base(int kind, double a, double b, double s, double&
       if (s <= b2) { r0 = s; r1 = 1.0; r2 = 0.0; }
       else {
         const double sq = sqrt(fmax(s, kTiny64));
+        const double isq = 1.0 / sq;
         r0 = 2.0 * a * sq - b2;
-        r1 = a / sq;
-        r2 = -0.5 * a / (sq * s);
+        r1 = a * isq;
+        r2 = -0.5 * a * isq / s;
       }
       return;
     }
     case CERES_B200_LOSS_SOFTLONE: {
       const double b2 = a * a;
-      const double z = 1.0 + s / b2;
+      const double ib2 = 1.0 / b2;
+      const double z = 1.0 + s * ib2;
       const double sz = sqrt(z);
+      const double isz = 1.0 / sz;
       r0 = 2.0 * b2 * (sz - 1.0);
-      r1 = 1.0 / sz;
-      r2 = -0.5 / (b2 * z * sz);
+      r1 = isz;
+      r2 = -0.5 * ib2 * isz * isz * isz;
       return;
     }
     case CERES_B200_LOSS_CAUCHY: {
       const double b2 = a * a;
-      const double z = 1.0 + s / b2;
+      const double ib2 = 1.0 / b2;
+      const double z = 1.0 + s * ib2;
+      const double iz = 1.0 / z;
       r0 = b2 * log(z);
-      r1 = 1.0 / z;
-      r2 = -1.0 / (b2 * z * z);
+      r1 = iz;
+      r2 = -ib2 * iz * iz;
       return;
     }
     case CERES_B200_LOSS_ARCTAN: {
-      const double z = s / a;
+      const double ia = 1.0 / a;
+      const double z = s * ia;
       const double den = 1.0 + z * z;
+      const double iden = 1.0 / den;
       r0 = a * atan(z);
-      r1 = 1.0 / den;
-      r2 = -2.0 * z / (a * den * den);
+      r1 = iden;
+      r2 = -2.0 * z * ia * iden * iden;
       return;
     }
     case CERES_B200_LOSS_TOLERANT: {
@@ -79,14 +89,15 @@ __device__ inline void loss_base(int kind, double a, double b, double s, double&
     }
     case CERES_B200_LOSS_TUKEY: {
       const double a2 = a * a;
-      const double z = s / a2;
+      const double ia2 = 1.0 / a2;
+      const double z = s * ia2;
       const double inner = 1.0 - z;
       if (s <= a2) {
-        r0 = (a2 / 3.0) * (1.0 - inner * inner * inner);
+        r0 = (a2 * (1.0 / 3.0)) * (1.0 - inner * inner * inner);
         r1 = inner * inner;
-        r2 = -2.0 * inner / a2;
+        r2 = -2.0 * inner * ia2;
       } else {
-        r0 = a2 / 3.0; r1 = 0.0; r2 = 0.0;
+        r0 = a2 * (1.0 / 3.0); r1 = 0.0; r2 = 0.0;
       }
       return;
     }
@@ -358,8 +369,10 @@ __device__ __forceinline__ double robustify(const LossSpec& L, ProjT<J>& o, unsi
   double rscale = sqrt_rho1, alpha_s = 0.0;
   if (s > 0.0 && r2 > 0.0) {
     if (r1 <= 0.0) err |= CERES_B200_DEVERR_LOSS;
-    const double alpha = 1.0 - sqrt(1.0 + 2.0 * s * r2 / r1);
-    rscale = sqrt_rho1 / (1.0 - alpha);
+    // alpha = 1 - sqrt(1 + 2 s rho''/rho'); 1 - alpha is that square root
+    const double root = sqrt(1.0 + 2.0 * s * r2 / r1);
+    const double alpha = 1.0 - root;
+    rscale = sqrt_rho1 / root;
     alpha_s = alpha / s;
   }
   if (kJac) {

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define CERES_B200_ABI_VERSION 2
+#define CERES_B200_ABI_VERSION 3
 
 /* status codes */
 #define CERES_B200_OK 0
@@ -262,6 +262,125 @@ int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, voi
  */
 int ceres_b200_dense_cholesky_solve(double* H, const double* rhs, double* x, int64_t n, uint32_t* flags,
                                     void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * Batched solves: many independent bundle-adjustment problems in one persistent launch.
+ *
+ * Each CTA takes whole problems from a work counter (queue[0], zeroed by the caller)
+ * and runs the complete Levenberg-Marquardt solve of one problem at a time on the
+ * device: evaluation, Schur assembly, implicit-Schur PCG, step and the trust-region
+ * decisions of ceres-torch's solver.py:35-357 (monotonic steps, ITERATIVE_SCHUR).
+ * No host round trip happens between iterations; a problem's result does not depend
+ * on the other problems of the batch. This has no counterpart in the reference, which
+ * solves one problem per tc.solve call.
+ *
+ * Problems are concatenated: problem b owns cameras [cam_off[b], cam_off[b+1]),
+ * slices [slice_off[b], slice_off[b+1]) and the sorted points 32 * slice_off[b] ...
+ * of the same sliced-ELL layout as ceres_b200_ba_t (slot_cam holds the camera index
+ * local to the problem; cam_entries hold (global slot, global sorted point)).
+ * ---------------------------------------------------------------------------------- */
+#define CERES_B200_BATCH_RESULT 16 /* float64 per problem in result[] */
+#define CERES_B200_BATCH_TRACE 10  /* float64 per iteration record in trace[] */
+
+enum { /* result[b * CERES_B200_BATCH_RESULT + i] */
+  CERES_B200_BR_INITIAL_COST = 0,
+  CERES_B200_BR_FINAL_COST = 1,
+  CERES_B200_BR_RECORDS = 2,          /* iteration records written (iteration 0 included) */
+  CERES_B200_BR_TERMINATION = 3,      /* CERES_B200_TERM_* */
+  CERES_B200_BR_MESSAGE = 4,          /* CERES_B200_MSG_* */
+  CERES_B200_BR_SUCCESSFUL = 5,
+  CERES_B200_BR_UNSUCCESSFUL = 6,
+  CERES_B200_BR_JACOBIAN_EVALS = 7,
+  CERES_B200_BR_RESIDUAL_EVALS = 8,
+  CERES_B200_BR_LINEAR_SOLVES = 9,
+  CERES_B200_BR_ERROR = 10,           /* OR of CERES_B200_DEVERR_* bits */
+  CERES_B200_BR_FINAL_GMAX = 11
+};
+enum { /* trace[(b * max_trace + k) * CERES_B200_BATCH_TRACE + i] */
+  CERES_B200_BT_COST = 0,
+  CERES_B200_BT_COST_CHANGE = 1,
+  CERES_B200_BT_GMAX = 2,
+  CERES_B200_BT_GNORM = 3,
+  CERES_B200_BT_STEP_NORM = 4,
+  CERES_B200_BT_RHO = 5,
+  CERES_B200_BT_RADIUS = 6,
+  CERES_B200_BT_LINEAR_ITERATIONS = 7,
+  CERES_B200_BT_FLAGS = 8             /* bit 0 valid, bit 1 successful, bit 2 nonmonotonic */
+};
+enum { CERES_B200_TERM_CONVERGENCE = 0, CERES_B200_TERM_NO_CONVERGENCE = 1, CERES_B200_TERM_FAILURE = 2 };
+enum {
+  CERES_B200_MSG_GRADIENT = 0,        /* "Gradient tolerance reached." */
+  CERES_B200_MSG_MAX_ITERATIONS = 1,  /* "Maximum iterations reached." */
+  CERES_B200_MSG_INVALID_STEPS = 2,   /* "Too many invalid trust-region steps." */
+  CERES_B200_MSG_PARAMETER = 3,       /* "Parameter tolerance reached." */
+  CERES_B200_MSG_FUNCTION = 4,        /* "Function tolerance reached." */
+  CERES_B200_MSG_MIN_RADIUS = 5       /* "Minimum trust-region radius reached." */
+};
+
+typedef struct ceres_b200_batch_t {
+  int32_t num_problems;
+  int32_t precision;            /* CERES_B200_FP64 or CERES_B200_FP32 (Jacobian store and PCG) */
+  int32_t max_cameras;          /* largest camera count of a problem (sizes the shared memory) */
+  int32_t has_duplicate_cameras;
+  int32_t loss_kind;
+  int32_t inner_loss_kind;
+  double loss_a, loss_b, loss_scale, inner_a, inner_b, inner_scale;
+  /* SolverOptions (types.py) */
+  int32_t max_num_iterations;
+  int32_t min_linear_solver_iterations;
+  int32_t max_linear_solver_iterations;
+  int32_t preconditioner;       /* CERES_B200_PRECOND_* */
+  int32_t jacobi_scaling;
+  int32_t max_consecutive_invalid_steps;
+  int32_t max_refinements;      /* float64 refinement passes after a float32 PCG that missed eta */
+  int32_t max_trace;            /* iteration records kept per problem */
+  double function_tolerance, gradient_tolerance, parameter_tolerance, min_relative_decrease;
+  double initial_radius, max_radius, min_radius, min_lm_diagonal, max_lm_diagonal, eta;
+  /* per-problem offsets, num_problems + 1 entries each */
+  const int32_t* cam_off;
+  const int32_t* slice_off;
+  /* layout (concatenated; see above) */
+  const int32_t* slice_base;
+  const int32_t* slice_len;
+  const int32_t* slot_cam;
+  const double* slot_obs;
+  const int32_t* cam_offsets;   /* [total cameras + 1], into cam_entries */
+  const int32_t* cam_entries;   /* [entries][2] */
+  const uint8_t* cam_const;
+  const uint8_t* pt_const;
+  /* state (float64 unless noted) */
+  double* cameras;              /* [total cameras][9], solved in place */
+  double* points;               /* [32 * total slices][3] sorted order, solved in place */
+  double* cand_cameras;
+  double* cand_points;
+  void* jac;                    /* [slots][24] float or double */
+  double* res;                  /* [slots][2] */
+  double* point_raw;            /* [points][9] */
+  void* winv;                   /* [points][6] float or double */
+  double* winv_ga;              /* [points][3] */
+  double* step_points;          /* [points][3] */
+  double* cam_diag;             /* [cameras][9] */
+  void* precond;                /* [cameras][81] float or double */
+  double* rhs;                  /* [cameras][9] */
+  double* step_cameras;         /* [cameras][9] */
+  double* cam_acc;              /* [cameras][72] */
+  double* frames;               /* [cameras][24] */
+  double* pcg;                  /* [7][9 * total cameras]: x, r, z, p, Ap, refinement residual, correction */
+  double* result;               /* [num_problems][CERES_B200_BATCH_RESULT] */
+  double* trace;                /* [num_problems][max_trace][CERES_B200_BATCH_TRACE] */
+  uint32_t* queue;              /* [1] work counter, zero before the launch */
+} ceres_b200_batch_t;
+
+/* sizeof(ceres_b200_batch_t) as compiled into the library (binding check). */
+int ceres_b200_batch_struct_bytes(void);
+
+/*
+ * Solves every problem of the batch in one persistent launch. Shapes (threads_per_cta,
+ * ctas_per_sm): (128, 1|2), (128, 4), (256, 1), (256, 2), (512, 1); ctas_per_sm sets
+ * the register cap, 0 picks (256, 1). Asynchronous on stream; results appear in
+ * result/trace and the parameters are updated in place.
+ */
+int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta, int ctas_per_sm, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,121 @@
+"""Batched solves (one persistent launch for many problems).
+
+CPU: the concatenated layout gives every problem the layout its single-problem
+solve would use (same slices, same slot order, same camera-major lists).
+GPU: each problem of a batch ends where its own ``tc.solve`` ends (float64: final
+cost 1e-8 relative, termination and iteration count equal up to +-2, parameters
+1e-5; mixed: final cost within 1e-6 of the float64 single solve), and a problem's
+result in a batch of one equals its result in the mix (1e-8 relative).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from ceres_torch_cuda_b200 import synthetic as S
+from ceres_torch_cuda_b200.batch import build_batch_layout
+from ceres_torch_cuda_b200.engine import build_layout
+
+
+def _concat(datas):
+    cam_counts = np.array([d.num_cameras for d in datas], dtype=np.int64)
+    pt_counts = np.array([d.num_points for d in datas], dtype=np.int64)
+    co = np.concatenate([[0], np.cumsum(cam_counts)])
+    po = np.concatenate([[0], np.cumsum(pt_counts)])
+    ci = torch.cat([torch.as_tensor(d.camera_index, dtype=torch.int64) + int(co[i]) for i, d in enumerate(datas)])
+    pi = torch.cat([torch.as_tensor(d.point_index, dtype=torch.int64) + int(po[i]) for i, d in enumerate(datas)])
+    obs = torch.cat([torch.as_tensor(d.observations) for d in datas])
+    return cam_counts, pt_counts, co, po, ci, pi, obs
+
+
+def test_batch_layout_matches_single_problem_layouts():
+    datas = S.make_batched_instances(5, seed=3, max_points=150)
+    cam_counts, pt_counts, co, po, ci, pi, obs = _concat(datas)
+    L = build_batch_layout(cam_counts, pt_counts, ci, pi, obs)
+    soff = L.slice_off.numpy()
+    assert (L.cam_off.numpy() == co).all()
+    for b, d in enumerate(datas):
+        one = build_layout(torch.as_tensor(d.camera_index), torch.as_tensor(d.point_index),
+                           torch.as_tensor(d.observations), d.num_cameras, d.num_points)
+        s0, s1 = soff[b], soff[b + 1]
+        assert s1 - s0 == one.num_slices
+        np.testing.assert_array_equal(L.slice_len.numpy()[s0:s1], one.slice_len.numpy())
+        base0 = int(L.slice_base.numpy()[s0])
+        np.testing.assert_array_equal(L.slice_base.numpy()[s0:s1] - base0, one.slice_base.numpy())
+        nslot = one.num_slots
+        np.testing.assert_array_equal(L.slot_cam.numpy()[base0:base0 + nslot], one.slot_cam.numpy()[:nslot])
+        np.testing.assert_array_equal(L.slot_obs.numpy()[base0:base0 + nslot], one.slot_obs.numpy()[:nslot])
+        lp = L.lane_point.numpy()[32 * s0:32 * s1]
+        ref = one.lane_point.numpy()
+        np.testing.assert_array_equal(np.where(lp >= 0, lp - po[b], -1), ref)
+        off = L.cam_offsets.numpy()
+        ent = L.cam_entries.numpy()
+        for c in range(d.num_cameras):
+            e = ent[off[co[b] + c]:off[co[b] + c + 1]]
+            e1 = one.cam_entries.numpy()[one.cam_offsets.numpy()[c]:one.cam_offsets.numpy()[c + 1]]
+            np.testing.assert_array_equal(e[:, 0] - base0, e1[:, 0])
+            np.testing.assert_array_equal(e[:, 1] - 32 * s0, e1[:, 1])
+
+
+def _problems(datas, loss=None):
+    import ceres_torch_cuda_b200 as tc
+    return [tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, d.observations, d.camera_index,
+                                                   d.point_index, loss=loss) for d in datas]
+
+
+def _options(max_iterations=30):
+    import ceres_torch_cuda_b200 as tc
+    return tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                            preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI,
+                            max_num_iterations=max_iterations)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_matches_single_solves(precision):
+    import ceres_torch_cuda_b200 as tc
+    datas = S.make_batched_instances(6, seed=11, max_points=300)
+    singles = _problems(datas)
+    ref = [tc.solve(_options(), p, precision="fp64") for p in singles]
+    batch = _problems(datas)
+    got = tc.solve_batch(_options(), batch, precision=precision)
+    for r, g, ps, pb in zip(ref, got, singles, batch):
+        if precision == "fp64":
+            np.testing.assert_allclose(g.final_cost, r.final_cost, rtol=1e-8)
+            assert g.termination_type == r.termination_type
+            assert abs(len(g.iterations) - len(r.iterations)) <= 2
+            np.testing.assert_allclose(pb.cameras.cpu().numpy(), ps.cameras.cpu().numpy(), rtol=1e-5, atol=1e-7)
+            np.testing.assert_allclose(pb.points.cpu().numpy(), ps.points.cpu().numpy(), rtol=1e-5, atol=1e-7)
+        else:
+            assert g.final_cost <= r.final_cost * (1 + 1e-6)
+            assert g.final_cost >= r.final_cost * (1 - 1e-6)
+        assert g.initial_cost == pytest.approx(r.initial_cost, rel=1e-12)
+        assert g.iterations[0].cost == pytest.approx(r.iterations[0].cost, rel=1e-12)
+
+
+@pytest.mark.gpu
+def test_batch_result_alone_equals_result_in_the_mix():
+    import ceres_torch_cuda_b200 as tc
+    datas = S.make_batched_instances(8, seed=5, max_points=200)
+    mix = tc.solve_batch(_options(), _problems(datas), precision="fp64")
+    for k in (0, 5):
+        alone = tc.solve_batch(_options(), _problems([datas[k]]), precision="fp64")[0]
+        np.testing.assert_allclose(alone.final_cost, mix[k].final_cost, rtol=1e-8)
+        assert abs(len(alone.iterations) - len(mix[k].iterations)) <= 2
+
+
+@pytest.mark.gpu
+def test_batch_with_loss_and_constant_camera():
+    import ceres_torch_cuda_b200 as tc
+    datas = S.make_batched_instances(3, seed=21, max_points=120)
+    singles = _problems(datas, loss=tc.CauchyLoss(2.0))
+    batch = _problems(datas, loss=tc.CauchyLoss(2.0))
+    for p in singles + batch:
+        p.camera_constant = torch.zeros(p.num_cameras, dtype=torch.bool, device=p.cameras.device)
+        p.camera_constant[0] = True
+    ref = [tc.solve(_options(), p, precision="fp64") for p in singles]
+    got = tc.solve_batch(_options(), batch, precision="fp64")
+    for r, g, pb, ps in zip(ref, got, batch, singles):
+        np.testing.assert_allclose(g.final_cost, r.final_cost, rtol=1e-8)
+        np.testing.assert_array_equal(pb.cameras[0].cpu().numpy(), ps.cameras[0].cpu().numpy())
