@@ -128,7 +128,7 @@ SIGNATURES = {
     "ceres_b200_ba_dense_schur_solve": (c_int32, [_P, c_void_p, c_void_p]),
     "ceres_b200_dense_cholesky_solve": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "ceres_b200_batch_struct_bytes": (c_int32, []),
-    "ceres_b200_batch_solve": (c_int32, [_PB, c_int32, c_int32, c_void_p]),
+    "ceres_b200_batch_solve": (c_int32, [_PB, c_int32, c_int32, c_int32, c_void_p]),
 }
 
 _LIB: ctypes.CDLL | None = None

@@ -209,7 +209,7 @@ class BatchSolver:
         self.step_cameras = torch.zeros((NC, 9), **f64)
         self.cam_acc = torch.zeros((NC, 72), **f64)
         self.frames = torch.zeros((NC, 24), **f64)
-        self.pcg = torch.zeros((7, 9 * NC), **f64)
+        self.pcg = torch.zeros((8, 9 * NC), **f64)
         self.max_trace = options.max_num_iterations + 1
         self.result = torch.zeros((len(problems), _lib.BATCH_RESULT), **f64)
         self.trace = torch.zeros((len(problems), self.max_trace, _lib.BATCH_TRACE), **f64)
@@ -257,12 +257,12 @@ class BatchSolver:
         st = self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
         return st.cuda_stream
 
-    def launch(self, threads_per_cta: int = 0, ctas_per_sm: int = 0) -> None:
-        """Enqueue the solve (asynchronous on the stream)."""
+    def launch(self, threads_per_cta: int = 0, ctas_per_sm: int = 0, cluster_size: int = 1) -> None:
+        """Enqueue the solve (asynchronous on the stream); ``cluster_size`` CTAs per problem."""
         with torch.cuda.device(self.device):
             self.queue.zero_()
             rc = self.lib.ceres_b200_batch_solve(ctypes.byref(self.struct), int(threads_per_cta), int(ctas_per_sm),
-                                                 self._stream_handle())
+                                                 int(cluster_size), self._stream_handle())
         _lib.check(rc, "ceres_b200_batch_solve")
 
     def write_back(self) -> None:
@@ -364,16 +364,17 @@ def autotune(options: SolverOptions, problems: list[BundleAdjustmentProblem], *,
 
 
 def solve_batch(options: SolverOptions, problems: list[BundleAdjustmentProblem], *, precision: str = "mixed",
-                max_refinements: int = 1, threads_per_cta: int = 0, ctas_per_sm: int = 0,
+                max_refinements: int = 1, threads_per_cta: int = 0, ctas_per_sm: int = 0, cluster_size: int = 1,
                 tune: bool = False) -> list[SolverSummary]:
     """Solve every problem (in place) in one persistent launch; one SolverSummary each.
-    ``tune`` picks the CTA shape with ``autotune`` (cached) unless one is given."""
+    ``cluster_size`` CTAs (one thread-block cluster) work on each problem. ``tune``
+    picks the CTA shape with ``autotune`` (cached) unless one is given."""
     start = time.perf_counter()
     if tune and threads_per_cta == 0:
         threads_per_cta, ctas_per_sm = autotune(options, problems, precision=precision)
     solver = BatchSolver(problems, options, precision=precision, max_refinements=max_refinements)
     prep = time.perf_counter() - start
-    solver.launch(threads_per_cta, ctas_per_sm)
+    solver.launch(threads_per_cta, ctas_per_sm, cluster_size)
     torch.cuda.synchronize(solver.device)
     solver.write_back()
     summaries = solver.summaries()

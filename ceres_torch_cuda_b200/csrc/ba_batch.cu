@@ -1,22 +1,32 @@
 // Batched bundle adjustment: many independent problems in one persistent launch.
 //
-// Every CTA pulls whole problems from a work counter and runs the complete
-// Levenberg-Marquardt solve of one problem at a time: the same evaluation, Schur
-// assembly, implicit-Schur PCG and step arithmetic as the single-problem kernels of
-// ba_kernels.cu, at CTA scope (warps walk the problem's slices, __syncthreads instead
-// of grid barriers), and the trust-region decisions of ceres-torch's solver.py:35-357
-// (LM radius rule solver.py:805-820, step quality solver.py:823-861, convergence
-// tests solver.py:320-336 and :1169-1175) on the device. There is no host round
-// trip between iterations and no spin-wait anywhere: a CTA only synchronises with
-// itself.
+// Every thread-block cluster (1 to 16 CTAs) pulls whole problems from a work counter
+// and runs the complete Levenberg-Marquardt solve of one problem at a time: the same
+// evaluation, Schur assembly, implicit-Schur PCG and step arithmetic as the
+// single-problem kernels of ba_kernels.cu, spread over the cluster's CTAs, and the
+// trust-region decisions of ceres-torch's solver.py:35-357 (LM radius rule
+// solver.py:805-820, step quality solver.py:823-861, convergence tests
+// solver.py:320-336 and :1169-1175) on the device. There is no host round trip
+// between iterations and no spin-wait: CTAs synchronise through the hardware cluster
+// barrier only, and reductions read the other CTAs' partial sums from distributed
+// shared memory in rank order, so every CTA of a cluster computes bit-identical
+// scalars and takes the same branches.
 //
-// Data written during the launch (Jacobian store, residuals, vectors) is read with
-// plain loads, never through the read-only path.
+// Ownership inside a cluster: slices (points) go to cluster warps round robin and
+// stay with them for the whole solve, camera ranges go to CTAs (PCG vectors, camera
+// steps, frames, accepted parameters), and the camera sums go to cluster warps.
+// Data written by one CTA and read by another (frames, camera vectors, the Jacobian
+// records in the camera-major pass) is read with ld.global.cg, so a stale line in
+// another SM's L1 is never used; data written and read by the same CTA uses plain
+// loads (never the read-only path: everything here is rewritten in-launch).
+#include <cooperative_groups.h>
+
 #include <cstdio>
 
 #include "ba_device.cuh"
 
 using namespace cb200;
+namespace cgp = cooperative_groups;
 
 namespace {
 
@@ -27,83 +37,133 @@ constexpr int kBatchStall = 20;  // float32 PCG: iterations without a 1% residua
 
 __device__ __forceinline__ int tri9b(int j, int l) { return j * 9 - (j * (j - 1)) / 2 + (l - j); }
 
-// Jacobian record loads through the coherent path (the store is rewritten in-launch).
+template <typename V>
+__device__ __forceinline__ V ldx(const V* p) { return __ldcg(p); }  // cross-CTA data
+
+// Jacobian record loads; kCross: through L2 only.
+template <bool kCross>
 __device__ __forceinline__ void rec_load(const float* base, size_t slot, float v[kRec]) {
   const float4* p = reinterpret_cast<const float4*>(base + slot * kRec);
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
-    const float4 t = p[i];
+    const float4 t = kCross ? __ldcg(p + i) : p[i];
     v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
   }
 }
+template <bool kCross>
 __device__ __forceinline__ void rec_load(const double* base, size_t slot, double v[kRec]) {
   const double2* p = reinterpret_cast<const double2*>(base + slot * kRec);
 #pragma unroll
   for (int i = 0; i < 12; ++i) {
-    const double2 t = p[i];
+    const double2 t = kCross ? __ldcg(p + i) : p[i];
     v[2 * i] = t.x; v[2 * i + 1] = t.y;
   }
 }
 
-// Reduce NV values over the CTA and hand the result to every thread.
-template <int NV>
-__device__ __forceinline__ void cta_allreduce(double v[NV], unsigned max_mask, double* red, double* bcast) {
-  block_reduce<NV>(v, max_mask, red);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) bcast[i] = v[i];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < NV; ++i) v[i] = bcast[i];
-  __syncthreads();
+struct Ctx {
+  int rank, G;   // CTA rank in the cluster, cluster size
+  int ct, CT;    // cluster-wide thread index and count
+  int cw, CW;    // cluster-wide warp index and count
+};
+
+__device__ __forceinline__ void csync() { cgp::this_cluster().sync(); }
+
+template <typename V>
+__device__ __forceinline__ V* remote(V* p, int rank) {
+  return cgp::this_cluster().map_shared_rank(p, rank);
 }
 
 struct Prob {
   int b;
   int nc, cam0;  // cameras [cam0, cam0 + nc)
   int ns, s0;    // slices [s0, s0 + ns); sorted points 32 * s0 ...
+  int c0, c1;    // this CTA's camera range (local indices)
 };
 
 struct Smem {
   double* red;    // [8 * kMaxWarps]
-  double* bcast;  // [8]
-  void* ps;       // [9 * max_cameras] T: the PCG direction
-  void* ys;       // [9 * max_cameras] T: the product accumulator
+  double* part;   // [8]: this CTA's partial sums for cluster reductions
+  void* ps;       // [9 * max_cameras] T: the PCG direction (all cameras)
+  void* ys;       // [9 * max_cameras] T: this CTA's product accumulator
   double* y64;    // [9 * max_cameras]: float64 product accumulator (refinement)
 };
 
+// Reduce NV values over the cluster (sum, or max where max_mask has the bit) and hand
+// the result to every thread; every CTA folds the CTA partials in rank order.
+template <int NV>
+__device__ __forceinline__ void cl_allreduce(double v[NV], unsigned max_mask, const Ctx& X, const Smem& S) {
+  block_reduce<NV>(v, max_mask, S.red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) S.part[i] = v[i];
+  }
+  csync();
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = ((max_mask >> i) & 1u) ? -INFINITY : 0.0;
+  for (int r = 0; r < X.G; ++r) {
+    const double* pr = remote(S.part, r);
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = ((max_mask >> i) & 1u) ? fmax(v[i], pr[i]) : v[i] + pr[i];
+  }
+  csync();
+}
+
 // ------------------------------------------------------------------------------------
-// camera frames of cams (nc x 9) into frames
+// camera frames of this CTA's cameras; the cluster barrier publishes them
 // ------------------------------------------------------------------------------------
 template <bool kJac>
-__device__ void cta_frames(const double* cams, double* frames, int nc) {
-  for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+__device__ void cl_frames(const double* cams, double* frames, const Prob& P) {
+  for (int c = P.c0 + threadIdx.x; c < P.c1; c += blockDim.x) {
     const double* cam = cams + 9 * (size_t)c;
-    const double aa[3] = {cam[0], cam[1], cam[2]};
+    double cv[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) cv[i] = cam[i];
+    const double aa[3] = {cv[0], cv[1], cv[2]};
     CamRot R;
     camera_rotation<kJac>(aa, R);
-    frame_store<kJac>(frames + kFrame * (size_t)c, R, cam);
+    frame_store<kJac>(frames + kFrame * (size_t)c, R, cv);
   }
-  __syncthreads();
+  csync();
+}
+
+__device__ __forceinline__ void frame_load_x(const double* f, CamRot& R, double tail[6], bool jac) {
+  const double2* f2 = reinterpret_cast<const double2*>(f);
+  double2 v = __ldcg(f2);
+  R.w = v.x; R.u[0] = v.y;
+  v = __ldcg(f2 + 1);
+  R.u[1] = v.x; R.u[2] = v.y;
+  if (jac) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      v = __ldcg(f2 + 2 + i);
+      R.dqn[(2 * i) / 3][(2 * i) % 3] = v.x;
+      R.dqn[(2 * i + 1) / 3][(2 * i + 1) % 3] = v.y;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    v = __ldcg(f2 + 8 + i);
+    tail[2 * i] = v.x;
+    tail[2 * i + 1] = v.y;
+  }
 }
 
 // ------------------------------------------------------------------------------------
 // evaluation at B.cameras / B.points: residuals, Jacobian records, point sums, cost
 // ------------------------------------------------------------------------------------
 template <typename T>
-__device__ double cta_evaluate(const ceres_b200_batch_t& B, const LossSpec& L, const Prob& P, const Smem& S,
-                               unsigned& err) {
-  cta_frames<true>(B.cameras + 9 * (size_t)P.cam0, B.frames + kFrame * (size_t)P.cam0, P.nc);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+__device__ double cl_evaluate(const ceres_b200_batch_t& B, const LossSpec& L, const Prob& P, const Ctx& X,
+                              const Smem& S, unsigned& err) {
+  cl_frames<true>(B.cameras + 9 * (size_t)P.cam0, B.frames + kFrame * (size_t)P.cam0, P);
+  const int lane = threadIdx.x & 31;
   T* jac = reinterpret_cast<T*>(B.jac);
   const double* frames = B.frames + kFrame * (size_t)P.cam0;
   double cost = 0.0;
-  for (int s = P.s0 + w; s < P.s0 + P.ns; s += nw) {
+  for (int s = P.s0 + X.cw; s < P.s0 + P.ns; s += X.CW) {
     const int q = s * 32 + lane;
     const int len = B.slice_len[s];
     const size_t base = (size_t)B.slice_base[s];
-    const double X[3] = {B.points[3 * (size_t)q], B.points[3 * (size_t)q + 1], B.points[3 * (size_t)q + 2]};
+    const double Xp[3] = {B.points[3 * (size_t)q], B.points[3 * (size_t)q + 1], B.points[3 * (size_t)q + 2]};
     const bool pconst = B.pt_const[q] != 0;
     double W[6] = {0, 0, 0, 0, 0, 0}, g[3] = {0, 0, 0};
     for (int k = 0; k < len; ++k) {
@@ -114,8 +174,8 @@ __device__ double cta_evaluate(const ceres_b200_batch_t& B, const LossSpec& L, c
       Proj o;
       CamRot R;
       double tail[6];
-      frame_load<true>(frames + kFrame * (size_t)c, R, tail);
-      snavely_project<true>(R, tail, X, ob.x, ob.y, o);
+      frame_load_x(frames + kFrame * (size_t)c, R, tail, true);
+      snavely_project<true>(R, tail, Xp, ob.x, ob.y, o);
       cost += robustify<true>(L, o, err);
       reinterpret_cast<double2*>(B.res)[slot] = make_double2(o.r[0], o.r[1]);
       if (B.cam_const[P.cam0 + c]) {
@@ -146,22 +206,22 @@ __device__ double cta_evaluate(const ceres_b200_batch_t& B, const LossSpec& L, c
     for (int i = 0; i < 3; ++i) pr[6 + i] = g[i];
   }
   double v[1] = {cost};
-  cta_allreduce<1>(v, 0u, S.red, S.bcast);
+  cl_allreduce<1>(v, 0u, X, S);
   return v[0];
 }
 
 // ------------------------------------------------------------------------------------
-// Schur assembly for a radius: point blocks, camera sums, camera finish.
-// Returns the gradient stats {gmax, gsq} over point and camera columns.
+// Schur assembly for a radius: point blocks (own slices), camera sums and finish
+// (cameras by cluster warp). Returns gmax and the gradient norm.
 // ------------------------------------------------------------------------------------
 template <typename T>
-__device__ void cta_point_assemble(const ceres_b200_batch_t& B, const Prob& P, double inv_radius, double& gmax,
-                                   double& gsq) {
+__device__ void cl_point_assemble(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, double inv_radius,
+                                  double& gmax, double& gsq) {
   T* winv = reinterpret_cast<T*>(B.winv);
   const double mn = B.min_lm_diagonal, mx = B.max_lm_diagonal;
-  const int q0 = 32 * P.s0, np = 32 * P.ns;
-  for (int ql = threadIdx.x; ql < np; ql += blockDim.x) {
-    const int q = q0 + ql;
+  const int lane = threadIdx.x & 31;
+  for (int s = P.s0 + X.cw; s < P.s0 + P.ns; s += X.CW) {
+    const int q = s * 32 + lane;
     const double* pr = B.point_raw + 9 * (size_t)q;
     double W[6], g[3];
 #pragma unroll
@@ -192,7 +252,8 @@ __device__ void cta_point_assemble(const ceres_b200_batch_t& B, const Prob& P, d
 
 // One of three passes over a camera's observations (a warp per camera); each pass
 // keeps a third of the 72 float64 sums in registers: pass 0 the Schur-block rows 0-2,
-// pass 1 rows 3-8, pass 2 the column sums, gradient and reduced rhs.
+// pass 1 rows 3-8, pass 2 the column sums, gradient and reduced rhs. The records,
+// point blocks and residuals come from other CTAs' slices: read through L2.
 template <typename T, int kPass>
 __device__ void warp_camera_pass(const ceres_b200_batch_t& B, int cg, int cl, double* acc_out) {
   constexpr int kN = kPass == 0 ? 24 : (kPass == 1 ? 21 : 27);
@@ -210,10 +271,10 @@ __device__ void warp_camera_pass(const ceres_b200_batch_t& B, int cg, int cl, do
     const size_t slot = (size_t)ent.x;
     const int q = ent.y;
     T rv[kRec];
-    rec_load(jac, slot, rv);
+    rec_load<true>(jac, slot, rv);
     double wi[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) wi[i] = (double)winv[6 * (size_t)q + i];
+    for (int i = 0; i < 6; ++i) wi[i] = (double)ldx(winv + 6 * (size_t)q + i);
     double jp0[3], jp1[3];
 #pragma unroll
     for (int m = 0; m < 3; ++m) { jp0[m] = rv[18 + m]; jp1[m] = rv[21 + m]; }
@@ -245,7 +306,7 @@ __device__ void warp_camera_pass(const ceres_b200_batch_t& B, int cg, int cl, do
           const size_t slot2 = sb + 32 * (size_t)k + ln;
           if (slot2 == slot || B.slot_cam[slot2] != cl) continue;
           T rk[kRec];
-          rec_load(jac, slot2, rk);
+          rec_load<true>(jac, slot2, rk);
           const double C00 = P0[0] * rk[18] + P0[1] * rk[19] + P0[2] * rk[20];
           const double C01 = P0[0] * rk[21] + P0[1] * rk[22] + P0[2] * rk[23];
           const double C10 = P1[0] * rk[18] + P1[1] * rk[19] + P1[2] * rk[20];
@@ -260,8 +321,9 @@ __device__ void warp_camera_pass(const ceres_b200_batch_t& B, int cg, int cl, do
         }
       }
     } else {
-      const double2 r = reinterpret_cast<const double2*>(B.res)[slot];
-      const double wg[3] = {B.winv_ga[3 * (size_t)q], B.winv_ga[3 * (size_t)q + 1], B.winv_ga[3 * (size_t)q + 2]};
+      const double2 r = __ldcg(reinterpret_cast<const double2*>(B.res) + slot);
+      const double wg[3] = {ldx(B.winv_ga + 3 * (size_t)q), ldx(B.winv_ga + 3 * (size_t)q + 1),
+                            ldx(B.winv_ga + 3 * (size_t)q + 2)};
       const double a0 = jp0[0] * wg[0] + jp0[1] * wg[1] + jp0[2] * wg[2];
       const double a1 = jp1[0] * wg[0] + jp1[1] * wg[1] + jp1[2] * wg[2];
 #pragma unroll
@@ -377,15 +439,14 @@ __device__ void warp_camera_finish(const ceres_b200_batch_t& B, int cg, double i
 }
 
 template <typename T>
-__device__ void cta_assemble(const ceres_b200_batch_t& B, const Prob& P, double radius, const Smem& S,
-                             double& gmax, double& gnorm) {
+__device__ void cl_assemble(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, double radius, const Smem& S,
+                            double& gmax, double& gnorm) {
   const double inv_radius = 1.0 / fmax(radius, kEps64);
   double gp = 0.0, gsp = 0.0;
-  cta_point_assemble<T>(B, P, inv_radius, gp, gsp);
-  __syncthreads();
-  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  cl_point_assemble<T>(B, P, X, inv_radius, gp, gsp);
+  csync();  // point blocks of every CTA before the camera sums read them
   double gc = 0.0, gsc = 0.0;
-  for (int cl = w; cl < P.nc; cl += nw) {
+  for (int cl = X.cw; cl < P.nc; cl += X.CW) {
     const int cg = P.cam0 + cl;
     double* acc = B.cam_acc + (size_t)cg * 72;
     if (!B.cam_const[cg]) {
@@ -397,22 +458,22 @@ __device__ void cta_assemble(const ceres_b200_batch_t& B, const Prob& P, double 
     warp_camera_finish<T>(B, cg, inv_radius, gc, gsc);
   }
   double v[4] = {gp, gsp, gc, gsc};
-  cta_allreduce<4>(v, 0x5u, S.red, S.bcast);
+  cl_allreduce<4>(v, 0x5u, X, S);  // also publishes the camera blocks
   gmax = fmax(v[0], v[2]);
   gnorm = sqrt(v[1] + v[3]);
 }
 
 // ------------------------------------------------------------------------------------
-// Implicit Schur product over the problem's slices (the point-major walk of
-// matvec_slices): y = (J_c^T J_c - H_cp W^-1 H_pc) p into shared memory, A the
-// accumulation type (T, or double for the refinement residual).
+// Implicit Schur product over this CTA's slices (the point-major walk of
+// matvec_slices): ys += (J_c^T J_c - H_cp W^-1 H_pc) p into shared memory.
+// kCrossP: p is a global float64 vector written by other CTAs.
 // ------------------------------------------------------------------------------------
-template <typename T, typename TP, typename A>
-__device__ void cta_schur_product(const ceres_b200_batch_t& B, const Prob& P, const TP* ps, A* ys) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+template <typename T, typename TP, typename A, bool kCrossP>
+__device__ void cl_schur_product(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, const TP* ps, A* ys) {
+  const int lane = threadIdx.x & 31;
   const T* jac = reinterpret_cast<const T*>(B.jac);
   const T* winv = reinterpret_cast<const T*>(B.winv);
-  for (int s = P.s0 + w; s < P.s0 + P.ns; s += nw) {
+  for (int s = P.s0 + X.cw; s < P.s0 + P.ns; s += X.CW) {
     const int q = s * 32 + lane;
     const int len = B.slice_len[s];
     const size_t base = (size_t)B.slice_base[s] + lane;
@@ -421,11 +482,15 @@ __device__ void cta_schur_product(const ceres_b200_batch_t& B, const Prob& P, co
       const size_t slot = base + 32 * (size_t)k;
       const int c = max(B.slot_cam[slot], 0);  // padding slots: zero Jacobians, camera 0 as the address
       T rv[kRec];
-      rec_load(jac, slot, rv);
+      rec_load<false>(jac, slot, rv);
       const TP* pc = ps + 9 * (size_t)c;
       A u0 = 0, u1 = 0;
 #pragma unroll
-      for (int j = 0; j < 9; ++j) { u0 += (A)rv[j] * (A)pc[j]; u1 += (A)rv[9 + j] * (A)pc[j]; }
+      for (int j = 0; j < 9; ++j) {
+        const A pj = kCrossP ? (A)ldx(pc + j) : (A)pc[j];
+        u0 += (A)rv[j] * pj;
+        u1 += (A)rv[9 + j] * pj;
+      }
       t0 += (A)rv[18] * u0 + (A)rv[21] * u1;
       t1 += (A)rv[19] * u0 + (A)rv[22] * u1;
       t2 += (A)rv[20] * u0 + (A)rv[23] * u1;
@@ -440,11 +505,15 @@ __device__ void cta_schur_product(const ceres_b200_batch_t& B, const Prob& P, co
       const int c = B.slot_cam[slot];
       if (c < 0) continue;
       T rv[kRec];
-      rec_load(jac, slot, rv);
+      rec_load<false>(jac, slot, rv);
       const TP* pc = ps + 9 * (size_t)c;
       A u0 = 0, u1 = 0;
 #pragma unroll
-      for (int j = 0; j < 9; ++j) { u0 += (A)rv[j] * (A)pc[j]; u1 += (A)rv[9 + j] * (A)pc[j]; }
+      for (int j = 0; j < 9; ++j) {
+        const A pj = kCrossP ? (A)ldx(pc + j) : (A)pc[j];
+        u0 += (A)rv[j] * pj;
+        u1 += (A)rv[9 + j] * pj;
+      }
       const A v0 = u0 - ((A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2);
       const A v1 = u1 - ((A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2);
       A* yc = ys + 9 * (size_t)c;
@@ -463,7 +532,7 @@ __device__ __forceinline__ void precond_apply_b(const T* M, const double* r, dou
   for (int i = 0; i < 9; ++i) {
     double s = 0.0;
 #pragma unroll
-    for (int j = 0; j < 9; ++j) s += (double)M[i * 9 + j] * rr[j];
+    for (int j = 0; j < 9; ++j) s += (double)ldx(M + i * 9 + j) * rr[j];
     z[i] = s;
   }
 }
@@ -475,83 +544,94 @@ struct PcgOut {
 };
 
 // PCG (linear.py:1216-1256) on S x = rhs for one problem: x0 = 0, stop when
-// |r| <= tol * max(|rhs| or *norm_ref, eps) after min_it; float64 vectors, the product
-// in T. accumulate: x_out += x, else x_out = x.
+// |r| <= tol * max(|rhs| or norm_ref, eps) after min_it; float64 vectors (each CTA
+// owns the entries of its camera range), the product in T over each CTA's slices,
+// folded across the cluster by the owner. accumulate: x_out += x, else x_out = x.
 template <typename T>
-__device__ PcgOut cta_pcg(const ceres_b200_batch_t& B, const Prob& P, const Smem& S, const double* rhs,
-                          double* x_out, bool accumulate, int min_it, int max_it, double tol, double norm_ref,
-                          int stall_window) {
+__device__ PcgOut cl_pcg(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, const Smem& S, const double* rhs,
+                         double* x_out, bool accumulate, int min_it, int max_it, double tol, double norm_ref,
+                         int stall_window) {
   const size_t N = 9 * (size_t)B.cam_off[B.num_problems];
   const int n = 9 * P.nc;
+  const int j0 = 9 * P.c0, j1 = 9 * P.c1;
   const size_t o = 9 * (size_t)P.cam0;
-  double* X = B.pcg + o;
+  double* Xv = B.pcg + o;
   double* R = B.pcg + N + o;
   double* Z = B.pcg + 2 * N + o;
-  double* Pv = B.pcg + 3 * N + o;
-  double* AP = B.pcg + 4 * N + o;
+  double* Pb[2] = {B.pcg + 3 * N + o, B.pcg + 4 * N + o};
+  double* AP = B.pcg + 5 * N + o;
   const T* Minv = reinterpret_cast<const T*>(B.precond) + 81 * (size_t)P.cam0;
   const double* D = B.cam_diag + o;
   T* ps = reinterpret_cast<T*>(S.ps);
   T* ys = reinterpret_cast<T*>(S.ys);
   const double eps = Eps<T>::v();
 
-  for (int j = threadIdx.x; j < n; j += blockDim.x) { X[j] = 0.0; R[j] = rhs[j]; }
+  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) { Xv[j] = 0.0; R[j] = ldx(rhs + j); }
   __syncthreads();
-  for (int c = threadIdx.x; c < P.nc; c += blockDim.x) precond_apply_b(Minv + 81 * (size_t)c, R + 9 * c, Z + 9 * c);
+  for (int c = P.c0 + threadIdx.x; c < P.c1; c += blockDim.x)
+    precond_apply_b(Minv + 81 * (size_t)c, R + 9 * c, Z + 9 * c);
   __syncthreads();
   double v3[3] = {0.0, 0.0, 0.0};
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    const double rhsj = ldx(rhs + j);
     v3[0] += R[j] * Z[j];
     v3[1] += R[j] * R[j];
-    v3[2] += rhs[j] * rhs[j];
+    v3[2] += rhsj * rhsj;
   }
-  cta_allreduce<3>(v3, 0u, S.red, S.bcast);
+  cl_allreduce<3>(v3, 0u, X, S);  // also publishes Z
   double rz_old = v3[0];
   double rnorm = sqrt(v3[1]);
   const double rhs_norm = fmax(norm_ref >= 0.0 ? norm_ref : sqrt(v3[2]), eps);
   PcgOut out{0, false, rnorm, rhs_norm};
   double rbest = rnorm, beta = 0.0;
-  int last_improvement = 0;
+  int last_improvement = 0, cur = 0;
   if (min_it <= 0 && rnorm <= tol * rhs_norm) {
     out.success = true;
   } else {
     for (int k = 0; k < max_it; ++k) {
+      const int nxt = k == 0 ? 0 : cur ^ 1;
+      const double* Pold = Pb[cur];
+      double* Pnew = Pb[nxt];
+      // every CTA builds the whole direction in shared memory; the owner stores its part
       for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        const double pv = (k == 0) ? Z[j] : Z[j] + beta * Pv[j];
-        Pv[j] = pv;
+        const double pv = (k == 0) ? ldx(Z + j) : ldx(Z + j) + beta * ldx(Pold + j);
         ps[j] = (T)pv;
         ys[j] = (T)0;
+        if (j >= j0 && j < j1) Pnew[j] = pv;
       }
+      cur = nxt;
       __syncthreads();
-      cta_schur_product<T, T, T>(B, P, ps, ys);
-      __syncthreads();
+      cl_schur_product<T, T, T, false>(B, P, X, ps, ys);
+      csync();  // every CTA's product accumulator is complete
       double v1[1] = {0.0};
-      for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        const double y = (double)ys[j] + D[j] * Pv[j];
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        double y = 0.0;
+        for (int r = 0; r < X.G; ++r) y += (double)remote(ys, r)[j];
+        y += ldx(D + j) * Pnew[j];
         AP[j] = y;
-        v1[0] += Pv[j] * y;
+        v1[0] += Pnew[j] * y;
       }
-      cta_allreduce<1>(v1, 0u, S.red, S.bcast);
+      cl_allreduce<1>(v1, 0u, X, S);
       const double denom = v1[0];
       if (fabs(denom) <= eps) {
         out.success = rnorm <= tol * rhs_norm;
         break;
       }
       const double alpha = rz_old / denom;
-      for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        X[j] += alpha * Pv[j];
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        Xv[j] += alpha * Pnew[j];
         R[j] -= alpha * AP[j];
       }
       __syncthreads();
-      for (int c = threadIdx.x; c < P.nc; c += blockDim.x)
+      for (int c = P.c0 + threadIdx.x; c < P.c1; c += blockDim.x)
         precond_apply_b(Minv + 81 * (size_t)c, R + 9 * c, Z + 9 * c);
       __syncthreads();
       double v2[2] = {0.0, 0.0};
-      for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
         v2[0] += R[j] * Z[j];
         v2[1] += R[j] * R[j];
       }
-      cta_allreduce<2>(v2, 0u, S.red, S.bcast);
+      cl_allreduce<2>(v2, 0u, X, S);  // also publishes Z and the new direction
       const double rz_new = v2[0];
       rnorm = sqrt(v2[1]);
       out.iterations = k + 1;
@@ -569,37 +649,42 @@ __device__ PcgOut cta_pcg(const ceres_b200_batch_t& B, const Prob& P, const Smem
     }
   }
   out.rnorm = rnorm;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) x_out[j] = accumulate ? x_out[j] + X[j] : X[j];
-  __syncthreads();
+  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) x_out[j] = accumulate ? x_out[j] + Xv[j] : Xv[j];
+  csync();  // the solution is published
   return out;
 }
 
 // The camera step: PCG with float64 refinement passes for the float32 store (the same
 // sequence as the single-problem entry point). Returns the PCG iterations.
 template <typename T>
-__device__ int cta_linear_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem& S) {
+__device__ int cl_linear_solve(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, const Smem& S) {
   const size_t N = 9 * (size_t)B.cam_off[B.num_problems];
   const size_t o = 9 * (size_t)P.cam0;
   const int n = 9 * P.nc;
+  const int j0 = 9 * P.c0, j1 = 9 * P.c1;
   double* step = B.step_cameras + o;
   const double* rhs = B.rhs + o;
   const bool refine = B.max_refinements > 0 && sizeof(T) == sizeof(float);
-  const PcgOut first = cta_pcg<T>(B, P, S, rhs, step, false, B.min_linear_solver_iterations,
-                                  B.max_linear_solver_iterations, B.eta, -1.0, refine ? kBatchStall : 0);
+  const PcgOut first = cl_pcg<T>(B, P, X, S, rhs, step, false, B.min_linear_solver_iterations,
+                                 B.max_linear_solver_iterations, B.eta, -1.0, refine ? kBatchStall : 0);
   int iterations = first.iterations;
   if (refine && !first.success) {
     // float64 refinement: r64 = rhs - S step with float64 accumulation, then a float32
     // solve of S dx = r64 (tolerance relative to the original |rhs|) added to the step
-    double* r64 = B.pcg + 5 * N + o;
+    double* r64 = B.pcg + 6 * N + o;
     for (int it = 0; it < B.max_refinements; ++it) {
       for (int j = threadIdx.x; j < n; j += blockDim.x) S.y64[j] = 0.0;
       __syncthreads();
-      cta_schur_product<T, double, double>(B, P, step, S.y64);
-      __syncthreads();
-      for (int j = threadIdx.x; j < n; j += blockDim.x) r64[j] = rhs[j] - (S.y64[j] + B.cam_diag[o + j] * step[j]);
-      __syncthreads();
-      const PcgOut corr = cta_pcg<T>(B, P, S, r64, step, true, 0, B.max_linear_solver_iterations, B.eta,
-                                     first.rhs_norm, kBatchStall);
+      cl_schur_product<T, double, double, true>(B, P, X, step, S.y64);
+      csync();
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        double y = 0.0;
+        for (int r = 0; r < X.G; ++r) y += remote(S.y64, r)[j];
+        r64[j] = ldx(rhs + j) - (y + ldx(B.cam_diag + o + j) * step[j]);
+      }
+      csync();
+      const PcgOut corr = cl_pcg<T>(B, P, X, S, r64, step, true, 0, B.max_linear_solver_iterations, B.eta,
+                                    first.rhs_norm, kBatchStall);
       iterations += corr.iterations;
     }
   }
@@ -607,17 +692,16 @@ __device__ int cta_linear_solve(const ceres_b200_batch_t& B, const Prob& P, cons
 }
 
 // ------------------------------------------------------------------------------------
-// Step: candidate cameras, point back-substitution, model decrease, candidate cost
-// (ceres_b200_ba_step at CTA scope). Outputs {cand cost, model, |dp|^2 + |dc|^2,
-// non-finite count, |x + step|^2}.
+// Step: candidate cameras (own range), point back-substitution, model decrease and
+// candidate cost (own slices). Outputs {cand cost, model, |step|^2, non-finite,
+// |x + step|^2} over the cluster.
 // ------------------------------------------------------------------------------------
 template <typename T>
-__device__ void cta_step(const ceres_b200_batch_t& B, const LossSpec& L, const Prob& P, const Smem& S,
-                         unsigned& err, double out[5]) {
+__device__ void cl_step(const ceres_b200_batch_t& B, const LossSpec& L, const Prob& P, const Ctx& X,
+                        const Smem& S, unsigned& err, double out[5]) {
   const size_t o = 9 * (size_t)P.cam0;
-  const int n = 9 * P.nc;
   double sq = 0.0, nonfinite = 0.0, state = 0.0, cand = 0.0, model = 0.0;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+  for (int j = 9 * P.c0 + threadIdx.x; j < 9 * P.c1; j += blockDim.x) {
     const int c = P.cam0 + j / 9;
     double d = B.cam_const[c] ? 0.0 : B.step_cameras[o + j];
     if (!B.cam_const[c]) {
@@ -630,13 +714,13 @@ __device__ void cta_step(const ceres_b200_batch_t& B, const LossSpec& L, const P
     state += xc * xc;
   }
   __syncthreads();
-  cta_frames<false>(B.cand_cameras + o, B.frames + kFrame * (size_t)P.cam0, P.nc);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  cl_frames<false>(B.cand_cameras + o, B.frames + kFrame * (size_t)P.cam0, P);  // ends with a cluster barrier
+  const int lane = threadIdx.x & 31;
   const T* jac = reinterpret_cast<const T*>(B.jac);
   const T* winv = reinterpret_cast<const T*>(B.winv);
   const double* frames = B.frames + kFrame * (size_t)P.cam0;
   const double* dcv = B.step_cameras + o;
-  for (int s = P.s0 + w; s < P.s0 + P.ns; s += nw) {
+  for (int s = P.s0 + X.cw; s < P.s0 + P.ns; s += X.CW) {
     const int q = s * 32 + lane;
     const int len = B.slice_len[s];
     const size_t base = (size_t)B.slice_base[s] + lane;
@@ -645,11 +729,15 @@ __device__ void cta_step(const ceres_b200_batch_t& B, const LossSpec& L, const P
       const size_t slot = base + 32 * (size_t)k;
       const int c = max(B.slot_cam[slot], 0);
       T rv[kRec];
-      rec_load(jac, slot, rv);
+      rec_load<false>(jac, slot, rv);
       const double* dc = dcv + 9 * (size_t)c;
       double u0 = 0.0, u1 = 0.0;
 #pragma unroll
-      for (int j = 0; j < 9; ++j) { u0 += (double)rv[j] * dc[j]; u1 += (double)rv[9 + j] * dc[j]; }
+      for (int j = 0; j < 9; ++j) {
+        const double dj = ldx(dc + j);
+        u0 += (double)rv[j] * dj;
+        u1 += (double)rv[9 + j] * dj;
+      }
 #pragma unroll
       for (int m = 0; m < 3; ++m) t[m] += (double)rv[18 + m] * u0 + (double)rv[21 + m] * u1;
     }
@@ -680,12 +768,16 @@ __device__ void cta_step(const ceres_b200_batch_t& B, const LossSpec& L, const P
       const int c = B.slot_cam[slot];
       if (c < 0) continue;
       T rv[kRec];
-      rec_load(jac, slot, rv);
+      rec_load<false>(jac, slot, rv);
       const double2 r = reinterpret_cast<const double2*>(B.res)[slot];
       const double* dc = dcv + 9 * (size_t)c;
       double j0 = 0.0, j1 = 0.0;
 #pragma unroll
-      for (int j = 0; j < 9; ++j) { j0 += (double)rv[j] * dc[j]; j1 += (double)rv[9 + j] * dc[j]; }
+      for (int j = 0; j < 9; ++j) {
+        const double dj = ldx(dc + j);
+        j0 += (double)rv[j] * dj;
+        j1 += (double)rv[9 + j] * dj;
+      }
 #pragma unroll
       for (int m = 0; m < 3; ++m) { j0 += (double)rv[18 + m] * dp[m]; j1 += (double)rv[21 + m] * dp[m]; }
       const double a0 = r.x + j0, a1 = r.y + j1;
@@ -694,38 +786,42 @@ __device__ void cta_step(const ceres_b200_batch_t& B, const LossSpec& L, const P
       Proj pj;
       CamRot R;
       double tail[6];
-      frame_load<false>(frames + kFrame * (size_t)c, R, tail);
+      frame_load_x(frames + kFrame * (size_t)c, R, tail, false);
       snavely_project<false>(R, tail, Xc, ob.x, ob.y, pj);
       cand += robustify<false>(L, pj, err);
     }
   }
   double v[5] = {cand, model, sq, nonfinite, state};
-  cta_allreduce<5>(v, 0u, S.red, S.bcast);
+  cl_allreduce<5>(v, 0u, X, S);
 #pragma unroll
   for (int i = 0; i < 5; ++i) out[i] = v[i];
 }
 
-// candidate -> current for one problem's cameras and points
-__device__ void cta_accept(const ceres_b200_batch_t& B, const Prob& P) {
+// candidate -> current: this CTA's camera range and its own slices' points
+__device__ void cl_accept(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X) {
   const size_t o = 9 * (size_t)P.cam0;
-  for (int j = threadIdx.x; j < 9 * P.nc; j += blockDim.x) B.cameras[o + j] = B.cand_cameras[o + j];
-  const size_t po = 3 * 32 * (size_t)P.s0;
-  for (int j = threadIdx.x; j < 3 * 32 * P.ns; j += blockDim.x) B.points[po + j] = B.cand_points[po + j];
-  __syncthreads();
+  for (int j = 9 * P.c0 + threadIdx.x; j < 9 * P.c1; j += blockDim.x) B.cameras[o + j] = B.cand_cameras[o + j];
+  const int lane = threadIdx.x & 31;
+  for (int s = P.s0 + X.cw; s < P.s0 + P.ns; s += X.CW) {
+    const size_t q = (size_t)s * 32 + lane;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) B.points[3 * q + m] = B.cand_points[3 * q + m];
+  }
+  csync();
 }
 
 // ------------------------------------------------------------------------------------
 // The trust-region solve of one problem (the host loop of engine.run_lm, monotonic
-// steps): scalars live in registers of every thread (all threads compute the same
-// values from broadcast reductions), thread 0 writes the records.
+// steps). Every thread of every CTA of the cluster holds the same scalars (computed
+// from cluster reductions); thread 0 of rank 0 writes the records.
 // ------------------------------------------------------------------------------------
 template <typename T>
-__device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem& S) {
+__device__ void cl_solve(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, const Smem& S) {
   const LossSpec L{B.loss_kind, B.loss_a, B.loss_b, B.loss_scale, B.inner_loss_kind, B.inner_a, B.inner_b,
                    B.inner_scale};
   double* res = B.result + (size_t)P.b * kBR;
   double* trace = B.trace + (size_t)P.b * B.max_trace * kBT;
-  const bool lead = threadIdx.x == 0;
+  const bool lead = threadIdx.x == 0 && X.rank == 0;
   unsigned err = 0;
   int records = 0, successful = 0, unsuccessful = 0, jac_evals = 0, res_evals = 0, linear_solves = 0;
   int term = CERES_B200_TERM_NO_CONVERGENCE, msg = CERES_B200_MSG_MAX_ITERATIONS;
@@ -750,9 +846,9 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
 
   double radius = B.initial_radius;
   double decrease_factor = 2.0;
-  double cost = cta_evaluate<T>(B, L, P, S, err);
+  double cost = cl_evaluate<T>(B, L, P, X, S, err);
   double gmax, gnorm;
-  cta_assemble<T>(B, P, radius, S, gmax, gnorm);
+  cl_assemble<T>(B, P, X, radius, S, gmax, gnorm);
   ++jac_evals;
   const double initial_cost = cost;
   double best_cost = cost;
@@ -766,8 +862,7 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
   int consecutive_invalid = 0;
   bool done = false;
 
-  // iteration 0
-  record(cost, 0.0, gmax, gnorm, 0.0, 0.0, radius, 0, 3);
+  record(cost, 0.0, gmax, gnorm, 0.0, 0.0, radius, 0, 3);  // iteration 0
   if (gmax <= B.gradient_tolerance) {
     term = CERES_B200_TERM_CONVERGENCE; msg = CERES_B200_MSG_GRADIENT; done = true;
   } else if (B.max_num_iterations == 0) {
@@ -775,15 +870,15 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
   }
   for (int iteration = 1; !done && iteration <= B.max_num_iterations; ++iteration) {
     if (need_assemble) {
-      double gm, gn;  // the gradient stats of a re-assembly are not reported (the host loop keeps the old ones)
-      cta_assemble<T>(B, P, radius, S, gm, gn);
+      double gm, gn;  // the host loop keeps the gradient stats of the last evaluation
+      cl_assemble<T>(B, P, X, radius, S, gm, gn);
       need_assemble = false;
     }
     ++jac_evals;
-    const int lin = P.nc > 0 ? cta_linear_solve<T>(B, P, S) : 1;
+    const int lin = cl_linear_solve<T>(B, P, X, S);
     ++linear_solves;
     double st[5];
-    cta_step<T>(B, L, P, S, err, st);
+    cl_step<T>(B, L, P, X, S, err, st);
     if (st[3] > 0.0) {  // non-finite step
       ++consecutive_invalid;
       radius = radius / decrease_factor;
@@ -813,7 +908,6 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
     if (accepted) {
       consecutive_invalid = 0;
       ++successful;
-      // step_accepted (max_nonmonotonic = 0)
       current_cost = cand_cost;
       acc_candidate += model_decrease;
       acc_reference += model_decrease;
@@ -824,7 +918,7 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
         if (cand_cost > candidate_cost_h) { candidate_cost_h = cand_cost; acc_candidate = 0.0; }
       }
       if (nonmonotonic == 0) { reference_cost = candidate_cost_h; acc_reference = acc_candidate; }
-      cta_accept(B, P);
+      cl_accept(B, P, X);
       if (cand_cost < best_cost) best_cost = cand_cost;
       else flags |= (cand_cost > best_cost) ? 4 : 0;
       const double tmp = 2.0 * rho - 1.0;
@@ -850,8 +944,8 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
       }
       previous_cost = cand_cost;
       previous_set = true;
-      cost = cta_evaluate<T>(B, L, P, S, err);
-      cta_assemble<T>(B, P, radius, S, gmax, gnorm);
+      cost = cl_evaluate<T>(B, L, P, X, S, err);
+      cl_assemble<T>(B, P, X, radius, S, gmax, gnorm);
       ++jac_evals;
       if (gmax <= B.gradient_tolerance) {
         term = CERES_B200_TERM_CONVERGENCE; msg = CERES_B200_MSG_GRADIENT;
@@ -864,8 +958,8 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
       break;
     }
   }
-  // err: OR over the threads
-  const unsigned any_err = __syncthreads_or(err);
+  double ev[1] = {(double)__syncthreads_or(err)};
+  cl_allreduce<1>(ev, 1u, X, S);
   if (lead) {
     res[CERES_B200_BR_INITIAL_COST] = initial_cost;
     res[CERES_B200_BR_FINAL_COST] = best_cost;
@@ -877,30 +971,37 @@ __device__ void cta_solve(const ceres_b200_batch_t& B, const Prob& P, const Smem
     res[CERES_B200_BR_JACOBIAN_EVALS] = (double)jac_evals;
     res[CERES_B200_BR_RESIDUAL_EVALS] = (double)res_evals;
     res[CERES_B200_BR_LINEAR_SOLVES] = (double)linear_solves;
-    res[CERES_B200_BR_ERROR] = (double)any_err;
+    res[CERES_B200_BR_ERROR] = ev[0];
     res[CERES_B200_BR_FINAL_GMAX] = gmax;
   }
-  __syncthreads();
 }
 
 template <typename T, int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_batch_solve(ceres_b200_batch_t B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[8 * kMaxWarps];
-  __shared__ double bcast[8];
+  __shared__ double part[8];
   __shared__ int next;
+  const cgp::cluster_group cluster = cgp::this_cluster();
+  Ctx X;
+  X.rank = (int)cluster.block_rank();
+  X.G = (int)cluster.num_blocks();
+  X.ct = X.rank * blockDim.x + threadIdx.x;
+  X.CT = X.G * blockDim.x;
+  X.cw = X.rank * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  X.CW = X.G * (blockDim.x >> 5);
   const size_t vec = (size_t)((9 * B.max_cameras + 3) & ~3);
   Smem S;
   S.red = red;
-  S.bcast = bcast;
+  S.part = part;
   S.y64 = reinterpret_cast<double*>(smem_raw);
   S.ps = smem_raw + (sizeof(T) == sizeof(float) ? vec * sizeof(double) : 0);
   S.ys = reinterpret_cast<unsigned char*>(S.ps) + vec * sizeof(T);
   for (;;) {
-    if (threadIdx.x == 0) next = (int)atomicAdd(B.queue, 1u);
-    __syncthreads();
-    const int b = next;
-    __syncthreads();
+    if (X.rank == 0 && threadIdx.x == 0) next = (int)atomicAdd(B.queue, 1u);
+    csync();
+    const int b = *remote(&next, 0);
+    csync();
     if (b >= B.num_problems) break;
     Prob P;
     P.b = b;
@@ -908,7 +1009,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_batch_solve(ceres_b200
     P.nc = B.cam_off[b + 1] - P.cam0;
     P.s0 = B.slice_off[b];
     P.ns = B.slice_off[b + 1] - P.s0;
-    cta_solve<T>(B, P, S);
+    const int per = (P.nc + X.G - 1) / X.G;
+    P.c0 = min(P.nc, X.rank * per);
+    P.c1 = min(P.nc, P.c0 + per);
+    cl_solve<T>(B, P, X, S);
   }
 }
 
@@ -932,7 +1036,8 @@ extern "C" {
 
 int ceres_b200_batch_struct_bytes(void) { return (int)sizeof(ceres_b200_batch_t); }
 
-int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta, int ctas_per_sm, void* stream) {
+int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta, int ctas_per_sm, int cluster_size,
+                           void* stream) {
   if (!batch || batch->num_problems < 0) return CERES_B200_EINVAL;
   if (batch->num_problems == 0) return CERES_B200_OK;
   const ceres_b200_batch_t& B = *batch;
@@ -946,6 +1051,8 @@ int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta,
   if (B.max_cameras < 0 || B.max_trace < 1 || B.max_num_iterations < 0) return CERES_B200_EINVAL;
   if (B.preconditioner < CERES_B200_PRECOND_IDENTITY || B.preconditioner > CERES_B200_PRECOND_SCHUR_JACOBI)
     return CERES_B200_EINVAL;
+  const int G = cluster_size == 0 ? 1 : cluster_size;
+  if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16) return CERES_B200_EINVAL;
   const int threads = threads_per_cta == 0 ? 256 : threads_per_cta;
   const int ctas = ctas_per_sm == 0 ? 1 : ctas_per_sm;
   const bool f32 = B.precision == CERES_B200_FP32;
@@ -963,12 +1070,26 @@ int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta,
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return CERES_B200_ESMEM;
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
-    return CERES_B200_ESMEM;
-  long long grid = (long long)sms * per_sm;
-  if (grid > B.num_problems) grid = B.num_problems;
-  kern<<<(int)grid, threads, smem, (cudaStream_t)stream>>>(B);
+  if (G > 8 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return CERES_B200_ECOOP;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)G;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3((unsigned)threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = (cudaStream_t)stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3((unsigned)G);
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) return CERES_B200_ECOOP;
+  long long n = clusters;
+  if (n > B.num_problems) n = B.num_problems;
+  cfg.gridDim = dim3((unsigned)(n * G));
+  if (cudaLaunchKernelEx(&cfg, kern, B) != cudaSuccess) return CERES_B200_ECUDA;
   return cudaGetLastError() == cudaSuccess ? CERES_B200_OK : CERES_B200_ECUDA;
 }
 

@@ -1,0 +1,203 @@
+"""Serving loop: continuous batching of bundle-adjustment solve requests on one GPU.
+
+Requests wait in an arrival queue. Whenever a stream slot is free, the server
+admits waiting requests, oldest first, while their device footprint fits the
+memory budget next to the batches already running. It launches them as one
+batched persistent solve (``BatchSolver``) on a stream of its own. Batches on
+different streams run side by side on the GPU: a batch of k problems occupies k
+CTAs. Requests that arrive while others run are admitted as soon as a slot and
+memory free up. Their work overlaps on the device with the batches in flight.
+
+A request's result does not depend on what it was batched with, because each
+problem is solved by one CTA from its own data.
+
+``BAServer.step()`` is non-blocking and does one round of completion, admission
+and launch. ``run_stream()`` replays a timed arrival stream through it and
+reports latency percentiles and throughput.
+"""
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .batch import BatchSolver
+from .problem import BundleAdjustmentProblem
+from .types import SolverOptions, SolverSummary
+
+
+def footprint_bytes(problem: BundleAdjustmentProblem, precision: str) -> int:
+    """Device bytes a request holds while it is solved (batch buffers and layout)."""
+    jb = 4 if precision == "mixed" else 8
+    no, npts, nc = problem.num_observations, problem.num_points, problem.num_cameras
+    slots = int(no * 1.15) + 32 * 8
+    nq = 32 * ((npts + 31) // 32)
+    per_slot = 24 * jb + 16 + 16 + 4
+    per_obs = 8 + 64  # camera-major entry and layout-building temporaries
+    per_point = 9 * 8 + 6 * jb + 4 * 3 * 8 + 3 * 8 + 8 + 1
+    per_camera = 4 * 9 * 8 + 81 * jb + 72 * 8 + 24 * 8 + 7 * 9 * 8
+    return slots * per_slot + no * per_obs + nq * per_point + nc * per_camera
+
+
+@dataclass
+class Request:
+    problem: BundleAdjustmentProblem
+    arrival: float                       # time.perf_counter() at submission
+    footprint: int = 0
+    admitted: float | None = None
+    done: float | None = None
+    summary: SolverSummary | None = None
+
+    @property
+    def latency(self) -> float | None:
+        return None if self.done is None else self.done - self.arrival
+
+
+@dataclass
+class _Flight:
+    solver: BatchSolver
+    requests: list
+    stream: torch.cuda.Stream
+    event: torch.cuda.Event
+    footprint: int
+
+
+@dataclass
+class BAServer:
+    """Continuous-batching server (one GPU, one host thread).
+
+    ``memory_budget``: device bytes the in-flight requests may hold (default: half of
+    the free memory at construction). ``max_inflight``: concurrent batches (streams).
+    ``max_batch``: requests per launch.
+    """
+
+    options: SolverOptions
+    precision: str = "mixed"
+    memory_budget: int | None = None
+    max_inflight: int = 4
+    max_batch: int = 512
+    threads_per_cta: int = 256
+    ctas_per_sm: int = 1
+    device: torch.device = field(default_factory=lambda: torch.device("cuda", torch.cuda.current_device()))
+    _waiting: deque = field(default_factory=deque, init=False, repr=False)
+    _flights: list = field(default_factory=list, init=False, repr=False)
+    _streams: list = field(default_factory=list, init=False, repr=False)
+    _in_use: int = field(default=0, init=False, repr=False)
+    completed: list = field(default_factory=list, init=False, repr=False)
+
+    def __post_init__(self):
+        if self.memory_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            self.memory_budget = int(free * 0.5)
+        self._streams = [torch.cuda.Stream(self.device) for _ in range(self.max_inflight)]
+
+    def submit(self, problem: BundleAdjustmentProblem, arrival: float | None = None) -> Request:
+        r = Request(problem, time.perf_counter() if arrival is None else arrival,
+                    footprint_bytes(problem, self.precision))
+        if r.footprint > self.memory_budget:
+            raise ValueError(f"request needs {r.footprint} device bytes, above the server budget {self.memory_budget}")
+        self._waiting.append(r)
+        return r
+
+    @property
+    def busy(self) -> bool:
+        return bool(self._waiting or self._flights)
+
+    def _complete(self) -> int:
+        n = 0
+        still = []
+        for f in self._flights:
+            if f.event.query():
+                f.solver.write_back()
+                sums = f.solver.summaries()
+                now = time.perf_counter()
+                for r, s in zip(f.requests, sums):
+                    r.summary = s
+                    r.done = now
+                    self.completed.append(r)
+                self._in_use -= f.footprint
+                n += len(f.requests)
+            else:
+                still.append(f)
+        self._flights = still
+        return n
+
+    def _admit(self) -> bool:
+        if not self._waiting or len(self._flights) >= self.max_inflight:
+            return False
+        batch, size = [], 0
+        while self._waiting and len(batch) < self.max_batch:
+            r = self._waiting[0]
+            if self._in_use + size + r.footprint > self.memory_budget:
+                break
+            batch.append(self._waiting.popleft())
+            size += r.footprint
+        if not batch:
+            return False
+        busy = {id(f.stream) for f in self._flights}
+        stream = next(s for s in self._streams if id(s) not in busy)
+        now = time.perf_counter()
+        with torch.cuda.stream(stream):
+            solver = BatchSolver([r.problem for r in batch], self.options, precision=self.precision, stream=stream)
+            solver.launch(self.threads_per_cta, self.ctas_per_sm)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        for r in batch:
+            r.admitted = now
+        self._flights.append(_Flight(solver, batch, stream, ev, size))
+        self._in_use += size
+        return True
+
+    def step(self) -> None:
+        """One non-blocking round: finish completed batches, then launch waiting requests."""
+        self._complete()
+        while self._admit():
+            pass
+
+    def drain(self, timeout_s: float = 600.0) -> None:
+        end = time.perf_counter() + timeout_s
+        while self.busy and time.perf_counter() < end:
+            self.step()
+            if self._flights and not self._waiting:
+                time.sleep(0.0002)
+        if self.busy:
+            raise TimeoutError("server did not drain")
+
+
+def run_stream(server: BAServer, arrivals: np.ndarray, problems: list[BundleAdjustmentProblem],
+               timeout_s: float = 600.0) -> dict:
+    """Replay an arrival stream (seconds from start) through ``server`` in real time and
+    report latency percentiles (ms) and throughput."""
+    order = np.argsort(arrivals, kind="stable")
+    reqs = [None] * len(problems)
+    t0 = time.perf_counter()
+    i = 0
+    end = t0 + timeout_s
+    while (i < len(order) or server.busy) and time.perf_counter() < end:
+        now = time.perf_counter() - t0
+        while i < len(order) and arrivals[order[i]] <= now:
+            k = int(order[i])
+            reqs[k] = server.submit(problems[k], arrival=t0 + float(arrivals[k]))
+            i += 1
+        server.step()
+        if i < len(order):
+            wait = arrivals[order[i]] - (time.perf_counter() - t0)
+            if wait > 0.0005 and not server._flights:
+                time.sleep(min(wait, 0.002))
+    if server.busy or i < len(order):
+        raise TimeoutError("arrival stream did not finish")
+    wall = time.perf_counter() - t0
+    lat = np.array([r.latency for r in reqs]) * 1e3
+    first = float(np.min(arrivals))
+    last_done = max(r.done for r in reqs) - t0
+    return {
+        "requests": len(reqs), "wall_s": wall,
+        "p50_ms": float(np.percentile(lat, 50)), "p90_ms": float(np.percentile(lat, 90)),
+        "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
+        "solves_per_s": len(reqs) / max(last_done - first, 1e-9),
+        "offered_rate_per_s": len(reqs) / max(float(np.max(arrivals)) - first, 1e-9),
+        "requests_list": reqs,
+    }

@@ -266,9 +266,9 @@ int ceres_b200_dense_cholesky_solve(double* H, const double* rhs, double* x, int
 /* ------------------------------------------------------------------------------------
  * Batched solves: many independent bundle-adjustment problems in one persistent launch.
  *
- * Each CTA takes whole problems from a work counter (queue[0], zeroed by the caller)
- * and runs the complete Levenberg-Marquardt solve of one problem at a time on the
- * device: evaluation, Schur assembly, implicit-Schur PCG, step and the trust-region
+ * Each thread-block cluster takes whole problems from a work counter (queue[0], zeroed
+ * by the caller) and runs the complete Levenberg-Marquardt solve of one problem at a
+ * time on the device: evaluation, Schur assembly, implicit-Schur PCG, step and the trust-region
  * decisions of ceres-torch's solver.py:35-357 (monotonic steps, ITERATIVE_SCHUR).
  * No host round trip happens between iterations; a problem's result does not depend
  * on the other problems of the batch. This has no counterpart in the reference, which
@@ -365,7 +365,7 @@ typedef struct ceres_b200_batch_t {
   double* step_cameras;         /* [cameras][9] */
   double* cam_acc;              /* [cameras][72] */
   double* frames;               /* [cameras][24] */
-  double* pcg;                  /* [7][9 * total cameras]: x, r, z, p, Ap, refinement residual, correction */
+  double* pcg;                  /* [8][9 * total cameras]: x, r, z, p (two buffers), Ap, refinement residual, spare */
   double* result;               /* [num_problems][CERES_B200_BATCH_RESULT] */
   double* trace;                /* [num_problems][max_trace][CERES_B200_BATCH_TRACE] */
   uint32_t* queue;              /* [1] work counter, zero before the launch */
@@ -375,12 +375,16 @@ typedef struct ceres_b200_batch_t {
 int ceres_b200_batch_struct_bytes(void);
 
 /*
- * Solves every problem of the batch in one persistent launch. Shapes (threads_per_cta,
- * ctas_per_sm): (128, 1|2), (128, 4), (256, 1), (256, 2), (512, 1); ctas_per_sm sets
- * the register cap, 0 picks (256, 1). Asynchronous on stream; results appear in
- * result/trace and the parameters are updated in place.
+ * Solves every problem of the batch in one persistent launch. A thread-block cluster
+ * of cluster_size CTAs (1, 2, 4, 8 or 16; 0 means 1) solves one problem at a time:
+ * larger clusters give a problem more SMs (lower latency per problem), smaller ones
+ * more problems in flight. CTA shapes (threads_per_cta, ctas_per_sm): (128, 1|2),
+ * (128, 4), (256, 1), (256, 2), (512, 1); ctas_per_sm sets the register cap, 0 picks
+ * (256, 1). Asynchronous on stream; results appear in result/trace and the
+ * parameters are updated in place.
  */
-int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta, int ctas_per_sm, void* stream);
+int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta, int ctas_per_sm, int cluster_size,
+                           void* stream);
 
 #ifdef __cplusplus
 }

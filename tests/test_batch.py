@@ -5,7 +5,8 @@ solve would use (same slices, same slot order, same camera-major lists).
 GPU: each problem of a batch ends where its own ``tc.solve`` ends (float64: final
 cost 1e-8 relative, termination and iteration count equal up to +-2, parameters
 1e-5; mixed: final cost within 1e-6 of the float64 single solve), and a problem's
-result in a batch of one equals its result in the mix (1e-8 relative).
+result in a batch of one equals its result in the mix (1e-8 relative). Clusters of
+1 to 16 CTAs per problem give the same results.
 """
 from __future__ import annotations
 
@@ -72,14 +73,14 @@ def _options(max_iterations=30):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batch_matches_single_solves(precision):
+@pytest.mark.parametrize("precision,cluster", [("fp64", 1), ("mixed", 1), ("fp64", 4), ("mixed", 8), ("fp64", 16)])
+def test_batch_matches_single_solves(precision, cluster):
     import ceres_torch_cuda_b200 as tc
     datas = S.make_batched_instances(6, seed=11, max_points=300)
     singles = _problems(datas)
     ref = [tc.solve(_options(), p, precision="fp64") for p in singles]
     batch = _problems(datas)
-    got = tc.solve_batch(_options(), batch, precision=precision)
+    got = tc.solve_batch(_options(), batch, precision=precision, cluster_size=cluster)
     for r, g, ps, pb in zip(ref, got, singles, batch):
         if precision == "fp64":
             np.testing.assert_allclose(g.final_cost, r.final_cost, rtol=1e-8)
