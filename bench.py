@@ -478,13 +478,131 @@ def run_kernel_pass(args):
     return 0
 
 
+def _batched_problems(tc, datas):
+    return [tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, d.observations, d.camera_index,
+                                                   d.point_index) for d in datas]
+
+
+def run_batched(args):
+    """Configuration 3: 4,096 independent instances solved in one persistent launch.
+    value = instances per second of the launch (inputs in HBM); e2e = solve_batch from
+    host arrays (upload, layout, launch, results back)."""
+    import torch
+
+    import ceres_torch_cuda_b200 as tc
+    from ceres_torch_cuda_b200 import synthetic as S
+
+    count = max(1, int(4096 * args.scale))
+    datas = S.make_batched_instances(count, seed=3)
+    opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                            preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI, max_num_iterations=50)
+    base = _batched_problems(tc, datas)
+    shape = tc.batch.autotune(opts, base, precision="mixed")
+    res = {}
+    for prec in ("mixed", "fp64"):
+        times, finals = [], None
+        for k in range(args.warmup + args.steps):
+            solver = tc.BatchSolver(base, opts, precision=prec)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            solver.launch(*shape)
+            e1.record()
+            torch.cuda.synchronize()
+            if k >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+            finals = solver.summaries()
+        res[prec] = {"ms": statistics.median(times), "summaries": finals}
+    mixed, fp64 = res["mixed"]["summaries"], res["fp64"]["summaries"]
+    rel = [abs(m.final_cost - f.final_cost) / max(f.final_cost, 1e-300) for m, f in zip(mixed, fp64)]
+    e2e = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ps = _batched_problems(tc, datas)
+        tc.solve_batch(opts, ps, precision="mixed", threads_per_cta=shape[0], ctas_per_sm=shape[1])
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    ms = res["mixed"]["ms"]
+    nobs = sum(d.num_observations for d in datas)
+    line = {
+        "metric": "batched BA solves/s (configuration 3, one persistent launch)", "value": count / (ms / 1e3),
+        "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32+f64", "data": "synthetic",
+        "config": {"workload": f"config3 {count} instances nc~U(3..32) np~U(50..2000) track~U(3..8)",
+                   "instances": count, "observations": nobs, "cta_shape": list(shape), "cluster_size": 1,
+                   "solver": "ITERATIVE_SCHUR+SCHUR_JACOBI, max 50 iterations"},
+        "fp64": {"ms": res["fp64"]["ms"], "solves_per_s": count / (res["fp64"]["ms"] / 1e3)},
+        "mixed": {"median_iterations": statistics.median(len(m.iterations) for m in mixed),
+                  "max_rel_final_cost_vs_fp64": max(rel), "median_rel_final_cost_vs_fp64": statistics.median(rel)},
+        "e2e": {"value": count / statistics.median(e2e), "unit": "solves/s",
+                "h2d_bytes_per_step": int(sum(d.cameras.nbytes + d.points.nbytes + d.observations.nbytes +
+                                              2 * 8 * d.num_observations for d in datas)),
+                "d2h_bytes_per_step": int(sum(d.cameras.nbytes + d.points.nbytes for d in datas))},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args):
+    """Configuration 4: a Poisson stream of solve requests through the continuous-batching
+    server; value = p99 latency (ms) at the offered rate, mixed precision; the float64
+    server is run on the same stream."""
+    import torch
+
+    import ceres_torch_cuda_b200 as tc
+    from ceres_torch_cuda_b200 import synthetic as S
+    from ceres_torch_cuda_b200.serving import BAServer, run_stream
+
+    rate = args.rate
+    count = max(16, int(rate * args.duration))
+    arrivals, datas = S.make_serving_requests(count, seed=4, rate_hz=rate)
+    opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                            preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI, max_num_iterations=50)
+    out = {}
+    for prec in ("mixed", "fp64"):
+        warm = BAServer(opts, precision=prec)
+        for p in _batched_problems(tc, datas[:8]):
+            warm.submit(p)
+        warm.drain()
+        probs = _batched_problems(tc, datas)
+        torch.cuda.synchronize()
+        server = BAServer(opts, precision=prec)
+        st = run_stream(server, arrivals, probs)
+        reqs = st.pop("requests_list")
+        st["median_iterations"] = statistics.median(len(r.summary.iterations) for r in reqs)
+        st["launches"] = server.launches
+        st["peak_inflight_batches"] = server.peak_inflight
+        st["final_costs"] = [r.summary.final_cost for r in reqs]
+        out[prec] = st
+    rel = [abs(a - b) / max(b, 1e-300) for a, b in zip(out["mixed"].pop("final_costs"), out["fp64"].pop("final_costs"))]
+    m = out["mixed"]
+    line = {
+        "metric": "served BA solve latency p99 (configuration 4, continuous batching)", "value": m["p99_ms"],
+        "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": m["wall_s"] * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "fp32+f64", "data": "synthetic",
+        "config": {"workload": f"config4 Poisson {rate:.0f} req/s, nc~lognormal(ln20,0.8) clip 3..500, np=250nc, "
+                               f"track~Poisson(4)+2", "requests": count,
+                   "observations": int(sum(d.num_observations for d in datas)),
+                   "server": {"cluster_size": 8, "max_inflight": 4, "threads_per_cta": 256}},
+        "mixed": m, "fp64": out["fp64"],
+        "max_rel_final_cost_mixed_vs_fp64": max(rel), "median_rel_final_cost_mixed_vs_fp64": statistics.median(rel),
+        "e2e": {"value": m["p99_ms"], "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "requests are device-resident at submission; latency = submission to solution on device"},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[0, 1, 2])
+    ap.add_argument("--config", type=int, default=2, choices=[0, 1, 2, 3, 4])
+    ap.add_argument("--rate", type=float, default=1000.0, help="configuration 4: requests per second")
+    ap.add_argument("--duration", type=float, default=2.0, help="configuration 4: seconds of arrivals")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-pass", action="store_true",
@@ -493,6 +611,10 @@ def main():
     args = ap.parse_args()
     if args.kernel_pass:
         return run_kernel_pass(args)
+    if args.impl == "ours" and args.config == 3:
+        return run_batched(args)
+    if args.impl == "ours" and args.config == 4:
+        return run_serving(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

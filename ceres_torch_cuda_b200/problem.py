@@ -19,6 +19,7 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
+import numpy as np
 import torch
 
 from .losses import LossFunction, device_loss
@@ -300,6 +301,36 @@ class BundleAdjustmentProblem:
                    t(camera_index, torch.int64), t(point_index, torch.int64), loss,
                    None if camera_constant is None else t(camera_constant, torch.bool),
                    None if point_constant is None else t(point_constant, torch.bool))
+
+    @classmethod
+    def from_bal_text(cls, text: str, *, loss=None, device: str | torch.device = "cuda"):
+        """Parse the BAL format (BALProblem.from_text, examples/simple_bundle_adjuster.py:33-70):
+        "nc np no", no lines "camera point x y", 9 nc camera values, 3 np point values,
+        whitespace separated. Vectorised (one numpy conversion of all values) instead of
+        one Python object per observation."""
+        tokens = text.split()
+        if len(tokens) < 3:
+            raise ValueError("BAL input is missing its header")
+        nc, npts, no = (int(t) for t in tokens[:3])
+        expected = 3 + 4 * no + 9 * nc + 3 * npts
+        if len(tokens) > expected:
+            raise ValueError("BAL input contains trailing values")
+        if len(tokens) < expected:
+            raise ValueError("BAL input is truncated")
+        vals = np.array(tokens[3:], dtype=np.float64)
+        obs_block = vals[:4 * no].reshape(no, 4)
+        ci, pi = obs_block[:, 0], obs_block[:, 1]
+        if not (np.all(ci == np.round(ci)) and np.all(pi == np.round(pi))):
+            raise ValueError("BAL camera and point indices must be integers")
+        cameras = vals[4 * no:4 * no + 9 * nc].reshape(nc, 9)
+        points = vals[4 * no + 9 * nc:].reshape(npts, 3)
+        return cls.from_arrays(cameras, points, obs_block[:, 2:4], ci.astype(np.int64), pi.astype(np.int64),
+                               loss=loss, device=device)
+
+    @classmethod
+    def from_bal_file(cls, path, *, loss=None, device: str | torch.device = "cuda"):
+        from pathlib import Path
+        return cls.from_bal_text(Path(path).read_text(), loss=loss, device=device)
 
     @property
     def num_cameras(self) -> int:

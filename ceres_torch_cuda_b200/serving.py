@@ -4,12 +4,13 @@ Requests wait in an arrival queue. Whenever a stream slot is free, the server
 admits waiting requests, oldest first, while their device footprint fits the
 memory budget next to the batches already running. It launches them as one
 batched persistent solve (``BatchSolver``) on a stream of its own. Batches on
-different streams run side by side on the GPU: a batch of k problems occupies k
-CTAs. Requests that arrive while others run are admitted as soon as a slot and
-memory free up. Their work overlaps on the device with the batches in flight.
+different streams run side by side on the GPU: a batch of k problems occupies at
+most k thread-block clusters. Requests that arrive while others run are admitted
+as soon as a slot and memory free up. Their work overlaps on the device with the
+batches in flight.
 
 A request's result does not depend on what it was batched with, because each
-problem is solved by one CTA from its own data.
+problem is solved by one cluster from its own data.
 
 ``BAServer.step()`` is non-blocking and does one round of completion, admission
 and launch. ``run_stream()`` replays a timed arrival stream through it and
@@ -71,7 +72,8 @@ class BAServer:
 
     ``memory_budget``: device bytes the in-flight requests may hold (default: half of
     the free memory at construction). ``max_inflight``: concurrent batches (streams).
-    ``max_batch``: requests per launch.
+    ``max_batch``: requests per launch. ``cluster_size``: CTAs (one thread-block
+    cluster) per request.
     """
 
     options: SolverOptions
@@ -81,12 +83,18 @@ class BAServer:
     max_batch: int = 512
     threads_per_cta: int = 256
     ctas_per_sm: int = 1
+    cluster_size: int = 8
     device: torch.device = field(default_factory=lambda: torch.device("cuda", torch.cuda.current_device()))
     _waiting: deque = field(default_factory=deque, init=False, repr=False)
     _flights: list = field(default_factory=list, init=False, repr=False)
     _streams: list = field(default_factory=list, init=False, repr=False)
     _in_use: int = field(default=0, init=False, repr=False)
     completed: list = field(default_factory=list, init=False, repr=False)
+    peak_inflight: int = field(default=0, init=False)
+    peak_bytes: int = field(default=0, init=False)
+    launches: int = field(default=0, init=False)
+    host_admit_s: float = field(default=0.0, init=False)      # host time building and launching batches
+    host_complete_s: float = field(default=0.0, init=False)   # host time collecting results
 
     def __post_init__(self):
         if self.memory_budget is None:
@@ -109,6 +117,7 @@ class BAServer:
     def _complete(self) -> int:
         n = 0
         still = []
+        t0 = time.perf_counter()
         for f in self._flights:
             if f.event.query():
                 f.solver.write_back()
@@ -123,6 +132,8 @@ class BAServer:
             else:
                 still.append(f)
         self._flights = still
+        if n:
+            self.host_complete_s += time.perf_counter() - t0
         return n
 
     def _admit(self) -> bool:
@@ -140,15 +151,20 @@ class BAServer:
         busy = {id(f.stream) for f in self._flights}
         stream = next(s for s in self._streams if id(s) not in busy)
         now = time.perf_counter()
+        t0 = now
         with torch.cuda.stream(stream):
             solver = BatchSolver([r.problem for r in batch], self.options, precision=self.precision, stream=stream)
-            solver.launch(self.threads_per_cta, self.ctas_per_sm)
+            solver.launch(self.threads_per_cta, self.ctas_per_sm, self.cluster_size)
             ev = torch.cuda.Event()
             ev.record(stream)
         for r in batch:
             r.admitted = now
         self._flights.append(_Flight(solver, batch, stream, ev, size))
         self._in_use += size
+        self.launches += 1
+        self.host_admit_s += time.perf_counter() - t0
+        self.peak_inflight = max(self.peak_inflight, len(self._flights))
+        self.peak_bytes = max(self.peak_bytes, self._in_use)
         return True
 
     def step(self) -> None:

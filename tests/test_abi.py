@@ -43,20 +43,21 @@ def test_abi_version_and_struct_size(lib):
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
-def test_struct_field_offsets_match_c(tmp_path):
-    fields = [f for f, _ in _lib.BAStruct._fields_]
+@pytest.mark.parametrize("ctype,mirror", [("ceres_b200_ba_t", _lib.BAStruct), ("ceres_b200_batch_t", _lib.BatchStruct)])
+def test_struct_field_offsets_match_c(tmp_path, ctype, mirror):
+    fields = [f for f, _ in mirror._fields_]
     src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {",
-           'printf("%zu\\n", sizeof(ceres_b200_ba_t));']
-    src += [f'printf("%zu\\n", offsetof(ceres_b200_ba_t, {f}));' for f in fields]
+           f'printf("%zu\\n", sizeof({ctype}));']
+    src += [f'printf("%zu\\n", offsetof({ctype}, {f}));' for f in fields]
     src += ["return 0; }"]
     c = tmp_path / "off.c"
     c.write_text("\n".join(src))
     exe = tmp_path / "off"
     subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(c)], check=True)
     out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
-    assert out[0] == ctypes.sizeof(_lib.BAStruct)
+    assert out[0] == ctypes.sizeof(mirror)
     for f, off in zip(fields, out[1:]):
-        assert getattr(_lib.BAStruct, f).offset == off, f
+        assert getattr(mirror, f).offset == off, f
 
 
 def test_stats_indices_match_header():
@@ -80,3 +81,8 @@ def test_invalid_arguments_are_rejected_without_a_gpu(lib):
     assert lib.ceres_b200_ba_step(ctypes.byref(s), None) == _lib.EINVAL
     assert lib.ceres_b200_ba_pcg(None, 2, 0, 10, 0.1, 0, None) == _lib.EINVAL
     assert lib.ceres_b200_dense_cholesky_solve(None, None, None, 4, None, None) == _lib.EINVAL
+    b = _lib.BatchStruct()
+    b.num_problems = 3  # no arrays set
+    assert lib.ceres_b200_batch_solve(ctypes.byref(b), 256, 1, 1, None) == _lib.EINVAL
+    assert lib.ceres_b200_batch_solve(None, 256, 1, 1, None) == _lib.EINVAL
+    assert lib.ceres_b200_batch_struct_bytes() == ctypes.sizeof(_lib.BatchStruct)

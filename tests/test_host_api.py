@@ -223,3 +223,29 @@ def test_snavely_residual_matches_generator_projection():
     r = cost.residuals(torch.tensor(d.cameras[d.camera_index[0]]), torch.tensor(d.points[d.point_index[0]]))
     expect = S.project(d.cameras[d.camera_index[:1]], d.points[d.point_index[:1]])[0] - d.observations[0]
     np.testing.assert_allclose(r.numpy(), expect, rtol=1e-12)
+
+
+def test_bal_text_round_trip_and_errors():
+    """BAL parsing (the format of examples/simple_bundle_adjuster.py:33-70) on CPU tensors."""
+    import numpy as np
+    import pytest
+
+    import ceres_torch_cuda_b200 as tc
+    from ceres_torch_cuda_b200 import synthetic as S
+
+    d = S.make_small_ba(3, 7, 2, seed=1)
+    lines = [f"{d.num_cameras} {d.num_points} {d.num_observations}"]
+    lines += [f"{int(c)} {int(p)} {float(x)!r} {float(y)!r}"
+              for c, p, (x, y) in zip(d.camera_index, d.point_index, d.observations)]
+    lines += [repr(float(v)) for v in d.cameras.ravel()] + [repr(float(v)) for v in d.points.ravel()]
+    text = "\n".join(lines) + "\n"
+    bal = tc.BundleAdjustmentProblem.from_bal_text(text, device="cpu")
+    np.testing.assert_array_equal(bal.cameras.numpy(), d.cameras)
+    np.testing.assert_array_equal(bal.points.numpy(), d.points)
+    np.testing.assert_array_equal(bal.observations.numpy(), d.observations)
+    np.testing.assert_array_equal(bal.camera_index.numpy(), d.camera_index)
+    np.testing.assert_array_equal(bal.point_index.numpy(), d.point_index)
+    with pytest.raises(ValueError, match="trailing"):
+        tc.BundleAdjustmentProblem.from_bal_text(text + " 1.0", device="cpu")
+    with pytest.raises(ValueError, match="truncated"):
+        tc.BundleAdjustmentProblem.from_bal_text(text.rsplit("\n", 2)[0], device="cpu")

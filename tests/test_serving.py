@@ -1,0 +1,55 @@
+"""Serving loop: continuous batching with admission by device footprint.
+
+Requests submitted in a burst run as several overlapping batches; each result
+equals the same request solved alone (float64: final cost 1e-8 relative,
+iteration count within +-2), and the in-flight footprint never exceeds the budget.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from ceres_torch_cuda_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(count=12, seed=4):
+    import ceres_torch_cuda_b200 as tc
+    arrivals, datas = S.make_serving_requests(count, seed=seed, max_cameras=12, points_per_camera=40)
+    opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                            preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI, max_num_iterations=30)
+
+    def probs():
+        return [tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, d.observations, d.camera_index,
+                                                       d.point_index) for d in datas]
+    return tc, opts, arrivals, probs
+
+
+def test_server_results_equal_alone_and_batches_overlap():
+    tc, opts, _, probs = _setup()
+    from ceres_torch_cuda_b200.serving import BAServer
+    server = BAServer(opts, precision="fp64", max_inflight=3, max_batch=3, cluster_size=2)
+    reqs = [server.submit(p) for p in probs()]
+    server.drain()
+    assert server.launches >= 4
+    assert server.peak_inflight >= 2
+    alone = [tc.solve_batch(opts, [p], precision="fp64", cluster_size=2)[0] for p in probs()]
+    for r, a in zip(reqs, alone):
+        assert r.summary is not None and r.latency is not None and r.latency >= 0
+        np.testing.assert_allclose(r.summary.final_cost, a.final_cost, rtol=1e-8)
+        assert abs(len(r.summary.iterations) - len(a.iterations)) <= 2
+
+
+def test_server_respects_memory_budget_and_stream_replay():
+    tc, opts, arrivals, probs = _setup(count=10, seed=6)
+    from ceres_torch_cuda_b200.serving import BAServer, footprint_bytes, run_stream
+    ps = probs()
+    biggest = max(footprint_bytes(p, "mixed") for p in ps)
+    server = BAServer(opts, precision="mixed", memory_budget=2 * biggest, max_inflight=4, cluster_size=1)
+    stats = run_stream(server, arrivals * 0.0 + np.linspace(0.0, 0.01, len(ps)), ps)
+    assert server.peak_bytes <= 2 * biggest
+    assert stats["requests"] == len(ps)
+    assert stats["p99_ms"] >= stats["p50_ms"] > 0
+    for r in stats["requests_list"]:
+        assert r.summary.termination_type in (tc.TerminationType.CONVERGENCE, tc.TerminationType.NO_CONVERGENCE)
