@@ -561,10 +561,9 @@ def run_serving(args):
                             preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI, max_num_iterations=50)
     out = {}
     for prec in ("mixed", "fp64"):
-        warm = BAServer(opts, precision=prec)
-        for p in _batched_problems(tc, datas[:8]):
-            warm.submit(p)
-        warm.drain()
+        # one untimed replay of the same stream first: it loads the kernels and grows
+        # the caching allocator to the stream's working set
+        run_stream(BAServer(opts, precision=prec), arrivals, _batched_problems(tc, datas))
         probs = _batched_problems(tc, datas)
         torch.cuda.synchronize()
         server = BAServer(opts, precision=prec)
@@ -573,6 +572,8 @@ def run_serving(args):
         st["median_iterations"] = statistics.median(len(r.summary.iterations) for r in reqs)
         st["launches"] = server.launches
         st["peak_inflight_batches"] = server.peak_inflight
+        st["host_admit_s"] = server.host_admit_s
+        st["host_complete_s"] = server.host_complete_s
         st["final_costs"] = [r.summary.final_cost for r in reqs]
         out[prec] = st
     rel = [abs(a - b) / max(b, 1e-300) for a, b in zip(out["mixed"].pop("final_costs"), out["fp64"].pop("final_costs"))]
@@ -584,7 +585,7 @@ def run_serving(args):
         "config": {"workload": f"config4 Poisson {rate:.0f} req/s, nc~lognormal(ln20,0.8) clip 3..500, np=250nc, "
                                f"track~Poisson(4)+2", "requests": count,
                    "observations": int(sum(d.num_observations for d in datas)),
-                   "server": {"cluster_size": 8, "max_inflight": 4, "threads_per_cta": 256}},
+                   "server": {"cluster_size": 16, "max_inflight": 16, "max_batch": 64, "threads_per_cta": 256}},
         "mixed": m, "fp64": out["fp64"],
         "max_rel_final_cost_mixed_vs_fp64": max(rel), "median_rel_final_cost_mixed_vs_fp64": statistics.median(rel),
         "e2e": {"value": m["p99_ms"], "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,

@@ -197,22 +197,24 @@ class BatchSolver:
         self.cand_cameras = torch.empty_like(self.cameras)
         self.cand_points = torch.empty_like(self.points)
         slots = max(L.num_slots, 1)
+        # padding slots keep zero Jacobians (the product walks them); every other buffer
+        # is written by the kernel before it is read
         self.jac = torch.zeros((slots, 24), dtype=jt, device=dev)
-        self.res = torch.zeros((slots, 2), **f64)
-        self.point_raw = torch.zeros((NQ, 9), **f64)
-        self.winv = torch.zeros((NQ, 6), dtype=jt, device=dev)
-        self.winv_ga = torch.zeros((NQ, 3), **f64)
-        self.step_points = torch.zeros((NQ, 3), **f64)
-        self.cam_diag = torch.zeros((NC, 9), **f64)
-        self.precond = torch.zeros((NC, 81), dtype=jt, device=dev)
-        self.rhs = torch.zeros((NC, 9), **f64)
-        self.step_cameras = torch.zeros((NC, 9), **f64)
-        self.cam_acc = torch.zeros((NC, 72), **f64)
-        self.frames = torch.zeros((NC, 24), **f64)
-        self.pcg = torch.zeros((8, 9 * NC), **f64)
+        self.res = torch.empty((slots, 2), **f64)
+        self.point_raw = torch.empty((NQ, 9), **f64)
+        self.winv = torch.empty((NQ, 6), dtype=jt, device=dev)
+        self.winv_ga = torch.empty((NQ, 3), **f64)
+        self.step_points = torch.empty((NQ, 3), **f64)
+        self.cam_diag = torch.empty((NC, 9), **f64)
+        self.precond = torch.empty((NC, 81), dtype=jt, device=dev)
+        self.rhs = torch.empty((NC, 9), **f64)
+        self.step_cameras = torch.empty((NC, 9), **f64)
+        self.cam_acc = torch.empty((NC, 72), **f64)
+        self.frames = torch.empty((NC, 24), **f64)
+        self.pcg = torch.empty((8, 9 * NC), **f64)
         self.max_trace = options.max_num_iterations + 1
-        self.result = torch.zeros((len(problems), _lib.BATCH_RESULT), **f64)
-        self.trace = torch.zeros((len(problems), self.max_trace, _lib.BATCH_TRACE), **f64)
+        self.result = torch.empty((len(problems), _lib.BATCH_RESULT), **f64)
+        self.trace = torch.empty((len(problems), self.max_trace, _lib.BATCH_TRACE), **f64)
         self.queue = torch.zeros(1, dtype=torch.int32, device=dev)
         self.stream = stream
         self.struct = self._struct(max_refinements)

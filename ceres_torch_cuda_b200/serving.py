@@ -79,11 +79,11 @@ class BAServer:
     options: SolverOptions
     precision: str = "mixed"
     memory_budget: int | None = None
-    max_inflight: int = 4
-    max_batch: int = 512
+    max_inflight: int = 16
+    max_batch: int = 64
     threads_per_cta: int = 256
     ctas_per_sm: int = 1
-    cluster_size: int = 8
+    cluster_size: int = 16
     device: torch.device = field(default_factory=lambda: torch.device("cuda", torch.cuda.current_device()))
     _waiting: deque = field(default_factory=deque, init=False, repr=False)
     _flights: list = field(default_factory=list, init=False, repr=False)
