@@ -46,13 +46,15 @@ class BatchLayout:
     num_slots: int
     has_duplicate_cameras: bool
     max_cameras: int
+    num_slices: int
 
 
 def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_index: torch.Tensor,
                        point_index: torch.Tensor, observations: torch.Tensor) -> BatchLayout:
     """``camera_index`` / ``point_index`` are global (problem offsets added). Points are
     sorted by track length (descending, stable in point id) within their problem, and
-    each problem is padded to whole slices of 32."""
+    each problem is padded to whole slices of 32. Device work on the current stream with
+    one device-to-host read (the slot count and the duplicate-camera flag)."""
     dev = camera_index.device
     B = len(cam_counts)
     ci = camera_index.to(torch.int64)
@@ -68,36 +70,46 @@ def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_ind
     slice_off = np.zeros(B + 1, dtype=np.int64)
     slice_off[1:] = np.cumsum(slices_per)
     S = int(slice_off[-1])
-    point_problem = torch.repeat_interleave(torch.arange(B, device=dev), torch.as_tensor(pt_counts, device=dev))
-    counts = torch.bincount(pi, minlength=NP) if no else torch.zeros(NP, dtype=torch.int64, device=dev)
-    maxc = int(counts.max()) + 1 if NP else 1
-    order = torch.argsort(point_problem * maxc + (maxc - 1 - counts), stable=True)  # grouped by problem
-    # position of each sorted point inside its problem -> global lane q
+    i64 = dict(dtype=torch.int64, device=dev)
+    point_problem = torch.repeat_interleave(torch.arange(B, device=dev), torch.as_tensor(pt_counts, device=dev),
+                                            output_size=NP)
+    counts = torch.zeros(NP, **i64)
+    if no:
+        counts.index_add_(0, pi, torch.ones(no, **i64))
+    # grouped by problem, then by track length descending, stable in point id
+    order = torch.argsort(point_problem * (1 << 32) + ((1 << 31) - 1 - counts), stable=True)
     start_in = torch.as_tensor(pt_off_in[:-1], device=dev)
     q_base = torch.as_tensor(32 * slice_off[:-1], device=dev)
     pos = torch.arange(NP, device=dev) - start_in[point_problem[order]]
     q_of_sorted = q_base[point_problem[order]] + pos
-    q_of_point = torch.empty(NP, dtype=torch.int64, device=dev)
+    q_of_point = torch.empty(NP, **i64)
     q_of_point[order] = q_of_sorted
-    lane_point = torch.full((32 * S,), -1, dtype=torch.int64, device=dev)
+    lane_point = torch.full((32 * S,), -1, **i64)
     lane_point[q_of_sorted] = order
-    counts_q = torch.zeros(32 * S, dtype=torch.int64, device=dev)
+    counts_q = torch.zeros(32 * S, **i64)
     counts_q[q_of_sorted] = counts[order]
     slice_len = counts_q.view(S, 32).amax(dim=1) if S else counts_q[:0]
     csum = torch.cumsum(slice_len, 0)
     slice_base = 32 * (csum - slice_len)
-    num_slots = int(32 * int(csum[-1])) if S else 0
+    dup = torch.zeros((), **i64)
+    if no > 1:
+        pk = torch.sort(pi * max(NC, 1) + ci).values
+        dup = (pk[1:] == pk[:-1]).any().to(torch.int64)
+    info = torch.stack([csum[-1] if S else torch.zeros((), **i64), dup]).cpu()
+    num_slots = 32 * int(info[0])
+    has_dup = bool(info[1])
     if no:
         obs_sorted = torch.argsort(pi, stable=True)
         pstart = torch.cumsum(counts, 0) - counts
-        rank = torch.empty(no, dtype=torch.int64, device=dev)
+        rank = torch.empty(no, **i64)
         rank[obs_sorted] = torch.arange(no, device=dev) - pstart[pi[obs_sorted]]
         q = q_of_point[pi]
         slot = slice_base[q // 32] + 32 * rank + (q % 32)
     else:
-        q = torch.zeros(0, dtype=torch.int64, device=dev)
+        q = torch.zeros(0, **i64)
         slot = q
-    cam_problem = torch.repeat_interleave(torch.arange(B, device=dev), torch.as_tensor(cam_counts, device=dev))
+    cam_problem = torch.repeat_interleave(torch.arange(B, device=dev), torch.as_tensor(cam_counts, device=dev),
+                                          output_size=NC)
     local_cam = ci - torch.as_tensor(cam_off[:-1], device=dev)[cam_problem[ci]] if no else ci
     slot_cam = torch.full((max(num_slots, 1),), -1, dtype=torch.int32, device=dev)
     slot_obs = torch.zeros((max(num_slots, 1), 2), dtype=torch.float64, device=dev)
@@ -107,20 +119,18 @@ def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_ind
     perm = torch.argsort(ci * max(num_slots, 1) + slot)
     cam_entries = torch.stack([slot[perm], q[perm]], dim=1).to(torch.int32).contiguous() if no else \
         torch.zeros((1, 2), dtype=torch.int32, device=dev)
-    cam_counts_t = torch.bincount(ci, minlength=NC) if no else torch.zeros(NC, dtype=torch.int64, device=dev)
-    cam_offsets = torch.zeros(NC + 1, dtype=torch.int64, device=dev)
+    cam_counts_t = torch.zeros(NC, **i64)
+    if no:
+        cam_counts_t.index_add_(0, ci, torch.ones(no, **i64))
+    cam_offsets = torch.zeros(NC + 1, **i64)
     cam_offsets[1:] = torch.cumsum(cam_counts_t, 0)
-    has_dup = False
-    if no > 1:
-        pk = torch.sort(pi * max(NC, 1) + ci).values
-        has_dup = bool((pk[1:] == pk[:-1]).any())
     return BatchLayout(
         num_problems=B, cam_off=torch.as_tensor(cam_off, dtype=torch.int32, device=dev),
         slice_off=torch.as_tensor(slice_off, dtype=torch.int32, device=dev),
         slice_base=slice_base.to(torch.int32).contiguous(), slice_len=slice_len.to(torch.int32).contiguous(),
         slot_cam=slot_cam, slot_obs=slot_obs, cam_offsets=cam_offsets.to(torch.int32).contiguous(),
         cam_entries=cam_entries, lane_point=lane_point, num_slots=num_slots, has_duplicate_cameras=has_dup,
-        max_cameras=int(cam_counts.max()) if B else 0)
+        max_cameras=int(cam_counts.max()) if B else 0, num_slices=S)
 
 
 def _check_options(options: SolverOptions) -> None:
@@ -177,23 +187,24 @@ class BatchSolver:
         obs = torch.cat([p.observations.to(dev, torch.float64) for p in problems])
         L = build_batch_layout(cam_counts, pt_counts, ci, pi, obs)
         self.layout = L
-        S = int(L.slice_off[-1].item()) if L.num_problems else 0
+        S = L.num_slices
         NQ = 32 * S
         NC = int(cam_off[-1])
         f64 = dict(dtype=torch.float64, device=dev)
         jt = torch.float32 if precision == "mixed" else torch.float64
         self.cameras = torch.cat([p.cameras.to(**f64) for p in problems]).contiguous()
-        pts_in = torch.cat([p.points.to(**f64) for p in problems])
-        self.points = torch.zeros((NQ, 3), **f64)
-        valid = L.lane_point >= 0
-        self.points[valid] = pts_in[L.lane_point[valid]]
+        # lanes -> input points; padding lanes (-1) read a zero row appended at the end
+        NPin = int(pt_off[-1])
+        self.lane_src = torch.where(L.lane_point >= 0, L.lane_point, torch.full_like(L.lane_point, NPin))
+        pts_in = torch.cat([p.points.to(**f64) for p in problems] + [torch.zeros((1, 3), **f64)])
+        self.points = pts_in.index_select(0, self.lane_src).contiguous()
         cam_const = torch.cat([(p.camera_constant if p.camera_constant is not None else
                                 torch.zeros(p.num_cameras, dtype=torch.bool, device=dev)).to(dev) for p in problems])
         pc_in = torch.cat([(p.point_constant if p.point_constant is not None else
-                            torch.zeros(p.num_points, dtype=torch.bool, device=dev)).to(dev) for p in problems])
+                            torch.zeros(p.num_points, dtype=torch.bool, device=dev)).to(dev) for p in problems]
+                          + [torch.ones(1, dtype=torch.bool, device=dev)])  # padding lanes are constant
         self.cam_const = cam_const.to(torch.uint8).contiguous()
-        self.pt_const = torch.ones(NQ, dtype=torch.uint8, device=dev)  # padding lanes are constant
-        self.pt_const[valid] = pc_in[L.lane_point[valid]].to(torch.uint8)
+        self.pt_const = pc_in.index_select(0, self.lane_src).to(torch.uint8).contiguous()
         self.cand_cameras = torch.empty_like(self.cameras)
         self.cand_points = torch.empty_like(self.points)
         slots = max(L.num_slots, 1)
@@ -269,10 +280,8 @@ class BatchSolver:
 
     def write_back(self) -> None:
         """Solved parameters into each problem's tensors."""
-        L = self.layout
-        valid = L.lane_point >= 0
-        pts = torch.empty((int(self.pt_off_np[-1]), 3), dtype=torch.float64, device=self.device)
-        pts[L.lane_point[valid]] = self.points[valid]
+        pts = torch.empty((int(self.pt_off_np[-1]) + 1, 3), dtype=torch.float64, device=self.device)
+        pts.index_copy_(0, self.lane_src, self.points)  # padding lanes land in the extra last row
         for i, p in enumerate(self.problems):
             with torch.no_grad():
                 p.cameras.copy_(self.cameras[self.cam_off_np[i]:self.cam_off_np[i + 1]].to(p.cameras.dtype))

@@ -43,6 +43,19 @@ def footprint_bytes(problem: BundleAdjustmentProblem, precision: str) -> int:
     return slots * per_slot + no * per_obs + nq * per_point + nc * per_camera
 
 
+_STREAMS: dict = {}
+
+
+def _stream_pool(device: torch.device, count: int) -> list:
+    """Streams shared by every server on a device. The caching allocator keeps freed
+    blocks per stream, so a server on fresh streams would grow the allocator (and call
+    cudaMalloc) during its first batches; reusing the streams reuses those blocks."""
+    pool = _STREAMS.setdefault(str(device), [])
+    while len(pool) < count:
+        pool.append(torch.cuda.Stream(device))
+    return pool[:count]
+
+
 @dataclass
 class Request:
     problem: BundleAdjustmentProblem
@@ -73,17 +86,21 @@ class BAServer:
     ``memory_budget``: device bytes the in-flight requests may hold (default: half of
     the free memory at construction). ``max_inflight``: concurrent batches (streams).
     ``max_batch``: requests per launch. ``cluster_size``: CTAs (one thread-block
-    cluster) per request.
+    cluster) per request. A launch waits until ``min_batch`` requests are waiting or
+    the oldest has waited ``batch_window_s`` (fewer, larger launches for less host time
+    per request).
     """
 
     options: SolverOptions
     precision: str = "mixed"
     memory_budget: int | None = None
     max_inflight: int = 16
-    max_batch: int = 64
+    max_batch: int = 16
     threads_per_cta: int = 256
     ctas_per_sm: int = 1
     cluster_size: int = 16
+    min_batch: int = 4                   # launch once this many requests wait ...
+    batch_window_s: float = 0.001        # ... or the oldest has waited this long
     device: torch.device = field(default_factory=lambda: torch.device("cuda", torch.cuda.current_device()))
     _waiting: deque = field(default_factory=deque, init=False, repr=False)
     _flights: list = field(default_factory=list, init=False, repr=False)
@@ -100,7 +117,7 @@ class BAServer:
         if self.memory_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             self.memory_budget = int(free * 0.5)
-        self._streams = [torch.cuda.Stream(self.device) for _ in range(self.max_inflight)]
+        self._streams = _stream_pool(self.device, self.max_inflight)
 
     def submit(self, problem: BundleAdjustmentProblem, arrival: float | None = None) -> Request:
         r = Request(problem, time.perf_counter() if arrival is None else arrival,
@@ -138,6 +155,9 @@ class BAServer:
 
     def _admit(self) -> bool:
         if not self._waiting or len(self._flights) >= self.max_inflight:
+            return False
+        if len(self._waiting) < self.min_batch and \
+                time.perf_counter() - self._waiting[0].arrival < self.batch_window_s:
             return False
         batch, size = [], 0
         while self._waiting and len(batch) < self.max_batch:
