@@ -353,12 +353,12 @@ def run_ours(args):
     return 0
 
 
-# DRAM traffic of the PCG kernel from one ncu capture (profiles/k_pcg_kernel_pass_ring_1.5M_obs.md):
-# k_pcg<float>, 10 iterations on the 1,503,061-observation problem (bench.py --kernel-pass
-# --scale 0.25), dram__bytes_read.sum + dram__bytes_write.sum = 1726.3 MB + 79.2 MB.
+# DRAM traffic of the PCG kernel from one ncu capture (--set full of k_pcg<float> on
+# `bench.py --kernel-pass --scale 0.25`: 10 iterations on the 1,503,061-observation
+# problem): dram__bytes_read.sum + dram__bytes_write.sum = 1722.2 MB + 83.6 MB.
 # Traffic grows with the observations (the Jacobian store is re-read every iteration), so
 # a launch on the full workload is credited that traffic per iteration and observation.
-PCG_CAPTURE = {"observations": 1503061, "iterations": 10, "dram_bytes": 1726.291e6 + 79.1936e6}
+PCG_CAPTURE = {"observations": 1503061, "iterations": 10, "dram_bytes": 1722.210e6 + 83.622e6}
 
 
 def pcg_traffic_per_launch(observations: int, iterations_per_launch: float) -> float:
