@@ -585,8 +585,9 @@ def run_serving(args):
         "config": {"workload": f"config4 Poisson {rate:.0f} req/s, nc~lognormal(ln20,0.8) clip 3..500, np=250nc, "
                                f"track~Poisson(4)+2", "requests": count,
                    "observations": int(sum(d.num_observations for d in datas)),
-                   "server": {"cluster_size": 16, "max_inflight": 16, "max_batch": 16, "min_batch": 4,
-                              "batch_window_ms": 1.0, "threads_per_cta": 256}},
+                   "server": {"cluster_size": "4 / 8 / 16 below 20k / 80k / above observations",
+                              "max_inflight": 16, "max_batch": 16, "min_batch": 4, "batch_window_ms": 1.0,
+                              "threads_per_cta": 256}},
         "mixed": m, "fp64": out["fp64"],
         "max_rel_final_cost_mixed_vs_fp64": max(rel), "median_rel_final_cost_mixed_vs_fp64": statistics.median(rel),
         "e2e": {"value": m["p99_ms"], "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,

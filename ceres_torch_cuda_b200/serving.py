@@ -86,7 +86,8 @@ class BAServer:
     ``memory_budget``: device bytes the in-flight requests may hold (default: half of
     the free memory at construction). ``max_inflight``: concurrent batches (streams).
     ``max_batch``: requests per launch. ``cluster_size``: CTAs (one thread-block
-    cluster) per request. A launch waits until ``min_batch`` requests are waiting or
+    cluster) per request, or 0 to pick it from the request's observation count
+    (``size_classes``: small requests on small clusters leave room for more of them). A launch waits until ``min_batch`` requests are waiting or
     the oldest has waited ``batch_window_s`` (fewer, larger launches for less host time
     per request).
     """
@@ -98,7 +99,8 @@ class BAServer:
     max_batch: int = 16
     threads_per_cta: int = 256
     ctas_per_sm: int = 1
-    cluster_size: int = 16
+    cluster_size: int = 0                # 0: by request size (size_classes)
+    size_classes: tuple = ((20_000, 4), (80_000, 8), (None, 16))  # (observations below, cluster size)
     min_batch: int = 4                   # launch once this many requests wait ...
     batch_window_s: float = 0.001        # ... or the oldest has waited this long
     device: torch.device = field(default_factory=lambda: torch.device("cuda", torch.cuda.current_device()))
@@ -159,13 +161,22 @@ class BAServer:
         if len(self._waiting) < self.min_batch and \
                 time.perf_counter() - self._waiting[0].arrival < self.batch_window_s:
             return False
-        batch, size = [], 0
-        while self._waiting and len(batch) < self.max_batch:
-            r = self._waiting[0]
-            if self._in_use + size + r.footprint > self.memory_budget:
-                break
-            batch.append(self._waiting.popleft())
-            size += r.footprint
+        # the oldest request sets the cluster size; waiting requests of the same size class
+        # join it in arrival order
+        G = self._cluster_for(self._waiting[0])
+        batch, size, rest = [], 0, deque()
+        while self._waiting:
+            r = self._waiting.popleft()
+            if (len(batch) < self.max_batch and self._cluster_for(r) == G
+                    and self._in_use + size + r.footprint <= self.memory_budget):
+                batch.append(r)
+                size += r.footprint
+            else:
+                rest.append(r)
+                if not batch:  # the oldest does not fit yet: keep the order and wait
+                    rest.extend(self._waiting)
+                    self._waiting.clear()
+        self._waiting = rest
         if not batch:
             return False
         busy = {id(f.stream) for f in self._flights}
@@ -174,7 +185,7 @@ class BAServer:
         t0 = now
         with torch.cuda.stream(stream):
             solver = BatchSolver([r.problem for r in batch], self.options, precision=self.precision, stream=stream)
-            solver.launch(self.threads_per_cta, self.ctas_per_sm, self.cluster_size)
+            solver.launch(self.threads_per_cta, self.ctas_per_sm, G)
             ev = torch.cuda.Event()
             ev.record(stream)
         for r in batch:
@@ -186,6 +197,15 @@ class BAServer:
         self.peak_inflight = max(self.peak_inflight, len(self._flights))
         self.peak_bytes = max(self.peak_bytes, self._in_use)
         return True
+
+    def _cluster_for(self, r: Request) -> int:
+        if self.cluster_size:
+            return self.cluster_size
+        no = r.problem.num_observations
+        for limit, g in self.size_classes:
+            if limit is None or no < limit:
+                return g
+        return self.size_classes[-1][1]
 
     def step(self) -> None:
         """One non-blocking round: finish completed batches, then launch waiting requests."""

@@ -29,12 +29,17 @@ def _setup(count=12, seed=4):
 def test_server_results_equal_alone_and_batches_overlap():
     tc, opts, _, probs = _setup()
     from ceres_torch_cuda_b200.serving import BAServer
-    server = BAServer(opts, precision="fp64", max_inflight=3, max_batch=3, cluster_size=2)
-    reqs = [server.submit(p) for p in probs()]
+    ps = probs()
+    cut = int(np.median([p.num_observations for p in ps]))
+    classes = ((cut, 1), (None, 2))  # two size classes, so batches of both cluster sizes run
+    server = BAServer(opts, precision="fp64", max_inflight=3, max_batch=3, cluster_size=0, size_classes=classes,
+                      min_batch=1)
+    reqs = [server.submit(p) for p in ps]
     server.drain()
     assert server.launches >= 4
     assert server.peak_inflight >= 2
-    alone = [tc.solve_batch(opts, [p], precision="fp64", cluster_size=2)[0] for p in probs()]
+    alone = [tc.solve_batch(opts, [p], precision="fp64", cluster_size=1 if p.num_observations < cut else 2)[0]
+             for p in probs()]
     for r, a in zip(reqs, alone):
         assert r.summary is not None and r.latency is not None and r.latency >= 0
         np.testing.assert_allclose(r.summary.final_cost, a.final_cost, rtol=1e-8)
@@ -46,7 +51,8 @@ def test_server_respects_memory_budget_and_stream_replay():
     from ceres_torch_cuda_b200.serving import BAServer, footprint_bytes, run_stream
     ps = probs()
     biggest = max(footprint_bytes(p, "mixed") for p in ps)
-    server = BAServer(opts, precision="mixed", memory_budget=2 * biggest, max_inflight=4, cluster_size=1)
+    server = BAServer(opts, precision="mixed", memory_budget=2 * biggest, max_inflight=4, cluster_size=1,
+                      min_batch=1)
     stats = run_stream(server, arrivals * 0.0 + np.linspace(0.0, 0.01, len(ps)), ps)
     assert server.peak_bytes <= 2 * biggest
     assert stats["requests"] == len(ps)
