@@ -328,6 +328,7 @@ def run_ours(args):
             "mixed": {"iterations_to_tol": len(summaries[-1].iterations),
                       "time_to_tol_steps_s": ttts,
                       "iterations_to_tol_steps": [len(s.iterations) for s in summaries],
+                      "preprocessor_s_steps": [s.preprocessor_time_in_seconds for s in summaries],
                       "e2e_steps_s": e2e_vals,
                       "best_cost": summaries[-1].final_cost,
                       "rel_err_vs_fp64_minimum": (summaries[-1].final_cost - cstar) / cstar,

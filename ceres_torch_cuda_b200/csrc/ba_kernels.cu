@@ -524,16 +524,14 @@ __device__ __forceinline__ void camera_product(const T* rv, const TP* __restrict
   }
 }
 
-template <typename T, typename TP, typename A, bool kCrossP = false>
-__device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int gw,
-                                              int nw) {
+// The product contribution of one slice s (lane = point), accumulated into y.
+template <typename T, typename TP, typename A, bool kCrossP>
+__device__ __forceinline__ void matvec_one_slice(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int s,
+                                                 int lane) {
   constexpr int U = Unroll<T>::v;
-  const int lane = threadIdx.x & 31;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  for (int r = 0; r * nw < ba.num_slices; ++r) {
-    const int s = snake_slice(r, gw, nw);
-    if (s >= ba.num_slices) continue;
+  {
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s] + lane;
@@ -611,6 +609,39 @@ __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const T
 #pragma unroll
       for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[j] * v0 + (A)rv[9 + j] * v1);
     }
+  }
+}
+
+// Static slice walk: warp gw of nw takes the slices of snake_slice(r, gw, nw).
+template <typename T, typename TP, typename A, bool kCrossP = false>
+__device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int gw,
+                                              int nw) {
+  const int lane = threadIdx.x & 31;
+  for (int r = 0; r * nw < ba.num_slices; ++r) {
+    const int s = snake_slice(r, gw, nw);
+    if (s >= ba.num_slices) continue;
+    matvec_one_slice<T, TP, A, kCrossP>(ba, pvec, y, s, lane);
+  }
+}
+
+// Balanced slice walk for the persistent PCG: CTA b owns one slice of every round of
+// gridDim.x slices (snake order over the CTAs, so the CTAs' totals agree to a few per
+// cent although slices are sorted by length), and its warps take the CTA's slices in
+// that order from a shared-memory counter (*counter zero on entry), longest first.
+// A static warp-by-warp assignment left the heaviest CTA with 1.3x the mean work, and
+// every CTA waited for it at the grid barrier.
+template <typename T, typename TP, typename A, bool kCrossP = false>
+__device__ __forceinline__ void matvec_slices_cta(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y,
+                                                  int* counter) {
+  const int lane = threadIdx.x & 31;
+  const int G = gridDim.x, b = blockIdx.x;
+  for (;;) {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(counter, 1);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    const long long s = (long long)i * G + ((i & 1) ? G - 1 - b : b);
+    if (s >= ba.num_slices) break;
+    matvec_one_slice<T, TP, A, kCrossP>(ba, pvec, y, (int)s, lane);
   }
 }
 
@@ -706,6 +737,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   __shared__ double red[2 * (kPcgBlock / 32)];
   __shared__ double sred[kPcgBlock];
   __shared__ double bcast[4];
+  __shared__ int slice_counter;
   const int n = a.n;
   T* ps = reinterpret_cast<T*>(smem_raw);
   T* ys = ps + ((n + 3) & ~3);
@@ -793,8 +825,9 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
           ys[j] = (T)0;
           if (j >= j0 && j < j1) Pnew[j] = pv;
         }
+        if (threadIdx.x == 0) slice_counter = 0;
         __syncthreads();
-        matvec_slices<T, T, T>(ba, ps, ys, gw, nw);
+        matvec_slices_cta<T, T, T>(ba, ps, ys, &slice_counter);
         __syncthreads();
         T* my = part_y + (size_t)blockIdx.x * n;
         for (int j = threadIdx.x; j < n; j += blockDim.x) my[j] = ys[j];
