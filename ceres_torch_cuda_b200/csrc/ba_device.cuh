@@ -581,6 +581,18 @@ __device__ inline void block9_inverse(double A[81], double inv[81]) {
 // Slices in "snake" order: round r of the grid-stride walk runs forward on even
 // rounds and backward on odd ones, so with slices sorted by length every warp
 // gets a mix of long and short tracks.
+// Balanced slice schedule: CTA b owns one slice of every round of gridDim.x slices
+// (snake order over the CTAs, so the CTAs' totals agree to a few per cent although the
+// slices are sorted by length) and its warps pull them in that order, longest first,
+// from a shared-memory counter (zero when the CTA starts). Returns -1 when done.
+__device__ __forceinline__ int next_cta_slice(int* counter, int num_slices) {
+  int i = 0;
+  if ((threadIdx.x & 31) == 0) i = atomicAdd(counter, 1);
+  i = __shfl_sync(0xffffffffu, i, 0);
+  const long long s = (long long)i * gridDim.x + ((i & 1) ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x);
+  return s < num_slices ? (int)s : -1;
+}
+
 __device__ __forceinline__ int snake_slice(int r, int gw, int nw) {
   return r * nw + ((r & 1) ? nw - 1 - gw : gw);
 }

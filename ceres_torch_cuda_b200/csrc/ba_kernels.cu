@@ -130,14 +130,14 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
   __shared__ double red[kWarpBlock / 32];
   const LossSpec L = loss_spec(ba);
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   double cost = 0.0;
   unsigned err = 0;
   T* __restrict__ jac = reinterpret_cast<T*>(ba.jac);
-  for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
-    const int s = snake_slice(r_, gw, nw);
-    if (s >= ba.num_slices) continue;
+  __shared__ int slice_counter;
+  if (threadIdx.x == 0) slice_counter = 0;
+  __syncthreads();
+  for (int s = next_cta_slice(&slice_counter, ba.num_slices); s >= 0;
+       s = next_cta_slice(&slice_counter, ba.num_slices)) {
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
@@ -983,12 +983,12 @@ __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step
   __shared__ double red[5 * (kWarpBlock / 32)];
   const LossSpec L = loss_spec(ba);
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
   double cand = 0.0, model = 0.0, sq = 0.0, nonfinite = 0.0, state = 0.0;
   unsigned err = 0;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
     const int s = snake_slice(r_, gw, nw);
     if (s >= ba.num_slices) continue;
