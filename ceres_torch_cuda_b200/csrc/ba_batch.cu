@@ -725,12 +725,15 @@ __device__ void cl_step(const ceres_b200_batch_t& B, const LossSpec& L, const Pr
     const int len = B.slice_len[s];
     const size_t base = (size_t)B.slice_base[s] + lane;
     double t[3] = {0, 0, 0};
+    double sa = 0.0;  // sum_o r_o.a_o + 0.5 |a_o|^2 with a_o = Jc_o dc
     for (int k = 0; k < len; ++k) {
       const size_t slot = base + 32 * (size_t)k;
-      const int c = max(B.slot_cam[slot], 0);
+      const int c = B.slot_cam[slot];
       T rv[kRec];
       rec_load<false>(jac, slot, rv);
-      const double* dc = dcv + 9 * (size_t)c;
+      double2 r = reinterpret_cast<const double2*>(B.res)[slot];
+      if (c < 0) r = make_double2(0.0, 0.0);  // padding: zero Jacobian, camera 0 as the address
+      const double* dc = dcv + 9 * (size_t)max(c, 0);
       double u0 = 0.0, u1 = 0.0;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
@@ -740,7 +743,11 @@ __device__ void cl_step(const ceres_b200_batch_t& B, const LossSpec& L, const Pr
       }
 #pragma unroll
       for (int m = 0; m < 3; ++m) t[m] += (double)rv[18 + m] * u0 + (double)rv[21 + m] * u1;
+      sa += r.x * u0 + r.y * u1 + 0.5 * (u0 * u0 + u1 * u1);
     }
+    // model decrease of the track: -sa - dp.(g + t) - 0.5 dp^T V dp, with V and g the
+    // point sums of the evaluation (the per-observation form expanded, so the records
+    // are read once)
     double dp[3] = {0, 0, 0};
     if (!B.pt_const[q]) {
       double wi[6];
@@ -754,7 +761,15 @@ __device__ void cl_step(const ceres_b200_batch_t& B, const LossSpec& L, const Pr
         if (!isfinite(dp[m])) nonfinite += 1.0;
         sq += dp[m] * dp[m];
       }
+      const double* pr = B.point_raw + 9 * (size_t)q;
+      double V[6], Vdp[3];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) V[i] = pr[i];
+      sym3_mul(V, dp, Vdp);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) model -= dp[m] * (pr[6 + m] + t[m] + 0.5 * Vdp[m]);
     }
+    model -= sa;
     double Xc[3];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
@@ -767,21 +782,6 @@ __device__ void cl_step(const ceres_b200_batch_t& B, const LossSpec& L, const Pr
       const size_t slot = base + 32 * (size_t)k;
       const int c = B.slot_cam[slot];
       if (c < 0) continue;
-      T rv[kRec];
-      rec_load<false>(jac, slot, rv);
-      const double2 r = reinterpret_cast<const double2*>(B.res)[slot];
-      const double* dc = dcv + 9 * (size_t)c;
-      double j0 = 0.0, j1 = 0.0;
-#pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        const double dj = ldx(dc + j);
-        j0 += (double)rv[j] * dj;
-        j1 += (double)rv[9 + j] * dj;
-      }
-#pragma unroll
-      for (int m = 0; m < 3; ++m) { j0 += (double)rv[18 + m] * dp[m]; j1 += (double)rv[21 + m] * dp[m]; }
-      const double a0 = r.x + j0, a1 = r.y + j1;
-      model += 0.5 * (r.x * r.x + r.y * r.y) - 0.5 * (a0 * a0 + a1 * a1);
       const double2 ob = reinterpret_cast<const double2*>(B.slot_obs)[slot];
       Proj pj;
       CamRot R;

@@ -978,6 +978,12 @@ __global__ void k_camera_step(ceres_b200_ba_t ba, double* partials) {
   grid_finish<3>(v, 0u, partials, &ba.counters[kCtrCamStep], ba.stats, out, red);
 }
 
+// The model decrease sum_o 0.5|r_o|^2 - 0.5|r_o + Jc_o dc + Jp_o dp|^2 of a point's
+// track is expanded as -sum_o (r_o.a_o + 0.5|a_o|^2) - dp.(g + t) - 0.5 dp^T V dp with
+// a_o = Jc_o dc, t = sum_o Jp_o^T a_o, and V = sum_o Jp_o^T Jp_o, g = sum_o Jp_o^T r_o
+// the point sums of the evaluation (point_raw). The first pass over the track reads the
+// Jacobian records and residuals once; the second pass (candidate cost) reads only the
+// observations and the candidate camera frames.
 template <typename T>
 __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step(ceres_b200_ba_t ba, double* partials, const double* __restrict__ frames) {
   __shared__ double red[5 * (kWarpBlock / 32)];
@@ -996,38 +1002,47 @@ __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
     double t[3] = {0, 0, 0};
-    // padding slots have zero Jacobians: read them with camera 0 as the address
+    double sa = 0.0;  // sum_o r_o.a_o + 0.5 |a_o|^2
+    // padding slots have zero Jacobians: read them with camera 0 as the address and a
+    // zero residual
     int k = 0;
     for (; k + 2 <= len; k += 2) {
       int c[2];
       T rv[2][kRec];
+      double2 r[2];
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
         const size_t slot = base + 32 * (size_t)(k + u) + lane;
-        c[u] = max(ba.slot_cam[slot], 0);
+        c[u] = ba.slot_cam[slot];
         load_rec(jac, slot, rv[u]);
+        r[u] = reinterpret_cast<const double2*>(ba.res)[slot];
       }
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
-        const double* dc = ba.step_cameras + 9 * (size_t)c[u];
+        if (c[u] < 0) r[u] = make_double2(0.0, 0.0);
+        const double* dc = ba.step_cameras + 9 * (size_t)max(c[u], 0);
         double u0 = 0.0, u1 = 0.0;
 #pragma unroll
         for (int j = 0; j < 9; ++j) { u0 += (double)rv[u][j] * dc[j]; u1 += (double)rv[u][9 + j] * dc[j]; }
 #pragma unroll
         for (int m = 0; m < 3; ++m) t[m] += (double)rv[u][18 + m] * u0 + (double)rv[u][21 + m] * u1;
+        sa += r[u].x * u0 + r[u].y * u1 + 0.5 * (u0 * u0 + u1 * u1);
       }
     }
     for (; k < len; ++k) {
       const size_t slot = base + 32 * (size_t)k + lane;
-      const int c = max(ba.slot_cam[slot], 0);
+      const int c = ba.slot_cam[slot];
       T rv[kRec];
       load_rec(jac, slot, rv);
-      const double* dc = ba.step_cameras + 9 * (size_t)c;
+      double2 r = reinterpret_cast<const double2*>(ba.res)[slot];
+      if (c < 0) r = make_double2(0.0, 0.0);
+      const double* dc = ba.step_cameras + 9 * (size_t)max(c, 0);
       double u0 = 0.0, u1 = 0.0;
 #pragma unroll
       for (int j = 0; j < 9; ++j) { u0 += (double)rv[j] * dc[j]; u1 += (double)rv[9 + j] * dc[j]; }
 #pragma unroll
       for (int m = 0; m < 3; ++m) t[m] += (double)rv[18 + m] * u0 + (double)rv[21 + m] * u1;
+      sa += r.x * u0 + r.y * u1 + 0.5 * (u0 * u0 + u1 * u1);
     }
     double dp[3] = {0, 0, 0};
     const bool pconst = ba.pt_const[q] != 0;
@@ -1043,7 +1058,15 @@ __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step
         if (!isfinite(dp[m])) nonfinite += 1.0;
         sq += dp[m] * dp[m];
       }
+      const double* pr = ba.point_raw + 9 * (size_t)q;
+      double V[6], Vdp[3];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) V[i] = pr[i];
+      sym3_mul(V, dp, Vdp);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) model -= dp[m] * (pr[6 + m] + t[m] + 0.5 * Vdp[m]);
     }
+    model -= sa;
     double Xc[3];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
@@ -1056,17 +1079,6 @@ __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step
       const size_t slot = base + 32 * (size_t)k + lane;
       const int c = ba.slot_cam[slot];
       if (c < 0) continue;
-      T rv[kRec];
-      load_rec(jac, slot, rv);
-      const double2 r = reinterpret_cast<const double2*>(ba.res)[slot];
-      const double* dc = ba.step_cameras + 9 * (size_t)c;
-      double j0 = 0.0, j1 = 0.0;
-#pragma unroll
-      for (int j = 0; j < 9; ++j) { j0 += (double)rv[j] * dc[j]; j1 += (double)rv[9 + j] * dc[j]; }
-#pragma unroll
-      for (int m = 0; m < 3; ++m) { j0 += (double)rv[18 + m] * dp[m]; j1 += (double)rv[21 + m] * dp[m]; }
-      const double a0 = r.x + j0, a1 = r.y + j1;
-      model += 0.5 * (r.x * r.x + r.y * r.y) - 0.5 * (a0 * a0 + a1 * a1);
       const double2 ob = reinterpret_cast<const double2*>(ba.slot_obs)[slot];
       Proj o;
       CamRot R;
