@@ -41,23 +41,9 @@ template <typename V>
 __device__ __forceinline__ V ldx(const V* p) { return __ldcg(p); }  // cross-CTA data
 
 // Jacobian record loads; kCross: through L2 only.
-template <bool kCross>
-__device__ __forceinline__ void rec_load(const float* base, size_t slot, float v[kRec]) {
-  const float4* p = reinterpret_cast<const float4*>(base + slot * kRec);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    const float4 t = kCross ? __ldcg(p + i) : p[i];
-    v[4 * i] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
-  }
-}
-template <bool kCross>
-__device__ __forceinline__ void rec_load(const double* base, size_t slot, double v[kRec]) {
-  const double2* p = reinterpret_cast<const double2*>(base + slot * kRec);
-#pragma unroll
-  for (int i = 0; i < 12; ++i) {
-    const double2 t = kCross ? __ldcg(p + i) : p[i];
-    v[2 * i] = t.x; v[2 * i + 1] = t.y;
-  }
+template <bool kCross, typename T>
+__device__ __forceinline__ void rec_load(const T* base, size_t slot, T v[kRec]) {
+  load_rec<kCross>(base, slot, v);
 }
 
 struct Ctx {
@@ -1048,6 +1034,7 @@ int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta,
       !B.trace || !B.queue)
     return CERES_B200_EINVAL;
   if (B.precision != CERES_B200_FP32 && B.precision != CERES_B200_FP64) return CERES_B200_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(B.jac) & 31) != 0) return CERES_B200_EINVAL;  // 256-bit record loads
   if (B.max_cameras < 0 || B.max_trace < 1 || B.max_num_iterations < 0) return CERES_B200_EINVAL;
   if (B.preconditioner < CERES_B200_PRECOND_IDENTITY || B.preconditioner > CERES_B200_PRECOND_SCHUR_JACOBI)
     return CERES_B200_EINVAL;

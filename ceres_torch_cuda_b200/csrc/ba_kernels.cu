@@ -280,7 +280,8 @@ template <typename T>
 __device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ jac, int e,
                                              CamObs<T>& o) {
   o.ent = reinterpret_cast<const int2*>(ba.cam_entries)[e];
-  load_rec(jac, (size_t)o.ent.x, o.rv);
+  if constexpr (sizeof(T) == 4) load_rec128(jac, (size_t)o.ent.x, o.rv);
+  else load_rec(jac, (size_t)o.ent.x, o.rv);
   o.r = reinterpret_cast<const double2*>(ba.res)[o.ent.x];
 }
 
@@ -1310,6 +1311,7 @@ bool valid(const ceres_b200_ba_t* ba) {
     return false;
   if (ba->num_cameras > 0 && (!ba->cam_offsets || !ba->cam_const || !ba->cam_diag || !ba->rhs || !ba->precond))
     return false;
+  if ((reinterpret_cast<uintptr_t>(ba->jac) & 31) != 0) return false;  // 256-bit record loads
   return true;
 }
 

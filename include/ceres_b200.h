@@ -126,7 +126,7 @@ typedef struct ceres_b200_ba_t {
   double* cand_points;         /* [num_points][3] */
 
   /* per-slot evaluation */
-  void* jac;                   /* [num_slots][24] float or double */
+  void* jac;                   /* [num_slots][24] float or double, 32-byte aligned */
   double* res;                 /* [num_slots][2] corrected residuals */
 
   /* point-side Schur pieces */
@@ -353,7 +353,7 @@ typedef struct ceres_b200_batch_t {
   double* points;               /* [32 * total slices][3] sorted order, solved in place */
   double* cand_cameras;
   double* cand_points;
-  void* jac;                    /* [slots][24] float or double */
+  void* jac;                    /* [slots][24] float or double, 32-byte aligned */
   double* res;                  /* [slots][2] */
   double* point_raw;            /* [points][9] */
   void* winv;                   /* [points][6] float or double */
