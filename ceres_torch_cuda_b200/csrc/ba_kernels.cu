@@ -274,15 +274,21 @@ struct CamObs {
   int2 ent;  // (slot, sorted point)
   T rv[kRec];
   double2 r;
+  T wi[6];
+  double wg[3];
 };
 
 template <typename T>
-__device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ jac, int e,
-                                             CamObs<T>& o) {
-  o.ent = reinterpret_cast<const int2*>(ba.cam_entries)[e];
-  if constexpr (sizeof(T) == 4) load_rec128(jac, (size_t)o.ent.x, o.rv);
-  else load_rec(jac, (size_t)o.ent.x, o.rv);
-  o.r = reinterpret_cast<const double2*>(ba.res)[o.ent.x];
+__device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ jac,
+                                             const T* __restrict__ winv, int2 ent, CamObs<T>& o) {
+  o.ent = ent;
+  if constexpr (sizeof(T) == 4) load_rec128(jac, (size_t)ent.x, o.rv);
+  else load_rec(jac, (size_t)ent.x, o.rv);
+  o.r = reinterpret_cast<const double2*>(ba.res)[ent.x];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) o.wi[i] = winv[6 * (size_t)ent.y + i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) o.wg[i] = ba.winv_ga[3 * (size_t)ent.y + i];
 }
 
 // Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
@@ -303,17 +309,28 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
   const bool cconst = ba.cam_const[c] != 0;
   const int e0 = ba.cam_offsets[c], e1 = ba.cam_offsets[c + 1];
   if (!cconst) {
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);
+    const int stride = blockDim.x;
+    const int first = e0 + threadIdx.x;
+    // entries are read two observations ahead, so each observation waits for one
+    // gather (its data) instead of two (entry, then data): 0.43 -> 0.39 ms on the
+    // 6.0M-observation problem (float32 store). Holding the next observation's data in
+    // registers as well spilled and ran slower.
+    int2 en1 = first < e1 ? ents[first] : make_int2(0, 0);
+    int2 en2 = first + stride < e1 ? ents[first + stride] : make_int2(0, 0);
+    for (int e = first; e < e1; e += stride) {
       CamObs<T> cur;
-      cam_obs_load(ba, jac, e, cur);
+      cam_obs_load(ba, jac, winv, en1, cur);
+      en1 = en2;
+      en2 = e + 2 * stride < e1 ? ents[e + 2 * stride] : make_int2(0, 0);
       const size_t slot = (size_t)cur.ent.x;
       const int q = cur.ent.y;
       const T* rv = cur.rv;
       const double2 r = cur.r;
       A wi[6];
 #pragma unroll
-      for (int i = 0; i < 6; ++i) wi[i] = (A)winv[6 * (size_t)q + i];
-      const double wg[3] = {ba.winv_ga[3 * (size_t)q], ba.winv_ga[3 * (size_t)q + 1], ba.winv_ga[3 * (size_t)q + 2]};
+      for (int i = 0; i < 6; ++i) wi[i] = (A)cur.wi[i];
+      const double* wg = cur.wg;
       A jp0[3], jp1[3];
 #pragma unroll
       for (int m = 0; m < 3; ++m) { jp0[m] = (A)rv[18 + m]; jp1[m] = (A)rv[21 + m]; }
