@@ -28,7 +28,9 @@ ceres-torch project root):
 * ``schur_solve_dense``         linear.py:667-699 (exact solve of S).
 * ``iterative_schur``           linear.py:702-776 with the PCG of linear.py:1216-1256 and the
   preconditioners of linear.py:462-536 / :1156-1182 (SCHUR_JACOBI = Cholesky of each retained
-  block of S; JACOBI = clamped diagonal; IDENTITY).
+  block of S; JACOBI = clamped diagonal; IDENTITY; SCHUR_POWER_SERIES_EXPANSION = the series
+  of linear.py:59-67 on the SCHUR_JACOBI factors of Hbb, linear.py:482-497) and the SPSE initial
+  point of linear.py:745-756.
 * ``solve``                     solver.py:35-357 (trust-region LM), with :798-802 (model
   decrease), :805-820 (LM radius), :823-861 (step evaluator), :1165-1175 (convergence tests),
   :661-676 (restore best state), :714-785 (parameter order, num_eliminate, visibility).
@@ -374,6 +376,15 @@ def schur_matvec(sys: SchurSystem, x: np.ndarray) -> np.ndarray:
     return y
 
 
+def schur_eliminated_matvec(sys: SchurSystem, x: np.ndarray) -> np.ndarray:
+    """E x = Hba Haa^-1 Hab x (the term S subtracts from Hbb; linear.py:809), x: [nc_a, 9]."""
+    both = (sys.pt >= 0) & (sys.cam >= 0)
+    pt, cam, F = sys.pt[both], sys.cam[both], sys.Fi[both]
+    t = _segment_sum(np.einsum("nij,nj->ni", F, x[cam]), pt, sys.n_pt)
+    s = np.einsum("nij,nj->ni", sys.Winv, t)
+    return _segment_sum(np.einsum("nij,ni->nj", F, s[pt]), cam, sys.n_cam)
+
+
 def schur_dense(sys: SchurSystem) -> np.ndarray:
     """Explicit S [9 nc_a, 9 nc_a] (small problems only)."""
     n = sys.n_cam
@@ -451,11 +462,36 @@ class _Preconditioner:
         return self.dinv * r
 
 
-def pcg(matvec, rhs: np.ndarray, prec: _Preconditioner, *, min_iterations=0, max_iterations=500,
-        tolerance=0.1, eps=EPS64):
-    """linear.py:1216-1256 (x0 = 0)."""
-    x = np.zeros_like(rhs)
-    r = rhs.copy()
+class _PowerSeries:
+    """SCHUR_POWER_SERIES_EXPANSION (linear.py:482-497, applied at :59-67):
+    z = sum_i (B E)^i B r with B the SCHUR_JACOBI factors of the damped Hbb blocks and
+    E = Hba Haa^-1 Hab; term i >= 1 is added while its norm is above
+    tolerance * max(|partial sum|, 1), at most ``max_terms`` terms in all."""
+
+    kind = "SCHUR_POWER_SERIES_EXPANSION"
+
+    def __init__(self, sys: SchurSystem, max_terms: int, tolerance: float):
+        self.base = _Preconditioner("SCHUR_JACOBI", sys.U)
+        self.sys = sys
+        self.max_terms = max_terms
+        self.tolerance = tolerance
+
+    def apply(self, r: np.ndarray) -> np.ndarray:
+        result = self.base.apply(r)
+        term = result
+        for _ in range(max(0, self.max_terms - 1)):
+            term = self.base.apply(schur_eliminated_matvec(self.sys, term))
+            if np.linalg.norm(term) <= self.tolerance * max(float(np.linalg.norm(result)), 1.0):
+                break
+            result = result + term
+        return result
+
+
+def pcg(matvec, rhs: np.ndarray, prec, *, min_iterations=0, max_iterations=500,
+        tolerance=0.1, eps=EPS64, initial_x: np.ndarray | None = None):
+    """linear.py:1216-1256."""
+    x = np.zeros_like(rhs) if initial_x is None else initial_x.copy()
+    r = rhs.copy() if initial_x is None else rhs - matvec(x)
     z = prec.apply(r)
     p = z.copy()
     rz_old = float(np.sum(r * z))
@@ -521,9 +557,15 @@ def solve_step(prob, ev, radius, opts, *, explicit_limit=1800):
             mv = lambda v: (S @ v.reshape(-1)).reshape(-1, 9)  # noqa: E731
         else:
             mv = lambda v: schur_matvec(sys, v)  # noqa: E731
-        prec = _Preconditioner(opts.preconditioner_type, schur_diag_blocks(sys))
+        if opts.preconditioner_type == "SCHUR_POWER_SERIES_EXPANSION":
+            prec = _PowerSeries(sys, opts.max_num_spse_iterations, opts.spse_tolerance)
+        else:
+            prec = _Preconditioner(opts.preconditioner_type, schur_diag_blocks(sys))
+        x0 = None
+        if opts.use_spse_initialization:
+            x0 = _PowerSeries(sys, opts.max_num_spse_iterations, opts.spse_tolerance).apply(sys.rhs)
         xb, its, _ = pcg(mv, sys.rhs, prec, min_iterations=opts.min_linear_solver_iterations,
-                         max_iterations=opts.max_linear_solver_iterations, tolerance=opts.eta)
+                         max_iterations=opts.max_linear_solver_iterations, tolerance=opts.eta, initial_x=x0)
     xa = back_substitute(sys, xb)
     return xa, xb, its
 
@@ -553,6 +595,9 @@ class OracleOptions:
     use_nonmonotonic_steps: bool = False
     max_consecutive_nonmonotonic_steps: int = 5
     explicit_schur_limit: int = 1800  # PCG on an explicit S up to this many camera columns
+    max_num_spse_iterations: int = 5
+    spse_tolerance: float = 0.1
+    use_spse_initialization: bool = False
 
 
 @dataclass

@@ -16,6 +16,9 @@ BA_CASES = [
     "ba_cauchy",
     "ba_const_camera_jacobi",
     "ba_fixed_cameras",
+    "ba_spse",
+    "ba_spse_cauchy",
+    "ba_spse_init",
 ]
 BIG_CASES = ["config0_dense", "config1_small", "config2_small"]
 

@@ -106,21 +106,24 @@ def _evaluate_blocks(tc, problem, data, constant_cameras):
                 eval_gradient=ev.gradient.numpy(), num_eliminate=ne, visibility_flat=vis_flat, visibility_len=vis_len)
 
 
-def make_case(tc, ex, name, data, *, solver, preconditioner="SCHUR_JACOBI", constant_cameras=(), max_iter=50, out=HERE):
+def make_case(tc, ex, name, data, *, solver, preconditioner="SCHUR_JACOBI", constant_cameras=(), max_iter=50, out=HERE,
+              spse=None):
     t0 = time.time()
     problem, cams, pts = _build(tc, ex, data, constant_cameras)
     blocks = _evaluate_blocks(tc, problem, data, constant_cameras)
+    spse = dict(spse or {})
     opts = tc.SolverOptions(
         max_num_iterations=max_iter,
         linear_solver_type=getattr(tc.LinearSolverType, solver),
         preconditioner_type=getattr(tc.PreconditionerType, preconditioner),
+        **spse,
     )
     summary = tc.solve(opts, problem)
     trace = np.array([[it.iteration, it.cost, it.cost_change, it.gradient_max_norm, it.step_norm,
                        it.relative_decrease, it.trust_region_radius, it.linear_solver_iterations,
                        float(it.step_is_successful)] for it in summary.iterations])
     meta = dict(name=name, solver=solver, preconditioner=preconditioner, loss=list(data.loss),
-                constant_cameras=list(constant_cameras), max_num_iterations=max_iter,
+                constant_cameras=list(constant_cameras), max_num_iterations=max_iter, spse=spse,
                 termination=summary.termination_type.value, message=summary.message,
                 initial_cost=summary.initial_cost, final_cost=summary.final_cost,
                 num_iterations=len(summary.iterations), num_successful_steps=summary.num_successful_steps,
@@ -227,6 +230,17 @@ def main():
     if want("ba_fixed_cameras"):
         fx = S.make_small_ba(2, 6, 2, seed=6)
         make_case(tc, ex, "ba_fixed_cameras", fx, solver="DENSE_SCHUR", constant_cameras=(0, 1), max_iter=40)
+    if want("ba_spse"):
+        sp = S.make_small_ba(5, 40, 3, seed=7)
+        make_case(tc, ex, "ba_spse", sp, solver="ITERATIVE_SCHUR", preconditioner="SCHUR_POWER_SERIES_EXPANSION")
+    if want("ba_spse_cauchy"):
+        sc = S.make_small_ba(6, 50, 3, seed=8, loss=("cauchy", 2.0), outlier_fraction=0.05)
+        make_case(tc, ex, "ba_spse_cauchy", sc, solver="ITERATIVE_SCHUR", preconditioner="SCHUR_POWER_SERIES_EXPANSION",
+                  spse=dict(max_num_spse_iterations=8, spse_tolerance=0.01))
+    if want("ba_spse_init"):
+        si = S.make_small_ba(5, 40, 3, seed=9)
+        make_case(tc, ex, "ba_spse_init", si, solver="ITERATIVE_SCHUR",
+                  spse=dict(use_spse_initialization=True, max_num_spse_iterations=3))
     if args.big and want("config0_dense"):
         make_case(tc, ex, "config0_dense", S.ba_config(0), solver="DENSE_SCHUR")
     if args.big and want("config1_small"):

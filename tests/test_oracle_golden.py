@@ -106,7 +106,7 @@ def test_lm_solve_matches_reference(name):
     meta = d["meta"]
     p = _problem(d)
     opts = O.OracleOptions(linear_solver_type=meta["solver"], preconditioner_type=meta["preconditioner"],
-                           max_num_iterations=meta["max_num_iterations"])
+                           max_num_iterations=meta["max_num_iterations"], **meta.get("spse", {}))
     r = O.solve(p, opts)
     trace = d["trace"]
     if name in CHAOTIC_PREFIX:
