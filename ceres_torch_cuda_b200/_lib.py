@@ -32,7 +32,8 @@ DEVERR_BARRIER = 2
 DEVERR_NOT_PD = 4
 
 LOSS_TRIVIAL, LOSS_HUBER, LOSS_SOFTLONE, LOSS_CAUCHY, LOSS_ARCTAN, LOSS_TOLERANT, LOSS_TUKEY = range(7)
-PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_SCHUR_JACOBI = range(3)
+PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_SCHUR_JACOBI, PRECOND_SCHUR_POWER_SERIES = range(4)
+PRECOND_FLAG_SPSE_BASE = 0x100  # camera_assemble: also build the Hbb blocks of the SPSE initial point
 FP64, FP32 = 0, 1
 
 (STAT_COST, STAT_GMAX_P, STAT_GSQ_P, STAT_GMAX_C, STAT_GSQ_C, STAT_CAND_COST, STAT_MODEL, STAT_STEP_SQ_P,
@@ -122,6 +123,8 @@ SIGNATURES = {
     "ceres_b200_ba_point_assemble": (c_int32, [_P, c_double, c_double, c_double, c_int32, c_void_p]),
     "ceres_b200_ba_camera_assemble": (c_int32, [_P, c_double, c_double, c_double, c_int32, c_int32, c_void_p]),
     "ceres_b200_ba_pcg": (c_int32, [_P, c_int32, c_int32, c_int32, c_double, c_int32, c_void_p]),
+    "ceres_b200_ba_pcg_spse": (c_int32, [_P, c_int32, c_int32, c_int32, c_double, c_int32, c_int32, c_double, c_int32,
+                                         c_void_p]),
     "ceres_b200_ba_schur_matvec": (c_int32, [_P, c_void_p, c_void_p, c_void_p]),
     "ceres_b200_ba_step": (c_int32, [_P, c_void_p]),
     "ceres_b200_dense_schur_bytes": (c_int32, [_P, ctypes.POINTER(c_int64)]),

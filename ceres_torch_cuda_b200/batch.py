@@ -22,8 +22,8 @@ from .engine import _PRECOND
 from .losses import device_loss
 from .problem import BundleAdjustmentProblem
 from .solver import _new_summary
-from .types import (IterationSummary, LinearSolverType, MinimizerType, SolverOptions, SolverSummary,
-                    TerminationType, TrustRegionStrategyType)
+from .types import (IterationSummary, LinearSolverType, MinimizerType, PreconditionerType, SolverOptions,
+                    SolverSummary, TerminationType, TrustRegionStrategyType)
 
 _TERMS = {_lib.TERM_CONVERGENCE: TerminationType.CONVERGENCE, _lib.TERM_NO_CONVERGENCE: TerminationType.NO_CONVERGENCE,
           _lib.TERM_FAILURE: TerminationType.FAILURE}
@@ -140,7 +140,8 @@ def _check_options(options: SolverOptions) -> None:
         raise NotImplementedError("batched solves run Levenberg-Marquardt trust-region steps only")
     if options.linear_solver_type is not LinearSolverType.ITERATIVE_SCHUR:
         raise NotImplementedError("batched solves use ITERATIVE_SCHUR")
-    if options.preconditioner_type not in _PRECOND:
+    if options.preconditioner_type not in _PRECOND or \
+            options.preconditioner_type is PreconditionerType.SCHUR_POWER_SERIES_EXPANSION:
         raise NotImplementedError(f"batched solves support IDENTITY, JACOBI and SCHUR_JACOBI, not "
                                   f"{options.preconditioner_type.value}")
     if options.use_nonmonotonic_steps:

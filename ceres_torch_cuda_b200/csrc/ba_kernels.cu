@@ -292,8 +292,9 @@ __device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T*
 }
 
 // Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
-// into acc_out[c][72] (float64).
-template <typename T, bool kDup>
+// into acc_out[c][72] (float64). kHbb: the camera block is the Hbb block sum Jc^T Jc
+// (M = I below) instead of the Schur block; the base of SCHUR_POWER_SERIES_EXPANSION.
+template <typename T, bool kDup, bool kHbb = false>
 __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba, double* __restrict__ acc_out) {
   using A = double;
   __shared__ double sred[kCamAcc * (kCamBlock / 32)];
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
       const A B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
       const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
       const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
-      const A M00 = (A)1 - B00, M01 = -B01, M11 = (A)1 - B11;
+      const A M00 = kHbb ? (A)1 : (A)1 - B00, M01 = kHbb ? (A)0 : -B01, M11 = kHbb ? (A)1 : (A)1 - B11;
       A K0[9], K1[9];
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
 #pragma unroll
         for (int l = j; l < 9; ++l) av[tri9(j, l)] += (A)rv[j] * K0[l] + (A)rv[9 + j] * K1[l];
 
-      if (kDup) {
+      if (kDup && !kHbb) {
         // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
         const int sidx = q >> 5, ln = q & 31;
         const int len = ba.slice_len[sidx];
@@ -421,7 +422,8 @@ constexpr int kFinishWarps = 4;  // cameras per CTA
 template <typename T>
 __global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_ba_t ba, const double* __restrict__ acc_in,
                                                                      double inv_radius, double mn, double mx,
-                                                                     int jacobi_scaling, int precond, double* partials) {
+                                                                     int jacobi_scaling, int precond, double* partials,
+                                                                     T* __restrict__ pre_out) {
   constexpr unsigned kFull = 0xffffffffu;
   __shared__ double sred2[2 * kFinishWarps];
   const int lane = threadIdx.x & 31;
@@ -429,7 +431,7 @@ __global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_
   double gmax = 0.0, gsq = 0.0;
   if (c < ba.num_cameras) {  // uniform in the warp
     const double* sacc = acc_in + (size_t)c * kCamAcc;
-    T* __restrict__ pre = reinterpret_cast<T*>(ba.precond) + 81 * (size_t)c;
+    T* __restrict__ pre = pre_out + 81 * (size_t)c;
     double* dc = ba.cam_diag + 9 * (size_t)c;
     double* rh = ba.rhs + 9 * (size_t)c;
     if (ba.cam_const[c]) {
@@ -543,7 +545,9 @@ __device__ __forceinline__ void camera_product(const T* rv, const TP* __restrict
 }
 
 // The product contribution of one slice s (lane = point), accumulated into y.
-template <typename T, typename TP, typename A, bool kCrossP>
+// kE: only the eliminated term E p = Hba Haa^-1 Hab p, y_c(k) += Jc_k^T Jp_k s (the
+// SCHUR_POWER_SERIES_EXPANSION series multiplies by E).
+template <typename T, typename TP, typename A, bool kCrossP, bool kE = false>
 __device__ __forceinline__ void matvec_one_slice(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int s,
                                                  int lane) {
   constexpr int U = Unroll<T>::v;
@@ -604,10 +608,14 @@ __device__ __forceinline__ void matvec_one_slice(const ceres_b200_ba_t& ba, cons
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (c[u] < 0) continue;
-        A u0, u1;
-        camera_product<T, TP, A, kCrossP>(rv[u], pvec + 9 * (size_t)c[u], u0, u1);
-        const A v0 = u0 - ((A)rv[u][18] * s0 + (A)rv[u][19] * s1 + (A)rv[u][20] * s2);
-        const A v1 = u1 - ((A)rv[u][21] * s0 + (A)rv[u][22] * s1 + (A)rv[u][23] * s2);
+        A v0 = (A)rv[u][18] * s0 + (A)rv[u][19] * s1 + (A)rv[u][20] * s2;
+        A v1 = (A)rv[u][21] * s0 + (A)rv[u][22] * s1 + (A)rv[u][23] * s2;
+        if constexpr (!kE) {
+          A u0, u1;
+          camera_product<T, TP, A, kCrossP>(rv[u], pvec + 9 * (size_t)c[u], u0, u1);
+          v0 = u0 - v0;
+          v1 = u1 - v1;
+        }
         A* yc = y + 9 * (size_t)c[u];
 #pragma unroll
         for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[u][j] * v0 + (A)rv[u][9 + j] * v1);
@@ -619,10 +627,14 @@ __device__ __forceinline__ void matvec_one_slice(const ceres_b200_ba_t& ba, cons
       if (c < 0) continue;
       T rv[kRec];
       load_rec(jac, slot, rv);
-      A u0, u1;
-      camera_product<T, TP, A, kCrossP>(rv, pvec + 9 * (size_t)c, u0, u1);
-      const A v0 = u0 - ((A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2);
-      const A v1 = u1 - ((A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2);
+      A v0 = (A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2;
+      A v1 = (A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2;
+      if constexpr (!kE) {
+        A u0, u1;
+        camera_product<T, TP, A, kCrossP>(rv, pvec + 9 * (size_t)c, u0, u1);
+        v0 = u0 - v0;
+        v1 = u1 - v1;
+      }
       A* yc = y + 9 * (size_t)c;
 #pragma unroll
       for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[j] * v0 + (A)rv[9 + j] * v1);
@@ -631,14 +643,14 @@ __device__ __forceinline__ void matvec_one_slice(const ceres_b200_ba_t& ba, cons
 }
 
 // Static slice walk: warp gw of nw takes the slices of snake_slice(r, gw, nw).
-template <typename T, typename TP, typename A, bool kCrossP = false>
+template <typename T, typename TP, typename A, bool kCrossP = false, bool kE = false>
 __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int gw,
                                               int nw) {
   const int lane = threadIdx.x & 31;
   for (int r = 0; r * nw < ba.num_slices; ++r) {
     const int s = snake_slice(r, gw, nw);
     if (s >= ba.num_slices) continue;
-    matvec_one_slice<T, TP, A, kCrossP>(ba, pvec, y, s, lane);
+    matvec_one_slice<T, TP, A, kCrossP, kE>(ba, pvec, y, s, lane);
   }
 }
 
@@ -648,7 +660,7 @@ __device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const T
 // that order from a shared-memory counter (*counter zero on entry), longest first.
 // A static warp-by-warp assignment left the heaviest CTA with 1.3x the mean work, and
 // every CTA waited for it at the grid barrier.
-template <typename T, typename TP, typename A, bool kCrossP = false>
+template <typename T, typename TP, typename A, bool kCrossP = false, bool kE = false>
 __device__ __forceinline__ void matvec_slices_cta(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y,
                                                   int* counter) {
   const int lane = threadIdx.x & 31;
@@ -659,7 +671,7 @@ __device__ __forceinline__ void matvec_slices_cta(const ceres_b200_ba_t& ba, con
     i = __shfl_sync(0xffffffffu, i, 0);
     const long long s = (long long)i * G + ((i & 1) ? G - 1 - b : b);
     if (s >= ba.num_slices) break;
-    matvec_one_slice<T, TP, A, kCrossP>(ba, pvec, y, (int)s, lane);
+    matvec_one_slice<T, TP, A, kCrossP, kE>(ba, pvec, y, (int)s, lane);
   }
 }
 
@@ -703,6 +715,13 @@ struct PcgArgs {
   const double* norm_ref;  // when set: the tolerance is relative to *norm_ref, not |rhs|
   const double* gate;      // when set and *gate != 0 (the solve before succeeded): do nothing
   int stall_window;        // > 0: stop when |r| has not dropped below 0.99 of its best for this many iterations
+  // SCHUR_POWER_SERIES_EXPANSION (linear.py:59-67, :482-497, :745-756)
+  int precond_series;      // z = sum_i (B E)^i B r with B = ba.precond (inverted damped Hbb blocks)
+  int init_series;         // x0 = the series applied to rhs with B = init_blocks
+  const void* init_blocks; // [nc][81] T
+  int series_terms;        // max_num_spse_iterations (>= 1)
+  double series_tol;       // spse_tolerance
+  double* part_s;          // [G][2] partials of the series norms and of |r|^2
 };
 
 constexpr int kPcgBlock = 512;
@@ -783,15 +802,93 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     }
     return;
   }
-  // ---- init: x = 0, r = rhs, z = M^-1 r, p = z (written at the first phase A)
-  {
-    double rz = 0.0, rr = 0.0;
-    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-      X[j] = 0.0;
-      R[j] = a.rhs[j];
+  // ---- products over the whole grid. Every CTA calls them; V is complete on all CTAs
+  // (a grid barrier precedes the call). out[j0..j1) = (S V) (kS) or (E V) of this
+  // CTA's cameras; ends after the fold, with the partials read.
+  auto product = [&](const double* V, double* out, bool kS) -> bool {
+    if (a.smem_vectors) {
+      for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        ps[j] = (T)ld_cross(V + j);
+        ys[j] = (T)0;
+      }
+      if (threadIdx.x == 0) slice_counter = 0;
+      __syncthreads();
+      if (kS) matvec_slices_cta<T, T, T, false, false>(ba, ps, ys, &slice_counter);
+      else matvec_slices_cta<T, T, T, false, true>(ba, ps, ys, &slice_counter);
+      __syncthreads();
+      T* my = part_y + (size_t)blockIdx.x * n;
+      for (int j = threadIdx.x; j < n; j += blockDim.x) my[j] = ys[j];
+      if (!grid_sync(gb)) return false;
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        double y = 0.0;
+#pragma unroll 4
+        for (int g = 0; g < G; ++g) y += (double)ld_cross(part_y + (size_t)g * n + j);
+        if (kS) y += ba.cam_diag[j] * ld_cross(V + j);
+        out[j] = y;
+      }
+    } else {
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) out[j] = 0.0;
+      if (!grid_sync(gb)) return false;
+      if (kS) matvec_slices<T, double, double, true, false>(ba, V, out, gw, nw);
+      else matvec_slices<T, double, double, true, true>(ba, V, out, gw, nw);
+      if (!grid_sync(gb)) return false;
+      if (kS)
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) out[j] = ld_cross(out + j) + ba.cam_diag[j] * ld_cross(V + j);
     }
     __syncthreads();
-    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+    return true;
+  };
+  // ---- the power series (linear.py:59-67): out = sum_i (B E)^i B in over this CTA's
+  // cameras; term and w are scratch vectors (term is read by every CTA).
+  auto series = [&](const T* B, const double* in, double* out, double* term, double* w) -> bool {
+    __syncthreads();
+    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(B, in, out, c);
+    __syncthreads();
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) term[j] = out[j];
+    for (int it = 1; it < a.series_terms; ++it) {
+      if (!grid_sync(gb)) return false;
+      if (!product(term, w, false)) return false;
+      for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(B, w, term, c);
+      __syncthreads();
+      double v[2] = {0.0, 0.0};
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const double t = term[j], o = out[j];
+        v[0] += t * t;
+        v[1] += o * o;
+      }
+      block_reduce<2>(v, 0u, red);
+      if (threadIdx.x == 0) { a.part_s[2 * blockIdx.x] = v[0]; a.part_s[2 * blockIdx.x + 1] = v[1]; }
+      if (!grid_sync(gb)) return false;
+      double t2[2];
+      cta_sum_partials<2>(a.part_s, G, 2, t2, red, bcast);
+      if (sqrt(t2[0]) <= a.series_tol * fmax(sqrt(t2[1]), 1.0)) break;  // same decision on every CTA
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) out[j] += term[j];
+    }
+    __syncthreads();
+    return true;
+  };
+
+  // ---- init: x = x0 (0, or the series applied to rhs), r = rhs - S x0, z = M^-1 r,
+  // p = z (written at the first phase A)
+  {
+    double rz = 0.0, rr = 0.0;
+    if (a.init_series) {
+      if (!series(reinterpret_cast<const T*>(a.init_blocks), a.rhs, X, Pbuf + n, AP)) return;
+      if (!grid_sync(gb)) return;
+      if (!product(X, Z, true)) return;
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) R[j] = a.rhs[j] - Z[j];
+    } else {
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        X[j] = 0.0;
+        R[j] = a.rhs[j];
+      }
+    }
+    __syncthreads();
+    if (a.precond_series) {
+      if (!series(Minv, R, Z, Pbuf + n, AP)) return;
+    } else {
+      for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+    }
     __syncthreads();
     for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
       const double r = (double)R[j], z = (double)Z[j];
@@ -913,6 +1010,46 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
         break;
       }
       const double alpha = rz_old / denom;
+      if (a.precond_series) {
+        // the reference's order: x, r; test |r|; only then z = M^-1 r (a series costs
+        // up to series_terms - 1 products)
+        double v[1] = {0.0};
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+          X[j] = X[j] + alpha * Pnew[j];
+          const double rj = R[j] - alpha * AP[j];
+          R[j] = rj;
+          v[0] += rj * rj;
+        }
+        block_reduce<1>(v, 0u, red);
+        if (threadIdx.x == 0) a.part_s[2 * blockIdx.x] = v[0];
+        if (!grid_sync(gb)) return;
+        double t[2];
+        cta_sum_partials<1>(a.part_s, G, 2, t, red, bcast);
+        rr = t[0];
+        rnorm = sqrt(rr);
+        iterations = k + 1;
+        if (iterations >= a.min_iterations && rnorm <= a.tolerance * rhs_norm) {
+          success = true;
+          break;
+        }
+        if (!series(Minv, R, Z, Pbuf + (size_t)(cur ^ 1) * n, AP)) return;
+        double v2[1] = {0.0};
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) v2[0] += R[j] * Z[j];
+        block_reduce<1>(v2, 0u, red);
+        if (threadIdx.x == 0) a.part_c[2 * blockIdx.x] = v2[0];
+        if (!grid_sync(gb)) return;
+        double t2[1];
+        cta_sum_partials<1>(a.part_c, G, 2, t2, red, bcast);
+        const double rz_new = t2[0];
+        if (fabs(rz_old) <= a.eps) break;
+        if (a.stall_window > 0) {
+          if (rnorm < 0.99 * rbest) { rbest = rnorm; last_improvement = iterations; }
+          else if (iterations - last_improvement >= a.stall_window) break;
+        }
+        beta = rz_new / rz_old;
+        rz_old = rz_new;
+        continue;
+      }
       // ---- phase C: x += alpha p ; r -= alpha Ap ; z = M^-1 r ; partial r.z, r.r
       {
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
@@ -1346,7 +1483,8 @@ struct PcgLayout {
   int cams_per_cta = 0;
   int smem_vectors = 0;
   size_t dyn_smem = 0;
-  size_t frames = 0, aux = 0, cam_acc = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0, total = 0;
+  size_t frames = 0, aux = 0, cam_acc = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0,
+         spse_base = 0, part_s = 0, total = 0;
 };
 
 template <typename T>
@@ -1382,6 +1520,8 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   off += (size_t)L.grid * sizeof(double);
   L.part_c = off;
   off += (size_t)L.grid * 2 * sizeof(double);
+  L.part_s = off;
+  off += (size_t)L.grid * 2 * sizeof(double);
   L.result = off;
   off += 8 * sizeof(double);
   off = (off + 255) & ~(size_t)255;
@@ -1389,6 +1529,9 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   off += (size_t)n * sizeof(double);
   L.r64 = off;
   off += (size_t)n * sizeof(double);
+  off = (off + 255) & ~(size_t)255;
+  L.spse_base = off;
+  off += (size_t)(ba.num_cameras > 0 ? ba.num_cameras : 1) * 81 * sizeof(T);
   L.total = (off + 255) & ~(size_t)255;
   return CERES_B200_OK;
 }
@@ -1401,11 +1544,24 @@ int scratch_bytes_impl(const ceres_b200_ba_t& ba, size_t& bytes) {
   return CERES_B200_OK;
 }
 
+// Series options of one PCG launch (SCHUR_POWER_SERIES_EXPANSION / SPSE initial point).
+struct SeriesOpts {
+  int precond = 0, init = 0, terms = 1;
+  double tol = 0.0;
+  const void* init_blocks = nullptr;
+};
+
 template <typename T>
 int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int accumulate, int min_it, int max_it,
                double tol, cudaStream_t st, const PcgLayout& L, char* scratch, double* result, const double* norm_ref,
-               const double* gate, int stall_window) {
+               const double* gate, int stall_window, const SeriesOpts& so = SeriesOpts()) {
   PcgArgs a;
+  a.precond_series = so.precond;
+  a.init_series = so.init;
+  a.init_blocks = so.init_blocks;
+  a.series_terms = so.terms;
+  a.series_tol = so.tol;
+  a.part_s = reinterpret_cast<double*>(scratch + L.part_s);
   a.rhs = rhs;
   a.x_out = x_out;
   a.accumulate = accumulate;
@@ -1460,8 +1616,38 @@ int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, const double
   return check_launch();
 }
 
+// Camera side of the assembly. pc: the preconditioner whose blocks go to ba.precond
+// (SCHUR_POWER_SERIES: the inverted damped Hbb blocks); FLAG_SPSE_BASE: the Hbb
+// blocks for the SPSE initial point as well, into the scratch. Each block set is one
+// reduction over the camera-major lists; the damping, rhs and gradient stats come
+// out of every reduction alike.
 template <typename T>
-int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, double tol, int max_ref, cudaStream_t st) {
+void camera_assemble_impl(const ceres_b200_ba_t& ba, const PcgLayout& L, char* scratch, double inv_radius,
+                          double mn, double mx, int jacobi_scaling, int pc, int flags, cudaStream_t st) {
+  double* partials = reinterpret_cast<double*>(scratch);
+  double* acc = reinterpret_cast<double*>(scratch + L.cam_acc);
+  const int nc = ba.num_cameras;
+  const int fgrid = (nc + kFinishWarps - 1) / kFinishWarps;
+  T* pre = reinterpret_cast<T*>(ba.precond);
+  const bool spse = pc == CERES_B200_PRECOND_SCHUR_POWER_SERIES;
+  count_launch(2);
+  if (spse) k_camera_reduce<T, false, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
+  else if (ba.has_duplicate_cameras) k_camera_reduce<T, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
+  else k_camera_reduce<T, false><<<nc, kCamBlock, 0, st>>>(ba, acc);
+  k_camera_finish<T><<<fgrid, 32 * kFinishWarps, 0, st>>>(ba, acc, inv_radius, mn, mx, jacobi_scaling,
+                                                         spse ? CERES_B200_PRECOND_SCHUR_JACOBI : pc, partials, pre);
+  if ((flags & CERES_B200_PRECOND_FLAG_SPSE_BASE) && !spse) {
+    count_launch(2);
+    k_camera_reduce<T, false, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
+    k_camera_finish<T><<<fgrid, 32 * kFinishWarps, 0, st>>>(ba, acc, inv_radius, mn, mx, jacobi_scaling,
+                                                           CERES_B200_PRECOND_SCHUR_JACOBI, partials,
+                                                           reinterpret_cast<T*>(scratch + L.spse_base));
+  }
+}
+
+template <typename T>
+int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, double tol, int max_ref, cudaStream_t st,
+             int series_terms = 1, double series_tol = 0.0, int series_init = 0) {
   PcgLayout L;
   CB_TRACE("pcg: layout");
   int rc = pcg_layout<T>(ba, L);
@@ -1471,12 +1657,19 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
   char* scratch = reinterpret_cast<char*>(ba.scratch);
   const int n = 9 * ba.num_cameras;
   if (n == 0) return CERES_B200_OK;
-  (void)precond;
   double* result = reinterpret_cast<double*>(scratch + L.result);
   const bool refine = max_ref > 0 && sizeof(T) == sizeof(float);
   const int stall = refine ? kStallWindow : 0;
+  SeriesOpts so;
+  so.precond = precond == CERES_B200_PRECOND_SCHUR_POWER_SERIES ? 1 : 0;
+  so.terms = series_terms;
+  so.tol = series_tol;
+  so.init = series_init ? 1 : 0;
+  so.init_blocks = so.precond ? ba.precond : static_cast<const void*>(scratch + L.spse_base);
+  SeriesOpts so_ref = so;  // refinement passes solve for a correction from zero
+  so_ref.init = 0;
   rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, min_it, max_it, tol, st, L, scratch, result, nullptr, nullptr,
-                     stall);
+                     stall, so);
   if (rc) return rc;
   count_launch();
   k_copy_result<<<1, 1, 0, st>>>(ba, result, -1.0);
@@ -1495,7 +1688,7 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
       rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st, gate);
       if (rc) return rc;
       rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, 0, max_it, tol, st, L, scratch, rref, result + 3, gate,
-                         stall);
+                         stall, so_ref);
       if (rc) return rc;
       count_launch();
       k_add_refinement<<<1, 1, 0, st>>>(ba, rref);
@@ -1654,8 +1847,10 @@ int ceres_b200_ba_point_assemble(const ceres_b200_ba_t* ba, double radius, doubl
 int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, double min_diagonal, double max_diagonal,
                                   int jacobi_scaling, int preconditioner, void* stream) {
   if (!valid(ba) || !ba->scratch) return CERES_B200_EINVAL;
-  if (preconditioner < CERES_B200_PRECOND_IDENTITY || preconditioner > CERES_B200_PRECOND_SCHUR_JACOBI)
-    return CERES_B200_EINVAL;
+  const int flags = preconditioner & ~0xff;
+  const int pc = preconditioner & 0xff;
+  if (pc < CERES_B200_PRECOND_IDENTITY || pc > CERES_B200_PRECOND_SCHUR_POWER_SERIES) return CERES_B200_EINVAL;
+  if ((flags & ~CERES_B200_PRECOND_FLAG_SPSE_BASE) != 0) return CERES_B200_EINVAL;
   if (ba->num_cameras == 0) return CERES_B200_OK;
   PcgLayout L;
   const int lrc = ba->precision == CERES_B200_FP32 ? pcg_layout<float>(*ba, L) : pcg_layout<double>(*ba, L);
@@ -1663,21 +1858,11 @@ int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, doub
   if ((size_t)ba->scratch_bytes < L.total) return CERES_B200_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   const double inv_radius = 1.0 / fmax(radius, kEps64);
-  double* partials = reinterpret_cast<double*>(ba->scratch);
-  double* acc = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + L.cam_acc);
-  const int nc = ba->num_cameras;
-  count_launch(2);
-  if (ba->precision == CERES_B200_FP32) {
-    if (ba->has_duplicate_cameras) k_camera_reduce<float, true><<<nc, kCamBlock, 0, st>>>(*ba, acc);
-    else k_camera_reduce<float, false><<<nc, kCamBlock, 0, st>>>(*ba, acc);
-    k_camera_finish<float><<<(nc + kFinishWarps - 1) / kFinishWarps, 32 * kFinishWarps, 0, st>>>(
-        *ba, acc, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, preconditioner, partials);
-  } else {
-    if (ba->has_duplicate_cameras) k_camera_reduce<double, true><<<nc, kCamBlock, 0, st>>>(*ba, acc);
-    else k_camera_reduce<double, false><<<nc, kCamBlock, 0, st>>>(*ba, acc);
-    k_camera_finish<double><<<(nc + kFinishWarps - 1) / kFinishWarps, 32 * kFinishWarps, 0, st>>>(
-        *ba, acc, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, preconditioner, partials);
-  }
+  char* scratch = reinterpret_cast<char*>(ba->scratch);
+  if (ba->precision == CERES_B200_FP32)
+    camera_assemble_impl<float>(*ba, L, scratch, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, pc, flags, st);
+  else
+    camera_assemble_impl<double>(*ba, L, scratch, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, pc, flags, st);
   return check_launch();
 }
 
@@ -1689,6 +1874,24 @@ int ceres_b200_ba_pcg(const ceres_b200_ba_t* ba, int preconditioner, int min_ite
   if (ba->precision == CERES_B200_FP32)
     return pcg_impl<float>(*ba, preconditioner, min_iterations, max_iterations, tolerance, max_refinements, st);
   return pcg_impl<double>(*ba, preconditioner, min_iterations, max_iterations, tolerance, max_refinements, st);
+}
+
+int ceres_b200_ba_pcg_spse(const ceres_b200_ba_t* ba, int preconditioner, int min_iterations, int max_iterations,
+                           double tolerance, int max_refinements, int spse_terms, double spse_tolerance, int spse_init,
+                           void* stream) {
+  if (!valid(ba) || max_iterations < 0 || min_iterations < 0 || max_refinements < 0) return CERES_B200_EINVAL;
+  if (!ba->pcg_x || !ba->pcg_r || !ba->pcg_z || !ba->pcg_p || !ba->pcg_ap || !ba->step_cameras) return CERES_B200_EINVAL;
+  if (preconditioner < CERES_B200_PRECOND_IDENTITY || preconditioner > CERES_B200_PRECOND_SCHUR_POWER_SERIES)
+    return CERES_B200_EINVAL;
+  const bool uses = preconditioner == CERES_B200_PRECOND_SCHUR_POWER_SERIES || spse_init != 0;
+  if (uses && (spse_terms < 1 || !(spse_tolerance >= 0.0))) return CERES_B200_EINVAL;
+  if (!uses) spse_terms = 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ba->precision == CERES_B200_FP32)
+    return pcg_impl<float>(*ba, preconditioner, min_iterations, max_iterations, tolerance, max_refinements, st,
+                           spse_terms, spse_tolerance, spse_init);
+  return pcg_impl<double>(*ba, preconditioner, min_iterations, max_iterations, tolerance, max_refinements, st,
+                          spse_terms, spse_tolerance, spse_init);
 }
 
 int ceres_b200_ba_schur_matvec(const ceres_b200_ba_t* ba, const double* x, double* y, void* stream) {

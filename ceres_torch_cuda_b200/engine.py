@@ -26,6 +26,7 @@ _PRECOND = {
     PreconditionerType.IDENTITY: _lib.PRECOND_IDENTITY,
     PreconditionerType.JACOBI: _lib.PRECOND_JACOBI,
     PreconditionerType.SCHUR_JACOBI: _lib.PRECOND_SCHUR_JACOBI,
+    PreconditionerType.SCHUR_POWER_SERIES_EXPANSION: _lib.PRECOND_SCHUR_POWER_SERIES,
 }
 
 PRECISIONS = ("fp64", "mixed")
@@ -282,16 +283,26 @@ class BAEngine:
     def evaluate(self, with_jacobian: bool = True) -> None:
         self._call("ceres_b200_ba_evaluate", int(with_jacobian))
 
-    def assemble(self, radius: float, options: SolverOptions, precond: int) -> None:
+    def assemble(self, radius: float, options: SolverOptions, precond: int, spse_base: bool = False) -> None:
+        flags = _lib.PRECOND_FLAG_SPSE_BASE if spse_base else 0
         self._call("ceres_b200_ba_point_assemble", float(radius), float(options.min_lm_diagonal),
                    float(options.max_lm_diagonal), int(options.jacobi_scaling))
         self._call("ceres_b200_ba_camera_assemble", float(radius), float(options.min_lm_diagonal),
-                   float(options.max_lm_diagonal), int(options.jacobi_scaling), int(precond))
+                   float(options.max_lm_diagonal), int(options.jacobi_scaling), int(precond) | flags)
 
     def pcg(self, precond: int, min_iterations: int, max_iterations: int, tolerance: float,
-            max_refinements: int = 0) -> None:
-        self._call("ceres_b200_ba_pcg", int(precond), int(min_iterations), int(max_iterations), float(tolerance),
-                   int(max_refinements))
+            max_refinements: int = 0, spse_terms: int = 0, spse_tolerance: float = 0.0,
+            spse_init: bool = False) -> None:
+        """PCG on the reduced camera system. With the SCHUR_POWER_SERIES preconditioner
+        or ``spse_init`` the series options apply (``spse_terms`` = max_num_spse_iterations);
+        ``spse_init`` needs the SPSE base blocks from ``assemble(..., spse_base=True)``
+        unless the preconditioner is the power series itself."""
+        if precond == _lib.PRECOND_SCHUR_POWER_SERIES or spse_init:
+            self._call("ceres_b200_ba_pcg_spse", int(precond), int(min_iterations), int(max_iterations),
+                       float(tolerance), int(max_refinements), int(spse_terms), float(spse_tolerance), int(bool(spse_init)))
+        else:
+            self._call("ceres_b200_ba_pcg", int(precond), int(min_iterations), int(max_iterations), float(tolerance),
+                       int(max_refinements))
 
     def dense_solve(self) -> None:
         if self.nc == 0:
@@ -414,9 +425,7 @@ def linear_solver_kind(options: SolverOptions) -> str:
         if options.preconditioner_type not in _PRECOND:
             raise NotImplementedError(
                 f"ITERATIVE_SCHUR with {options.preconditioner_type.value} is not implemented on the GPU path "
-                "(IDENTITY, JACOBI and SCHUR_JACOBI are)")
-        if options.use_spse_initialization:
-            raise NotImplementedError("use_spse_initialization is not implemented on the GPU path")
+                "(IDENTITY, JACOBI, SCHUR_JACOBI and SCHUR_POWER_SERIES_EXPANSION are)")
         return "iterative"
     raise NotImplementedError(f"{lst.value} is not a Schur solver; the GPU path implements DENSE_SCHUR, "
                               "SPARSE_SCHUR and ITERATIVE_SCHUR")
@@ -435,6 +444,8 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
     """
     kind = linear_solver_kind(options)
     precond = _PRECOND.get(options.preconditioner_type, _lib.PRECOND_SCHUR_JACOBI)
+    spse_init = kind == "iterative" and bool(options.use_spse_initialization)
+    spse_base = spse_init and precond != _lib.PRECOND_SCHUR_POWER_SERIES
     refinements = max_refinements if engine.precision == "mixed" else 0
     lm = _LMRadius(options.initial_trust_region_radius, options.max_trust_region_radius)
     radius = lm.radius
@@ -445,7 +456,7 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
 
     t0 = time.perf_counter()
     engine.evaluate(True)
-    engine.assemble(radius, options, precond)
+    engine.assemble(radius, options, precond, spse_base)
     st = engine.read_stats()
     eval_time = time.perf_counter() - t0
     summary.jacobian_evaluation_time_in_seconds += eval_time
@@ -484,7 +495,7 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
         jac_time = 0.0
         if need_assemble:
             t0 = time.perf_counter()
-            engine.assemble(radius, options, precond)
+            engine.assemble(radius, options, precond, spse_base)
             need_assemble = False
             jac_time = time.perf_counter() - t0
         summary.num_jacobian_evaluations += 1
@@ -516,7 +527,7 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
             lin_iters = 1
         else:
             engine.pcg(precond, options.min_linear_solver_iterations, options.max_linear_solver_iterations,
-                       options.eta, refinements)
+                       options.eta, refinements, options.max_num_spse_iterations, options.spse_tolerance, spse_init)
         engine.step()
         st = engine.read_stats()
         lin_time = time.perf_counter() - lin_start
@@ -636,7 +647,7 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
             previous_cost = candidate_cost
             t0 = time.perf_counter()
             engine.evaluate(True)
-            engine.assemble(radius, options, precond)
+            engine.assemble(radius, options, precond, spse_base)
             st = engine.read_stats()
             jt = time.perf_counter() - t0
             summary.jacobian_evaluation_time_in_seconds += jt

@@ -49,8 +49,14 @@ enum {
 enum {
   CERES_B200_PRECOND_IDENTITY = 0,
   CERES_B200_PRECOND_JACOBI = 1,
-  CERES_B200_PRECOND_SCHUR_JACOBI = 2
+  CERES_B200_PRECOND_SCHUR_JACOBI = 2,
+  /* SCHUR_POWER_SERIES_EXPANSION (linear.py:482-497): blocks of the damped Hbb,
+   * series in ceres_b200_ba_pcg_spse; single-problem path only */
+  CERES_B200_PRECOND_SCHUR_POWER_SERIES = 3
 };
+/* or-ed into camera_assemble's preconditioner: also build the Hbb blocks of the
+ * SPSE initial point (use_spse_initialization, linear.py:745-756) in the scratch */
+#define CERES_B200_PRECOND_FLAG_SPSE_BASE 0x100
 
 /* precision of the Jacobian store, point-block inverses and PCG vectors */
 enum { CERES_B200_FP64 = 0, CERES_B200_FP32 = 1 };
@@ -225,6 +231,21 @@ int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, doub
  */
 int ceres_b200_ba_pcg(const ceres_b200_ba_t* ba, int preconditioner, int min_iterations,
                       int max_iterations, double tolerance, int max_refinements, void* stream);
+
+/*
+ * ceres_b200_ba_pcg with the power series of SCHUR_POWER_SERIES_EXPANSION
+ * (preconditioner CERES_B200_PRECOND_SCHUR_POWER_SERIES; linear.py:59-67):
+ * z = sum_i (B E)^i B r, B the inverted damped Hbb blocks, E = H_ba W^-1 H_ab,
+ * term i >= 1 added while |term| > spse_tolerance * max(|sum so far|, 1), at
+ * most spse_terms terms (max_num_spse_iterations). spse_init != 0: the start
+ * point is x0 = that series applied to rhs with the Hbb blocks of
+ * camera_assemble's CERES_B200_PRECOND_FLAG_SPSE_BASE (or of the preconditioner
+ * itself when it is the power series), and r0 = rhs - S x0 (linear.py:745-756,
+ * :1226-1227). spse_terms >= 1 and spse_tolerance >= 0 when either is used.
+ */
+int ceres_b200_ba_pcg_spse(const ceres_b200_ba_t* ba, int preconditioner, int min_iterations,
+                           int max_iterations, double tolerance, int max_refinements, int spse_terms,
+                           double spse_tolerance, int spse_init, void* stream);
 
 /*
  * y = S x for a camera vector x (float64 in and out, accumulated in float64

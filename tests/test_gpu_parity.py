@@ -133,6 +133,63 @@ def test_pcg_matches_oracle(name):
             np.testing.assert_allclose(xg, xb, rtol=1e-7, atol=1e-9 * np.abs(xb).max())
 
 
+@pytest.mark.parametrize("name", ["ba_spse", "ba_spse_cauchy", "config1_small"])
+@pytest.mark.parametrize("terms,stol,init", [(5, 0.1, False), (8, 0.01, False), (1, 0.1, False), (3, 0.1, True),
+                                             (4, 0.0, True)])
+def test_power_series_pcg_matches_oracle(name, terms, stol, init):
+    """SCHUR_POWER_SERIES_EXPANSION (linear.py:59-67, :482-497) and the SPSE initial
+    point (linear.py:745-756) through ceres_b200_ba_pcg_spse against the oracle: the
+    same iteration counts and iterates (1e-7) at eta and at a fixed iteration count.
+    ``init`` runs SCHUR_JACOBI from the SPSE start point."""
+    tc = _tc()
+    from ceres_torch_cuda_b200 import _lib
+    d = G.load(name)
+    eng = _engine(d)
+    p = _oracle_problem(d)
+    pre_name = "SCHUR_JACOBI" if init else "SCHUR_POWER_SERIES_EXPANSION"
+    pre = getattr(tc.PreconditionerType, pre_name)
+    code = _lib.PRECOND_SCHUR_JACOBI if init else _lib.PRECOND_SCHUR_POWER_SERIES
+    opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR, preconditioner_type=pre)
+    radius = 1e3
+    eng.evaluate(True)
+    eng.assemble(radius, opts, code, spse_base=init)
+    ev = O.evaluate(p, p.cameras, p.points)
+    for tol, its in ((0.1, 500), (0.0, 5)):
+        eng.pcg(code, 0, its, tol, 0, terms, stol, init)
+        st = eng.read_stats()
+        opts_o = O.OracleOptions(eta=tol, max_linear_solver_iterations=its, preconditioner_type=pre_name,
+                                 max_num_spse_iterations=terms, spse_tolerance=stol, use_spse_initialization=init)
+        xa, xb, n_it = O.solve_step(p, ev, radius, opts_o, explicit_limit=0)
+        xg = eng.step_cameras[: eng.nc].cpu().numpy()
+        assert int(st[10]) == n_it, (tol, int(st[10]), n_it)
+        np.testing.assert_allclose(xg, xb, rtol=1e-7, atol=1e-9 * np.abs(xb).max())
+
+
+def test_power_series_base_blocks_are_hbb_inverses():
+    """The SPSE base: inverses of the damped Hbb camera blocks (linear.py:484-489)."""
+    tc = _tc()
+    from ceres_torch_cuda_b200 import _lib
+    d = G.load("ba_spse")
+    eng = _engine(d)
+    p = _oracle_problem(d)
+    opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                            preconditioner_type=tc.PreconditionerType.SCHUR_POWER_SERIES_EXPANSION)
+    radius = 77.0
+    eng.evaluate(True)
+    eng.assemble(radius, opts, _lib.PRECOND_SCHUR_POWER_SERIES)
+    ev = O.evaluate(p, p.cameras, p.points)
+    pt = p.pt_col[p.point_index]
+    cam = p.cam_col[p.camera_index]
+    col_p = O._segment_sum(np.sum(ev.Jp ** 2, axis=1), pt, p.active_pts.size)
+    col_c = O._segment_sum(np.sum(ev.Jc ** 2, axis=1), cam, p.active_cams.size)
+    sys = O.build_schur(p, ev, O.jacobi_damping(col_p, radius, 1e-6, 1e32), O.jacobi_damping(col_c, radius, 1e-6, 1e32))
+    Minv = eng.precond[: eng.nc].cpu().numpy().reshape(-1, 9, 9)
+    ref = np.linalg.inv(sys.U)
+    np.testing.assert_allclose(Minv, ref, rtol=1e-8, atol=1e-10 * np.abs(ref).max())
+    rhs = eng.rhs[: eng.nc].cpu().numpy()
+    np.testing.assert_allclose(rhs, sys.rhs, rtol=1e-9, atol=1e-9 * np.abs(sys.rhs).max())
+
+
 @pytest.mark.parametrize("name", G.BA_CASES + G.BIG_CASES)
 def test_lm_solve_matches_reference(name):
     tc = _tc()
@@ -146,7 +203,8 @@ def test_lm_solve_matches_reference(name):
                                       camera_constant=t(G.constant_mask(nc, meta["constant_cameras"]), torch.bool))
     opts = tc.SolverOptions(max_num_iterations=meta["max_num_iterations"],
                             linear_solver_type=getattr(tc.LinearSolverType, meta["solver"]),
-                            preconditioner_type=getattr(tc.PreconditionerType, meta["preconditioner"]))
+                            preconditioner_type=getattr(tc.PreconditionerType, meta["preconditioner"]),
+                            **meta.get("spse", {}))
     s = tc.solve(opts, prob, precision="fp64")
     if name == "ba_const_camera_jacobi":  # chaotic trajectory (see test_oracle_golden)
         np.testing.assert_allclose(s.final_cost, meta["final_cost"], rtol=1e-3)
@@ -163,8 +221,10 @@ def test_lm_solve_matches_reference(name):
 
 # ba_huber_outliers is left out: with 10% outliers two correct trajectories can settle in
 # different local minima (1% apart), which says nothing about precision.
-@pytest.mark.parametrize("name", ["ba_small_iterative", "ba_cauchy", "config1_small", "config2_small"])
-def test_mixed_precision_reaches_fp64_cost(name):
+@pytest.mark.parametrize("name,precond", [("ba_small_iterative", None), ("ba_cauchy", None), ("config1_small", None),
+                                          ("config2_small", None),
+                                          ("ba_small_iterative", "SCHUR_POWER_SERIES_EXPANSION")])
+def test_mixed_precision_reaches_fp64_cost(name, precond):
     """FP32 Jacobian/PCG with float64 cost, gain ratio and refinement reaches the
     float64 minimum within 1e-6 relative. Both paths run to a tight function
     tolerance so that each stops at the minimum, not at the first small decrease."""
@@ -179,7 +239,7 @@ def test_mixed_precision_reaches_fp64_cost(name):
                                           loss=_loss_obj(G.loss_spec(meta["loss"])))
         opts = tc.SolverOptions(max_num_iterations=200, function_tolerance=1e-12, parameter_tolerance=1e-14,
                                 linear_solver_type=getattr(tc.LinearSolverType, meta["solver"]),
-                                preconditioner_type=getattr(tc.PreconditionerType, meta["preconditioner"]))
+                                preconditioner_type=getattr(tc.PreconditionerType, precond or meta["preconditioner"]))
         return tc.solve(opts, prob, precision=precision)
 
     s64 = run("fp64")
