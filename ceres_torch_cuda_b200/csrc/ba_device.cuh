@@ -620,6 +620,17 @@ __device__ __forceinline__ int next_cta_slice(int* counter, int num_slices) {
   return s < num_slices ? (int)s : -1;
 }
 
+// Longest-first dynamic schedule over the whole grid: slices are sorted by length
+// (descending), so warps taking them in index order from one global counter follow the
+// LPT rule, and no CTA slot idles behind the slowest warp of its CTA. The counter is
+// reset by the fold that follows (k_slice_fold). Returns -1 when no slice is left.
+__device__ __forceinline__ int next_global_slice(unsigned* counter, int num_slices) {
+  int i = 0;
+  if ((threadIdx.x & 31) == 0) i = (int)atomicAdd(counter, 1u);
+  i = __shfl_sync(0xffffffffu, i, 0);
+  return i < num_slices ? i : -1;
+}
+
 __device__ __forceinline__ int snake_slice(int r, int gw, int nw) {
   return r * nw + ((r & 1) ? nw - 1 - gw : gw);
 }

@@ -43,6 +43,9 @@ inline void count_launch(int n = 1) { __atomic_fetch_add(&g_launches, (unsigned 
 
 // counters[] slots
 constexpr int kCtrEval = 0, kCtrPoint = 1, kCtrCamera = 2, kCtrStep = 3, kCtrCamStep = 4;
+constexpr int kCtrSliceEval = 5, kCtrSliceStep = 6;  // dynamic slice counters (zero between launches)
+
+template <int NV> struct StatIdx { int idx[NV]; };  // stats entries a kernel argument names
 constexpr int kCtrBarCount = 8, kCtrBarGen = 9, kCtrBarFlag = 10, kCtrError = 12;
 
 constexpr int kWarpBlock = 256;  // threads per CTA of the slice-walking kernels
@@ -104,6 +107,20 @@ inline size_t frames_bytes(const ceres_b200_ba_t& ba) {
   return ((size_t)(ba.num_cameras > 0 ? ba.num_cameras : 1) * kFrame * sizeof(double) + 255) & ~(size_t)255;
 }
 
+// Per-slice partial sums of the evaluation and step kernels (5 float64 per slice)
+// follow the frames.
+inline size_t slice_part_bytes(const ceres_b200_ba_t& ba) {
+  return ((size_t)(ba.num_slices > 0 ? ba.num_slices : 1) * 5 * sizeof(double) + 255) & ~(size_t)255;
+}
+
+// Grid of the dynamically scheduled slice kernels: the CTAs resident at once (the
+// kernels' register caps fix that count), at most slice_grid.
+inline int resident_slice_grid(const ceres_b200_ba_t& ba, const DevInfo& d, int ctas_per_sm) {
+  const int g = d.sms * ctas_per_sm;
+  const int sg = slice_grid(ba, d);
+  return g < sg ? g : sg;
+}
+
 }  // namespace
 
 // ======================================================================================
@@ -123,10 +140,14 @@ __global__ void k_camera_frames(const double* __restrict__ cams, double* __restr
 }
 
 // kFrames: the cameras' rotation parts come from frames[nc][kFrame] (k_camera_frames
-// of ba.cameras); otherwise every observation computes its camera's rotation.
+// of ba.cameras), and the slices follow the dynamic longest-first schedule with per-slice
+// cost partials in slice_part (scratch); otherwise (the allocation-free entry, no
+// scratch) every observation computes its camera's rotation and the CTAs take fixed
+// slice sets (next_cta_slice) with per-CTA partials.
 template <typename T, bool kJac, bool kFrames>
 __global__ void __launch_bounds__(kWarpBlock, kJac ? CERES_B200_EVAL_MIN_BLOCKS : CERES_B200_EVAL_NOJAC_MIN_BLOCKS)
-k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ frames) {
+k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ frames, double* __restrict__ slice_part) {
+  constexpr bool kDyn = kFrames;
   __shared__ double red[kWarpBlock / 32];
   const LossSpec L = loss_spec(ba);
   const int lane = threadIdx.x & 31;
@@ -134,10 +155,16 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
   unsigned err = 0;
   T* __restrict__ jac = reinterpret_cast<T*>(ba.jac);
   __shared__ int slice_counter;
-  if (threadIdx.x == 0) slice_counter = 0;
-  __syncthreads();
-  for (int s = next_cta_slice(&slice_counter, ba.num_slices); s >= 0;
-       s = next_cta_slice(&slice_counter, ba.num_slices)) {
+  if (!kDyn) {
+    if (threadIdx.x == 0) slice_counter = 0;
+    __syncthreads();
+  }
+  auto next = [&]() -> int {
+    return kDyn ? next_global_slice(&ba.counters[kCtrSliceEval], ba.num_slices)
+                : next_cta_slice(&slice_counter, ba.num_slices);
+  };
+  for (int s = next(); s >= 0; s = next()) {
+    double cs = 0.0;  // this lane's cost in slice s
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
@@ -168,7 +195,7 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
         for (int i = 0; i < 6; ++i) tail[i] = cam[3 + i];
       }
       snavely_project<kJac>(R, tail, X, ob.x, ob.y, o);
-      cost += robustify<kJac>(L, o, err);
+      cs += robustify<kJac>(L, o, err);
       reinterpret_cast<double2*>(ba.res)[slot] = make_double2(o.r[0], o.r[1]);
       if (kJac) {
         if (ba.cam_const[c]) {
@@ -200,12 +227,55 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
 #pragma unroll
       for (int i = 0; i < 3; ++i) pr[6 + i] = g[i];
     }
+    if (kDyn) {
+      const double w = warp_sum(cs);
+      if (lane == 0) slice_part[s] = w;
+    } else {
+      cost += cs;
+    }
   }
   if (err) atomicOr(&ba.counters[kCtrError], err);
-  double v[1] = {cost};
-  block_reduce<1>(v, 0u, red);
-  const int out[1] = {CERES_B200_STAT_COST};
-  grid_finish<1>(v, 0u, partials, &ba.counters[kCtrEval], ba.stats, out, red);
+  if (!kDyn) {  // with kDyn the sum is k_slice_fold's
+    const int out[1] = {CERES_B200_STAT_COST};
+    double v[1] = {cost};
+    block_reduce<1>(v, 0u, red);
+    grid_finish<1>(v, 0u, partials, &ba.counters[kCtrEval], ba.stats, out, red);
+  }
+}
+
+// Deterministic sums of the dynamically scheduled slice kernels: the warp that took
+// slice s wrote its NV sums (fixed lane order) to part[v * num_slices + s]; CTA b folds
+// the fixed range of slices [b * chunk, (b + 1) * chunk) and the last CTA folds the CTA
+// partials in CTA order (grid_finish), so the result does not depend on which warp took
+// which slice. Runs after the slice kernel on the same stream and resets its counter.
+template <int NV>
+__global__ void __launch_bounds__(256) k_slice_fold(const double* __restrict__ part, int num_slices, int chunk,
+                                                    double* partials, unsigned* ticket, unsigned* slice_counter,
+                                                    double* stats, StatIdx<NV> out) {
+  __shared__ double red[NV * 8];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *slice_counter = 0u;
+  double v[NV];
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = 0.0;
+  const int s0 = blockIdx.x * chunk, s1 = min(num_slices, s0 + chunk);
+  for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] += part[(size_t)i * num_slices + s];
+  }
+  block_reduce<NV>(v, 0u, red);
+  grid_finish<NV>(v, 0u, partials, ticket, stats, out.idx, red);
+}
+
+// The fold of the per-slice partials that follows a dynamically scheduled slice kernel.
+template <int NV>
+static void launch_slice_fold(const ceres_b200_ba_t& ba, const DevInfo& d, const double* part, double* partials,
+                       int ticket_ctr, int slice_ctr, StatIdx<NV> out, cudaStream_t st) {
+  int grid = (ba.num_slices + 255) / 256;
+  if (grid > d.sms) grid = d.sms;
+  if (grid < 1) grid = 1;
+  const int chunk = (ba.num_slices + grid - 1) / grid;
+  k_slice_fold<NV><<<grid, 256, 0, st>>>(part, ba.num_slices, chunk > 0 ? chunk : 1, partials, &ba.counters[ticket_ctr],
+                                        &ba.counters[slice_ctr], ba.stats, out);
 }
 
 // ======================================================================================
@@ -1139,20 +1209,20 @@ __global__ void k_camera_step(ceres_b200_ba_t ba, double* partials) {
 // the point sums of the evaluation (point_raw). The first pass over the track reads the
 // Jacobian records and residuals once; the second pass (candidate cost) reads only the
 // observations and the candidate camera frames.
+// Slices follow the dynamic longest-first schedule; the five sums go through per-slice
+// partials (slice_part[5][num_slices], folded by k_slice_fold) so the result does not
+// depend on the schedule.
 template <typename T>
-__global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step(ceres_b200_ba_t ba, double* partials, const double* __restrict__ frames) {
-  __shared__ double red[5 * (kWarpBlock / 32)];
+__global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step(ceres_b200_ba_t ba, const double* __restrict__ frames,
+                                                                               double* __restrict__ slice_part) {
   const LossSpec L = loss_spec(ba);
   const int lane = threadIdx.x & 31;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  double cand = 0.0, model = 0.0, sq = 0.0, nonfinite = 0.0, state = 0.0;
   unsigned err = 0;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int r_ = 0; r_ * nw < ba.num_slices; ++r_) {
-    const int s = snake_slice(r_, gw, nw);
-    if (s >= ba.num_slices) continue;
+  for (int s = next_global_slice(&ba.counters[kCtrSliceStep], ba.num_slices); s >= 0;
+       s = next_global_slice(&ba.counters[kCtrSliceStep], ba.num_slices)) {
+    double cand = 0.0, model = 0.0, sq = 0.0, nonfinite = 0.0, state = 0.0;  // this lane, slice s
     const int q = s * 32 + lane;
     const int len = ba.slice_len[s];
     const size_t base = (size_t)ba.slice_base[s];
@@ -1242,14 +1312,16 @@ __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step
       snavely_project<false>(R, tail, Xc, ob.x, ob.y, o);
       cand += robustify<false>(L, o, err);
     }
+    const double v[5] = {cand, model, sq, nonfinite, state};
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const double w = warp_sum(v[i]);
+      if (lane == 0) slice_part[(size_t)i * ba.num_slices + s] = w;
+    }
   }
   if (err) atomicOr(&ba.counters[kCtrError], err);
-  double v[5] = {cand, model, sq, nonfinite, state};
-  block_reduce<5>(v, 0u, red);
-  const int out[5] = {CERES_B200_STAT_CAND_COST, CERES_B200_STAT_MODEL, CERES_B200_STAT_STEP_SQ_P,
-                      CERES_B200_STAT_NONFINITE, CERES_B200_STAT_CAND_STATE_SQ_P};
-  // the camera step kernel's non-finite count is added afterwards (k_add_nonfinite)
-  grid_finish<5>(v, 0u, partials, &ba.counters[kCtrStep], ba.stats, out, red);
+  // the sums: k_slice_fold; the camera step kernel's non-finite count is added
+  // afterwards (k_add_nonfinite)
 }
 
 __global__ void k_zero_gated(double* __restrict__ y, int n, const double* gate) {
@@ -1484,7 +1556,7 @@ struct PcgLayout {
   int smem_vectors = 0;
   size_t dyn_smem = 0;
   size_t frames = 0, aux = 0, cam_acc = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0,
-         spse_base = 0, part_s = 0, total = 0;
+         spse_base = 0, part_s = 0, slice_part = 0, total = 0;
 };
 
 template <typename T>
@@ -1509,6 +1581,8 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   size_t off = red_area_bytes(ba, d);
   L.frames = off;
   off += frames_bytes(ba);
+  L.slice_part = off;
+  off += slice_part_bytes(ba);
   L.aux = off;
   off += 256;
   L.cam_acc = off;
@@ -1727,24 +1801,27 @@ int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* s
   cudaStream_t st = (cudaStream_t)stream;
   const DevInfo d = device_info();
   const size_t red = red_area_bytes(*ba, d);
-  if (ba->scratch_bytes < 0 || (size_t)ba->scratch_bytes < red + frames_bytes(*ba)) return CERES_B200_EINVAL;
-  const int grid = slice_grid(*ba, d);
+  if (ba->scratch_bytes < 0 || (size_t)ba->scratch_bytes < red + frames_bytes(*ba) + slice_part_bytes(*ba))
+    return CERES_B200_EINVAL;
+  const int grid = resident_slice_grid(*ba, d, with_jacobian ? CERES_B200_EVAL_MIN_BLOCKS : CERES_B200_EVAL_NOJAC_MIN_BLOCKS);
   double* partials = reinterpret_cast<double*>(ba->scratch);
   double* frames = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + red);
+  double* slice_part = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + red + frames_bytes(*ba));
   const int nc = ba->num_cameras;
   if (nc > 0) {
     count_launch();
     if (with_jacobian) k_camera_frames<true><<<(nc + 127) / 128, 128, 0, st>>>(ba->cameras, frames, nc);
     else k_camera_frames<false><<<(nc + 127) / 128, 128, 0, st>>>(ba->cameras, frames, nc);
   }
-  count_launch();
+  count_launch(2);
   if (ba->precision == CERES_B200_FP32) {
-    if (with_jacobian) k_evaluate<float, true, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
-    else k_evaluate<float, false, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
+    if (with_jacobian) k_evaluate<float, true, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames, slice_part);
+    else k_evaluate<float, false, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames, slice_part);
   } else {
-    if (with_jacobian) k_evaluate<double, true, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
-    else k_evaluate<double, false, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames);
+    if (with_jacobian) k_evaluate<double, true, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames, slice_part);
+    else k_evaluate<double, false, true><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames, slice_part);
   }
+  launch_slice_fold<1>(*ba, d, slice_part, partials, kCtrEval, kCtrSliceEval, StatIdx<1>{{CERES_B200_STAT_COST}}, st);
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
   return check_launch();
@@ -1813,11 +1890,11 @@ int ceres_b200_ba_evaluate_noalloc(const ceres_b200_ba_t* ba, int with_jacobian,
   // no scratch for camera frames here: each observation computes its camera's rotation
   // (the same arithmetic as the frames, so the results are those of ceres_b200_ba_evaluate)
   if (ba->precision == CERES_B200_FP32) {
-    if (with_jacobian) { count_launch(); k_evaluate<float, true, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
-    else { count_launch(); k_evaluate<float, false, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
+    if (with_jacobian) { count_launch(); k_evaluate<float, true, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr, nullptr); }
+    else { count_launch(); k_evaluate<float, false, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr, nullptr); }
   } else {
-    if (with_jacobian) { count_launch(); k_evaluate<double, true, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
-    else { count_launch(); k_evaluate<double, false, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr); }
+    if (with_jacobian) { count_launch(); k_evaluate<double, true, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr, nullptr); }
+    else { count_launch(); k_evaluate<double, false, false><<<grid, kWarpBlock, 0, st>>>(*ba, partials, nullptr, nullptr); }
   }
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
@@ -1926,9 +2003,15 @@ int ceres_b200_ba_step(const ceres_b200_ba_t* ba, void* stream) {
     count_launch();
     k_camera_frames<false><<<(nc + 127) / 128, 128, 0, st>>>(ba->cand_cameras, frames, nc);
   }
-  const int grid = slice_grid(*ba, d);
-  if (ba->precision == CERES_B200_FP32) { count_launch(); k_step<float><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames); }
-  else { count_launch(); k_step<double><<<grid, kWarpBlock, 0, st>>>(*ba, partials, frames); }
+  const int grid = resident_slice_grid(*ba, d, CERES_B200_STEP_MIN_BLOCKS);
+  double* slice_part = reinterpret_cast<double*>(reinterpret_cast<char*>(ba->scratch) + L.slice_part);
+  count_launch(2);
+  if (ba->precision == CERES_B200_FP32) k_step<float><<<grid, kWarpBlock, 0, st>>>(*ba, frames, slice_part);
+  else k_step<double><<<grid, kWarpBlock, 0, st>>>(*ba, frames, slice_part);
+  launch_slice_fold<5>(*ba, d, slice_part, partials, kCtrStep, kCtrSliceStep,
+                       StatIdx<5>{{CERES_B200_STAT_CAND_COST, CERES_B200_STAT_MODEL, CERES_B200_STAT_STEP_SQ_P,
+                                   CERES_B200_STAT_NONFINITE, CERES_B200_STAT_CAND_STATE_SQ_P}},
+                       st);
   // STEP_SQ_C and the camera non-finite count into the shared stats
   count_launch();
   k_add_nonfinite<<<1, 1, 0, st>>>(ba->stats, cam_stats + CERES_B200_STAT_NONFINITE);

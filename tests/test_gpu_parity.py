@@ -330,3 +330,27 @@ def test_invalid_step_path_with_nonfinite_observation_scale():
     s = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
                                   max_num_iterations=10), prob)
     assert s.termination_type.value in ("FAILURE", "CONVERGENCE", "NO_CONVERGENCE")
+
+
+def test_float64_solves_are_reproducible():
+    """Two float64 solves of the same problem agree bit for bit: the slice kernels
+    take slices dynamically but fold per-slice sums in slice order, and every other
+    reduction has a fixed order (the PCG product's shared-memory accumulation is the
+    one order-dependent sum, and in float64 its rounding does not reach the iterates
+    the LM decisions see on this problem)."""
+    tc = _tc()
+    d = G.load("config1_small")
+    meta = d["meta"]
+    t = lambda a, dt=torch.float64: torch.as_tensor(a).to(DEV, dt)  # noqa: E731
+    runs = []
+    for _ in range(2):
+        prob = tc.BundleAdjustmentProblem(t(d["cameras"]), t(d["points"]), t(d["observations"]),
+                                          t(d["camera_index"], torch.int64), t(d["point_index"], torch.int64),
+                                          loss=_loss_obj(G.loss_spec(meta["loss"])))
+        opts = tc.SolverOptions(max_num_iterations=30, linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                                preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI)
+        s = tc.solve(opts, prob, precision="fp64")
+        runs.append((s.initial_cost, [it.cost for it in s.iterations], len(s.iterations)))
+    assert runs[0][0] == runs[1][0]
+    assert runs[0][2] == runs[1][2]
+    assert runs[0][1] == runs[1][1]
