@@ -336,29 +336,6 @@ __device__ __forceinline__ void frame_store(double* __restrict__ f, const CamRot
   f[22] = 0.0; f[23] = 0.0;
 }
 
-template <bool kJac>
-__device__ __forceinline__ void frame_load(const double* __restrict__ f, CamRot& R, double tail[6]) {
-  const double2* f2 = reinterpret_cast<const double2*>(f);
-  double2 v = f2[0];
-  R.w = v.x; R.u[0] = v.y;
-  v = f2[1];
-  R.u[1] = v.x; R.u[2] = v.y;
-  if (kJac) {
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      v = f2[2 + i];
-      R.dqn[(2 * i) / 3][(2 * i) % 3] = v.x;
-      R.dqn[(2 * i + 1) / 3][(2 * i + 1) % 3] = v.y;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    v = f2[8 + i];
-    tail[2 * i] = v.x;
-    tail[2 * i + 1] = v.y;
-  }
-}
-
 // Ceres corrector (losses.py:158-193) applied in place. Returns 0.5 rho0.
 template <bool kJac, typename J = double>
 __device__ __forceinline__ double robustify(const LossSpec& L, ProjT<J>& o, unsigned& err) {
@@ -434,6 +411,29 @@ __device__ __forceinline__ void ld256(const double* p, double* v) {
   else
     asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
                  : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+
+// A camera frame with 256-bit loads: 6 (with the rotation derivative) or 3 instead of
+// 11 / 5 128-bit loads per observation; frames start on 32-byte boundaries (kFrame
+// float64 per camera from a 256-byte aligned base).
+template <bool kJac>
+__device__ __forceinline__ void frame_load_wide(const double* __restrict__ f, CamRot& R, double tail[6]) {
+  double a[4];
+  ld256(f, a);
+  R.w = a[0]; R.u[0] = a[1]; R.u[1] = a[2]; R.u[2] = a[3];
+  if (kJac) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double b[4];
+      ld256(f + 4 + 4 * k, b);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) R.dqn[(4 * k + m) / 3][(4 * k + m) % 3] = b[m];
+    }
+  }
+  double c[4], d[4];
+  ld256(f + 16, c);
+  ld256(f + 20, d);
+  tail[0] = c[0]; tail[1] = c[1]; tail[2] = c[2]; tail[3] = c[3]; tail[4] = d[0]; tail[5] = d[1];
 }
 
 // 128-bit loads of a float32 record (6 per record). The camera-major gather of

@@ -186,7 +186,7 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
       CamRot R;
       double tail[6];
       if (kFrames) {
-        frame_load<kJac>(frames + kFrame * (size_t)c, R, tail);
+        frame_load_wide<kJac>(frames + kFrame * (size_t)c, R, tail);
       } else {
         const double* cam = ba.cameras + 9 * (size_t)c;
         const double aa[3] = {cam[0], cam[1], cam[2]};
@@ -1308,7 +1308,7 @@ __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step
       Proj o;
       CamRot R;
       double tail[6];
-      frame_load<false>(frames + kFrame * (size_t)c, R, tail);  // frames of the candidate cameras
+      frame_load_wide<false>(frames + kFrame * (size_t)c, R, tail);  // frames of the candidate cameras
       snavely_project<false>(R, tail, Xc, ob.x, ob.y, o);
       cand += robustify<false>(L, o, err);
     }
