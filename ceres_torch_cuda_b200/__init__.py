@@ -23,6 +23,8 @@ from .losses import (ArctanLoss, CauchyLoss, ComposedLoss, HuberLoss, LossFuncti
 from .problem import (BundleAdjustmentProblem, CostFunction, ParameterBlock, Problem, ProblemOptions, ResidualBlock,
                       SnavelyReprojectionError, snavely_project)
 from .solver import solve
+from .dropin import install
+from .covariance import Covariance, CovarianceOptions, CovarianceSummary
 from .types import (DYNAMIC, CallbackReturnType, DenseLinearAlgebraLibraryType, DoglegType, IterationSummary,
                     LinearSolverType, LineSearchDirectionType, LineSearchInterpolationType, LineSearchType,
                     LoggingType, MinimizerType, NonlinearConjugateGradientType, PreconditionerType, SolverOptions,

@@ -16,7 +16,7 @@ c_int64 = ctypes.c_int64
 c_double = ctypes.c_double
 c_void_p = ctypes.c_void_p
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 OK = 0
 EINVAL = -1
@@ -35,6 +35,7 @@ LOSS_TRIVIAL, LOSS_HUBER, LOSS_SOFTLONE, LOSS_CAUCHY, LOSS_ARCTAN, LOSS_TOLERANT
 PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_SCHUR_JACOBI, PRECOND_SCHUR_POWER_SERIES = range(4)
 PRECOND_FLAG_SPSE_BASE = 0x100  # camera_assemble: also build the Hbb blocks of the SPSE initial point
 FP64, FP32 = 0, 1
+CAM_ITEM = 256  # CERES_B200_CAM_ITEM: entries per camera work item
 
 (STAT_COST, STAT_GMAX_P, STAT_GSQ_P, STAT_GMAX_C, STAT_GSQ_C, STAT_CAND_COST, STAT_MODEL, STAT_STEP_SQ_P,
  STAT_STEP_SQ_C, STAT_NONFINITE, STAT_PCG_ITERS, STAT_PCG_SUCCESS, STAT_PCG_RNORM, STAT_ERROR, STAT_RHS_NORM,
@@ -65,6 +66,8 @@ class BAStruct(ctypes.Structure):
         ("point_raw", c_void_p), ("winv", c_void_p), ("winv_ga", c_void_p), ("step_points", c_void_p),
         ("cam_diag", c_void_p), ("precond", c_void_p), ("rhs", c_void_p), ("step_cameras", c_void_p),
         ("pcg_x", c_void_p), ("pcg_r", c_void_p), ("pcg_z", c_void_p), ("pcg_p", c_void_p), ("pcg_ap", c_void_p),
+        ("slot_pos", c_void_p), ("cm_jac", c_void_p), ("cam_items", c_void_p), ("items", c_void_p),
+        ("num_items", c_int32), ("max_camera_obs", c_int32),
         ("scratch", c_void_p), ("scratch_bytes", c_int64),
         ("counters", c_void_p), ("stats", c_void_p),
     ]
@@ -132,6 +135,9 @@ SIGNATURES = {
     "ceres_b200_dense_cholesky_solve": (c_int32, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
     "ceres_b200_batch_struct_bytes": (c_int32, []),
     "ceres_b200_batch_solve": (c_int32, [_PB, c_int32, c_int32, c_int32, c_void_p]),
+    "ceres_b200_debug_barrier_timeout": (c_int32, [c_void_p, ctypes.c_uint32, c_void_p]),
+    "ceres_b200_ba_schur_matrix": (c_int32, [_P, c_void_p, c_void_p]),
+    "ceres_b200_dense_spd_inverse": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
 }
 
 _LIB: ctypes.CDLL | None = None

@@ -25,10 +25,15 @@ def library_path() -> Path:
     return LIBDIR / LIBNAME
 
 
+OBJDIR = PKG / "_build"
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
 def _inputs() -> list[Path]:
-    files = [CSRC / s for s in SOURCES]
-    files += sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
-    return files
+    return [CSRC / s for s in SOURCES] + _headers()
 
 
 def is_stale() -> bool:
@@ -39,26 +44,69 @@ def is_stale() -> bool:
     return any(f.stat().st_mtime > mtime for f in _inputs())
 
 
+def _object(src: str) -> Path:
+    return OBJDIR / (Path(src).stem + ".o")
+
+
+def _object_stale(src: str) -> bool:
+    obj = _object(src)
+    if not obj.exists():
+        return True
+    mtime = obj.stat().st_mtime
+    return any(f.stat().st_mtime > mtime for f in [CSRC / src, *_headers()])
+
+
+def _nvcc() -> str:
+    return shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+
+
+def _common_flags() -> list[str]:
+    return [*ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "--Werror", "all-warnings", "-Xcompiler", "-fPIC",
+            f"-I{INCLUDE}"]
+
+
 def nvcc_command(output: Path, extra: list[str] | None = None) -> list[str]:
-    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    return [nvcc, *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "--Werror", "all-warnings", "-Xcompiler", "-fPIC", "-shared",
-            f"-I{INCLUDE}", "-o", str(output), *[str(CSRC / s) for s in SOURCES], *(extra or [])]
+    """One nvcc line that compiles every source into ``output`` (a shared library)."""
+    return [_nvcc(), *_common_flags(), "-shared", "-o", str(output), *[str(CSRC / s) for s in SOURCES],
+            *(extra or [])]
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the library if it is missing or older than its sources."""
+    """Compile the library if it is missing or older than its sources. Each source is
+    compiled to its own object (in parallel, only when it or a header changed), then
+    the objects are linked."""
     lib = library_path()
     if not force and not is_stale():
         return lib
     LIBDIR.mkdir(parents=True, exist_ok=True)
+    OBJDIR.mkdir(parents=True, exist_ok=True)
+    procs = []
+    for src in SOURCES:
+        if not force and not _object_stale(src):
+            continue
+        tmp = _object(src).with_suffix(f".o.tmp{os.getpid()}")
+        cmd = [_nvcc(), *_common_flags(), "-c", "-o", str(tmp), str(CSRC / src)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((src, tmp, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    failed = []
+    for src, tmp, proc in procs:
+        out, _ = proc.communicate()
+        if proc.returncode != 0:
+            sys.stderr.write(out)
+            failed.append(src)
+        else:
+            os.replace(tmp, _object(src))
+    if failed:
+        raise RuntimeError(f"nvcc failed compiling {', '.join(failed)} for {LIBNAME}")
     tmp = lib.with_suffix(f".so.tmp{os.getpid()}")
-    cmd = nvcc_command(tmp)
+    cmd = [_nvcc(), *ARCH_FLAGS, "-shared", "-o", str(tmp), *[str(_object(s)) for s in SOURCES]]
     if verbose:
         print(" ".join(cmd), flush=True)
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         sys.stderr.write(proc.stdout + proc.stderr)
-        raise RuntimeError(f"nvcc failed building {LIBNAME} (exit {proc.returncode})")
+        raise RuntimeError(f"nvcc failed linking {LIBNAME} (exit {proc.returncode})")
     os.replace(tmp, lib)
     return lib
 

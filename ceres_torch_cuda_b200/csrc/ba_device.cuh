@@ -721,6 +721,7 @@ struct GridBarrier {
   unsigned* count;
   unsigned* generation;
   unsigned* flag;
+  unsigned limit = kSpinLimit;  // polls before the wait gives up
 };
 
 __device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
@@ -745,7 +746,7 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& gb) {
         unsigned spins = 0;
         while (gen.load(cuda::memory_order_acquire) == my_gen) {
           if (flg.load(cuda::memory_order_relaxed) != 0u) { good = 0; break; }
-          if (++spins > kSpinLimit) {
+          if (++spins > gb.limit) {
             flg.fetch_or(CERES_B200_DEVERR_BARRIER, cuda::memory_order_relaxed);
             good = 0;
             break;

@@ -6,6 +6,7 @@
 // (96 B in FP32, 192 B in FP64) read with 128-bit loads. Every kernel is
 // bandwidth-bound; all reductions are deterministic (fixed CTA count, fixed
 // fold order) so a solve is bit-reproducible on one device.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -207,6 +208,8 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
           for (int j = 0; j < 3; ++j) o.jp[0][j] = o.jp[1][j] = 0.0;
         }
         store_rec(jac, slot, o);
+        // the camera-major copy (the camera-side passes stream it in camera order)
+        store_rec(reinterpret_cast<T*>(ba.cm_jac), (size_t)ba.slot_pos[slot], o);
         double a[3], b[3];
 #pragma unroll
         for (int m = 0; m < 3; ++m) { a[m] = (double)(T)o.jp[0][m]; b[m] = (double)(T)o.jp[1][m]; }
@@ -348,12 +351,13 @@ struct CamObs {
   double wg[3];
 };
 
+// The record comes from the camera-major copy (entry e: consecutive threads read
+// consecutive records); residual and point blocks are gathered by slot and point.
 template <typename T>
-__device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ jac,
-                                             const T* __restrict__ winv, int2 ent, CamObs<T>& o) {
+__device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ cm,
+                                             const T* __restrict__ winv, int e, int2 ent, CamObs<T>& o) {
   o.ent = ent;
-  if constexpr (sizeof(T) == 4) load_rec128(jac, (size_t)ent.x, o.rv);
-  else load_rec(jac, (size_t)ent.x, o.rv);
+  load_rec(cm, (size_t)e, o.rv);
   o.r = reinterpret_cast<const double2*>(ba.res)[ent.x];
 #pragma unroll
   for (int i = 0; i < 6; ++i) o.wi[i] = winv[6 * (size_t)ent.y + i];
@@ -370,6 +374,7 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
   __shared__ double sred[kCamAcc * (kCamBlock / 32)];
   const int c = blockIdx.x;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  const T* __restrict__ cm = reinterpret_cast<const T*>(ba.cm_jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
   A av[54];      // Schur block (upper triangle, 45), column sums (9)
   double ag[18]; // gradient (9), reduced rhs (9)
@@ -391,7 +396,7 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
     int2 en2 = first + stride < e1 ? ents[first + stride] : make_int2(0, 0);
     for (int e = first; e < e1; e += stride) {
       CamObs<T> cur;
-      cam_obs_load(ba, jac, winv, en1, cur);
+      cam_obs_load(ba, cm, winv, e, en1, cur);
       en1 = en2;
       en2 = e + 2 * stride < e1 ? ents[e + 2 * stride] : make_int2(0, 0);
       const size_t slot = (size_t)cur.ent.x;
@@ -594,13 +599,20 @@ __global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_
 }
 
 // ======================================================================================
-// Implicit Schur product, point-major: for the points of one slice lane,
-//   t = sum_k Jp_k^T (Jc_k p_c(k)),  s = W^-1 t,  y_c(k) += Jc_k^T (Jc_k p_c(k) - Jp_k s)
-// The accumulation target y is shared memory (per-CTA partial) or global memory.
+// Implicit Schur product S p = (U + D) p - H_cp W^-1 H_pc p in two passes that need no
+// atomics and give the same sums whatever the schedule:
+//   point pass  (point-major store, lane = point, a warp per slice):
+//                 s_q = W_q^-1 sum_k Jp_k^T (Jc_k p_c(k))
+//   camera pass (camera-major copy, a warp per camera work item):
+//                 y_item = sum over the item's entries of Jc^T (Jc p_c - Jp s_q)
+//               summed across the warp by a fixed shuffle tree; a camera's items are then
+//               added in item order (fold_items).
+// kE: the eliminated term E p = H_cp W^-1 H_pc p only, y = sum Jc^T Jp s_q (the
+// SCHUR_POWER_SERIES_EXPANSION series multiplies by E).
 // ======================================================================================
-// Observations processed per step of a lane's track walk: their loads are all
-// issued before any is used, so a warp keeps kUnroll records in flight.
-template <typename T> struct Unroll { static constexpr int v = 2; };
+// Observations processed per step of a lane's walk: their loads are all issued before
+// any is used, so a warp keeps two records in flight per lane.
+constexpr int kUnroll = 2;
 
 template <typename T, typename TP, typename A, bool kCrossP>
 __device__ __forceinline__ void camera_product(const T* rv, const TP* __restrict__ pc, A& u0, A& u1) {
@@ -614,177 +626,215 @@ __device__ __forceinline__ void camera_product(const T* rv, const TP* __restrict
   }
 }
 
-// The product contribution of one slice s (lane = point), accumulated into y.
-// kE: only the eliminated term E p = Hba Haa^-1 Hab p, y_c(k) += Jc_k^T Jp_k s (the
-// SCHUR_POWER_SERIES_EXPANSION series multiplies by E).
-template <typename T, typename TP, typename A, bool kCrossP, bool kE = false>
-__device__ __forceinline__ void matvec_one_slice(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int s,
-                                                 int lane) {
-  constexpr int U = Unroll<T>::v;
+// Point pass of slice s: sv[q] = W_q^-1 t_q with t_q = sum_k Jp_k^T (Jc_k p_c(k)) (float64).
+template <typename T, typename TP, typename A, bool kCrossP>
+__device__ __forceinline__ void point_pass_slice(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec,
+                                                 double* __restrict__ sv, int s, int lane) {
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  {
-    const int q = s * 32 + lane;
-    const int len = ba.slice_len[s];
-    const size_t base = (size_t)ba.slice_base[s] + lane;
-    // padding slots hold zero Jacobians and camera -1; they are read like any slot
-    // (camera 0 stands in for the address) and add nothing
-    A t0 = 0, t1 = 0, t2 = 0;
-    int k = 0;
-    for (; k + U <= len; k += U) {
-      int c[U];
-      T rv[U][kRec];
+  const int q = s * 32 + lane;
+  const int len = ba.slice_len[s];
+  const size_t base = (size_t)ba.slice_base[s] + lane;
+  // padding slots hold zero Jacobians and camera -1; they are read like any slot
+  // (camera 0 stands in for the address) and add nothing
+  A t0 = 0, t1 = 0, t2 = 0;
+  int k = 0;
+  for (; k + kUnroll <= len; k += kUnroll) {
+    int c[kUnroll];
+    T rv[kUnroll][kRec];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const size_t slot = base + 32 * (size_t)(k + u);
-        c[u] = ba.slot_cam[slot];
-        load_rec(jac, slot, rv[u]);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        A u0, u1;
-        camera_product<T, TP, A, kCrossP>(rv[u], pvec + 9 * (size_t)max(c[u], 0), u0, u1);
-        t0 += (A)rv[u][18] * u0 + (A)rv[u][21] * u1;
-        t1 += (A)rv[u][19] * u0 + (A)rv[u][22] * u1;
-        t2 += (A)rv[u][20] * u0 + (A)rv[u][23] * u1;
-      }
+    for (int u = 0; u < kUnroll; ++u) {
+      const size_t slot = base + 32 * (size_t)(k + u);
+      c[u] = ba.slot_cam[slot];
+      load_rec(jac, slot, rv[u]);
     }
-    for (; k < len; ++k) {
-      const size_t slot = base + 32 * (size_t)k;
-      const int c = ba.slot_cam[slot];
-      T rv[kRec];
-      load_rec(jac, slot, rv);
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
       A u0, u1;
-      camera_product<T, TP, A, kCrossP>(rv, pvec + 9 * (size_t)max(c, 0), u0, u1);
-      t0 += (A)rv[18] * u0 + (A)rv[21] * u1;
-      t1 += (A)rv[19] * u0 + (A)rv[22] * u1;
-      t2 += (A)rv[20] * u0 + (A)rv[23] * u1;
-    }
-    const T* wi = winv + 6 * (size_t)q;
-    const A w0 = (A)wi[0], w1 = (A)wi[1], w2 = (A)wi[2], w3 = (A)wi[3], w4 = (A)wi[4], w5 = (A)wi[5];
-    const A s0 = w0 * t0 + w1 * t1 + w2 * t2;
-    const A s1 = w1 * t0 + w3 * t1 + w4 * t2;
-    const A s2 = w2 * t0 + w4 * t1 + w5 * t2;
-    k = 0;
-    for (; k + U <= len; k += U) {
-      int c[U];
-      T rv[U][kRec];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const size_t slot = base + 32 * (size_t)(k + u);
-        c[u] = ba.slot_cam[slot];
-        load_rec(jac, slot, rv[u]);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (c[u] < 0) continue;
-        A v0 = (A)rv[u][18] * s0 + (A)rv[u][19] * s1 + (A)rv[u][20] * s2;
-        A v1 = (A)rv[u][21] * s0 + (A)rv[u][22] * s1 + (A)rv[u][23] * s2;
-        if constexpr (!kE) {
-          A u0, u1;
-          camera_product<T, TP, A, kCrossP>(rv[u], pvec + 9 * (size_t)c[u], u0, u1);
-          v0 = u0 - v0;
-          v1 = u1 - v1;
-        }
-        A* yc = y + 9 * (size_t)c[u];
-#pragma unroll
-        for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[u][j] * v0 + (A)rv[u][9 + j] * v1);
-      }
-    }
-    for (; k < len; ++k) {
-      const size_t slot = base + 32 * (size_t)k;
-      const int c = ba.slot_cam[slot];
-      if (c < 0) continue;
-      T rv[kRec];
-      load_rec(jac, slot, rv);
-      A v0 = (A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2;
-      A v1 = (A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2;
-      if constexpr (!kE) {
-        A u0, u1;
-        camera_product<T, TP, A, kCrossP>(rv, pvec + 9 * (size_t)c, u0, u1);
-        v0 = u0 - v0;
-        v1 = u1 - v1;
-      }
-      A* yc = y + 9 * (size_t)c;
-#pragma unroll
-      for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[j] * v0 + (A)rv[9 + j] * v1);
+      camera_product<T, TP, A, kCrossP>(rv[u], pvec + 9 * (size_t)max(c[u], 0), u0, u1);
+      t0 += (A)rv[u][18] * u0 + (A)rv[u][21] * u1;
+      t1 += (A)rv[u][19] * u0 + (A)rv[u][22] * u1;
+      t2 += (A)rv[u][20] * u0 + (A)rv[u][23] * u1;
     }
   }
+  for (; k < len; ++k) {
+    const size_t slot = base + 32 * (size_t)k;
+    const int c = ba.slot_cam[slot];
+    T rv[kRec];
+    load_rec(jac, slot, rv);
+    A u0, u1;
+    camera_product<T, TP, A, kCrossP>(rv, pvec + 9 * (size_t)max(c, 0), u0, u1);
+    t0 += (A)rv[18] * u0 + (A)rv[21] * u1;
+    t1 += (A)rv[19] * u0 + (A)rv[22] * u1;
+    t2 += (A)rv[20] * u0 + (A)rv[23] * u1;
+  }
+  const T* wi = winv + 6 * (size_t)q;
+  const A w0 = (A)wi[0], w1 = (A)wi[1], w2 = (A)wi[2], w3 = (A)wi[3], w4 = (A)wi[4], w5 = (A)wi[5];
+  double* o = sv + 3 * (size_t)q;
+  o[0] = (double)(w0 * t0 + w1 * t1 + w2 * t2);
+  o[1] = (double)(w1 * t0 + w3 * t1 + w4 * t2);
+  o[2] = (double)(w2 * t0 + w4 * t1 + w5 * t2);
 }
 
-// Static slice walk: warp gw of nw takes the slices of snake_slice(r, gw, nw).
-template <typename T, typename TP, typename A, bool kCrossP = false, bool kE = false>
-__device__ __forceinline__ void matvec_slices(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y, int gw,
-                                              int nw) {
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum_any(double v) { return warp_sum(v); }
+__device__ __forceinline__ float warp_sum_any(float v) { return warp_sum_f(v); }
+
+// Camera pass of work item `item` (camera c, entries e0..e1-1 of the camera-major copy):
+// y = sum_e Jc_e^T (Jc_e p_c - Jp_e s_q(e)) (kE: Jc_e^T Jp_e s_q(e)). Lane l takes
+// entries e0 + l, e0 + l + 32, ...; the 32 lane sums are added by a butterfly whose
+// pairwise additions commute, so every lane ends with the same bits. sv was written by
+// other CTAs of the same launch (read through L2).
+template <typename T, typename TP, typename A, bool kCrossP, bool kE>
+__device__ __forceinline__ int camera_pass_item(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec,
+                                                const double* __restrict__ sv, int item, int lane, A y[9]) {
+  const int2 it = reinterpret_cast<const int2*>(ba.items)[item];
+  const int c = it.x, e0 = it.y;
+  const int e1 = min(e0 + CERES_B200_CAM_ITEM, ba.cam_offsets[c + 1]);
+  const T* __restrict__ cm = reinterpret_cast<const T*>(ba.cm_jac);
+  const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);
+  A pc[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    pc[j] = 0;
+    if (!kE) pc[j] = kCrossP ? (A)ld_cross(pvec + 9 * (size_t)c + j) : (A)pvec[9 * (size_t)c + j];
+    y[j] = 0;
+  }
+  auto one = [&](const T* rv, int q) {
+    const double* sq = sv + 3 * (size_t)q;
+    const A s0 = (A)ld_cross(sq), s1 = (A)ld_cross(sq + 1), s2 = (A)ld_cross(sq + 2);
+    A v0 = (A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2;
+    A v1 = (A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2;
+    if constexpr (!kE) {
+      A u0 = 0, u1 = 0;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        u0 += (A)rv[j] * pc[j];
+        u1 += (A)rv[9 + j] * pc[j];
+      }
+      v0 = u0 - v0;
+      v1 = u1 - v1;
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) y[j] += (A)rv[j] * v0 + (A)rv[9 + j] * v1;
+  };
+  int e = e0 + lane;
+  for (; e + 32 * (kUnroll - 1) < e1; e += 32 * kUnroll) {
+    T rv[kUnroll][kRec];
+    int q[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      load_rec(cm, (size_t)(e + 32 * u), rv[u]);
+      q[u] = ents[e + 32 * u].y;
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) one(rv[u], q[u]);
+  }
+  for (; e < e1; e += 32) {
+    T rv[kRec];
+    load_rec(cm, (size_t)e, rv);
+    one(rv, ents[e].y);
+  }
+#pragma unroll
+  for (int j = 0; j < 9; ++j) y[j] = warp_sum_any(y[j]);
+  return c;
+}
+
+// The camera pass over a range of warps: warp gw of nw takes items gw, gw + nw, ... and
+// writes each item's 9 sums (float64) to part[item]. Returns this thread's share of
+// sum_items dot_p_c . y_item (lane 0 only; 0 elsewhere) when dot_p is set.
+template <typename T, typename TP, typename A, bool kCrossP, bool kE>
+__device__ __forceinline__ double camera_pass(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec,
+                                              const double* __restrict__ sv, double* __restrict__ part,
+                                              const double* __restrict__ dot_p, int gw, int nw) {
   const int lane = threadIdx.x & 31;
-  for (int r = 0; r * nw < ba.num_slices; ++r) {
-    const int s = snake_slice(r, gw, nw);
-    if (s >= ba.num_slices) continue;
-    matvec_one_slice<T, TP, A, kCrossP, kE>(ba, pvec, y, s, lane);
+  double dot = 0.0;
+  for (int i = gw; i < ba.num_items; i += nw) {
+    A y[9];
+    const int c = camera_pass_item<T, TP, A, kCrossP, kE>(ba, pvec, sv, i, lane, y);
+    double mine = 0.0;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) mine = (lane == j) ? (double)y[j] : mine;
+    if (lane < 9) part[9 * (size_t)i + lane] = mine;
+    if (dot_p != nullptr && lane == 0) {
+      double d = 0.0;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) d += ld_cross(dot_p + 9 * (size_t)c + j) * (double)y[j];
+      dot += d;
+    }
   }
+  return dot;
 }
 
-// Balanced slice walk for the persistent PCG: CTA b owns one slice of every round of
-// gridDim.x slices (snake order over the CTAs, so the CTAs' totals agree to a few per
-// cent although slices are sorted by length), and its warps take the CTA's slices in
-// that order from a shared-memory counter (*counter zero on entry), longest first.
-// A static warp-by-warp assignment left the heaviest CTA with 1.3x the mean work, and
-// every CTA waited for it at the grid barrier.
-template <typename T, typename TP, typename A, bool kCrossP = false, bool kE = false>
-__device__ __forceinline__ void matvec_slices_cta(const ceres_b200_ba_t& ba, const TP* __restrict__ pvec, A* y,
-                                                  int* counter) {
-  const int lane = threadIdx.x & 31;
-  const int G = gridDim.x, b = blockIdx.x;
-  for (;;) {
-    int i = 0;
-    if (lane == 0) i = atomicAdd(counter, 1);
-    i = __shfl_sync(0xffffffffu, i, 0);
-    const long long s = (long long)i * G + ((i & 1) ? G - 1 - b : b);
-    if (s >= ba.num_slices) break;
-    matvec_one_slice<T, TP, A, kCrossP, kE>(ba, pvec, y, (int)s, lane);
+// out[j] for camera entries j in [j0, j1): the camera's item sums in item order, plus
+// D V when add_diag. Returns this thread's share of sum_j V_j out_j.
+__device__ __forceinline__ double fold_items(const ceres_b200_ba_t& ba, const double* __restrict__ part,
+                                             const double* __restrict__ V, double* __restrict__ out, int j0, int j1,
+                                             bool add_diag) {
+  double dot = 0.0;
+  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+    const int c = j / 9, m = j - 9 * c;
+    double y = 0.0;
+    const int i1 = ba.cam_items[c + 1];
+    for (int i = ba.cam_items[c]; i < i1; ++i) y += ld_cross(part + 9 * (size_t)i + m);
+    const double vj = ld_cross(V + j);
+    if (add_diag) y += ba.cam_diag[j] * vj;
+    out[j] = y;
+    dot += vj * y;
   }
+  return dot;
 }
 
-// y = S x with float64 accumulation (global atomics), for tests and refinement.
+// y = S x for the test entry point: the same two passes in float64 arithmetic, one
+// launch each, then the fold.
 template <typename T>
-__global__ void __launch_bounds__(kWarpBlock) k_matvec_points(ceres_b200_ba_t ba, const double* __restrict__ x,
-                                                              double* y, const double* gate) {
-  if (gate != nullptr && *gate != 0.0) return;
+__global__ void __launch_bounds__(kWarpBlock) k_point_pass64(ceres_b200_ba_t ba, const double* __restrict__ x,
+                                                             double* __restrict__ sv) {
+  const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  matvec_slices<T, double, double>(ba, x, y, gw, nw);
+  for (int s = gw; s < ba.num_slices; s += nw) point_pass_slice<T, double, double, true>(ba, x, sv, s, lane);
 }
 
-__global__ void k_matvec_diag(ceres_b200_ba_t ba, const double* __restrict__ x, double* y, const double* __restrict__ rhs,
-                              double* out_res, const double* gate) {
-  if (gate != nullptr && *gate != 0.0) return;
+template <typename T>
+__global__ void __launch_bounds__(kWarpBlock) k_camera_pass64(ceres_b200_ba_t ba, const double* __restrict__ x,
+                                                              const double* __restrict__ sv, double* __restrict__ part) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  (void)camera_pass<T, double, double, true, false>(ba, x, sv, part, nullptr, gw, nw);
+}
+
+__global__ void k_fold_items(ceres_b200_ba_t ba, const double* __restrict__ part, const double* __restrict__ x,
+                             double* __restrict__ y) {
   const int n = 9 * ba.num_cameras;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    const double v = y[j] + ba.cam_diag[j] * x[j];
-    y[j] = v;
-    if (out_res) out_res[j] = rhs[j] - v;
-  }
+  const int j0 = blockIdx.x * blockDim.x;
+  const int j1 = min(n, j0 + (int)blockDim.x);
+  (void)fold_items(ba, part, x, y, j0, j1, true);
 }
 
 // ======================================================================================
-// Cooperative persistent PCG (linear.py:1216-1256) on the reduced camera system.
+// Cooperative persistent PCG (linear.py:1216-1256) on the reduced camera system, with
+// the float64 refinement of the float32 store in the same launch.
 // ======================================================================================
 struct PcgArgs {
   const double* rhs;   // [n] right-hand side (float64)
-  double* x_out;       // [n] solution (float64); accumulated into when accumulate != 0
-  int accumulate;
+  double* x_out;       // [n] solution (float64)
   int min_iterations, max_iterations;
   double tolerance, eps;
   int n;               // 9 * num_cameras
   int cams_per_cta;
-  int smem_vectors;    // 1: p and y staged in shared memory
-  double* part_y_raw;  // [G][n] T  (smem mode)
+  int smem_vectors;    // 1: a copy of p (in T) in shared memory for the product
+  double* sv;          // [num_points][3] point-pass results s_q
+  double* item_part;   // [num_items][9] camera-pass item sums
   double* part_b;      // [G]
   double* part_c;      // [G][2]
-  double* result;      // [4]: iterations, success, rnorm, rhs_norm
-  const double* norm_ref;  // when set: the tolerance is relative to *norm_ref, not |rhs|
-  const double* gate;      // when set and *gate != 0 (the solve before succeeded): do nothing
-  int stall_window;        // > 0: stop when |r| has not dropped below 0.99 of its best for this many iterations
+  double* r64;         // [n] refinement right-hand side rhs - S x
+  int stall_window;    // > 0: stop when |r| has not dropped below 0.99 of its best for this many iterations
+  int max_refinements; // float32 store: float64 refinement passes after a solve that missed the tolerance
   // SCHUR_POWER_SERIES_EXPANSION (linear.py:59-67, :482-497, :745-756)
   int precond_series;      // z = sum_i (B E)^i B r with B = ba.precond (inverted damped Hbb blocks)
   int init_series;         // x0 = the series applied to rhs with B = init_blocks
@@ -838,73 +888,74 @@ __device__ __forceinline__ void cta_sum_partials(const double* part, int G, int 
   __syncthreads();
 }
 
+// Product kinds of the persistent PCG: S and E in the store's precision T, S in
+// float64 arithmetic (the float32 store's refinement residual)
+enum { kProdS = 0, kProdE = 1, kProdS64 = 2 };
+
 template <typename T>
 __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[2 * (kPcgBlock / 32)];
-  __shared__ double sred[kPcgBlock];
   __shared__ double bcast[4];
   __shared__ int slice_counter;
   const int n = a.n;
   T* ps = reinterpret_cast<T*>(smem_raw);
-  T* ys = ps + ((n + 3) & ~3);
-  // PCG state vectors are float64 in both precisions; the product S p streams the
-  // Jacobian store in T with T accumulation.
+  // PCG state vectors are float64 in both precisions; the products S p and E p stream
+  // the Jacobian store in T with T arithmetic.
   double* __restrict__ X = reinterpret_cast<double*>(ba.pcg_x);
   double* __restrict__ R = reinterpret_cast<double*>(ba.pcg_r);
   double* __restrict__ Z = reinterpret_cast<double*>(ba.pcg_z);
   double* __restrict__ Pbuf = reinterpret_cast<double*>(ba.pcg_p);
   double* __restrict__ AP = reinterpret_cast<double*>(ba.pcg_ap);
   const T* __restrict__ Minv = reinterpret_cast<const T*>(ba.precond);
-  T* part_y = reinterpret_cast<T*>(a.part_y_raw);
-  const GridBarrier gb{&ba.counters[kCtrBarCount], &ba.counters[kCtrBarGen], &ba.counters[kCtrBarFlag]};
+  const GridBarrier gb{&ba.counters[kCtrBarCount], &ba.counters[kCtrBarGen], &ba.counters[kCtrBarFlag], kSpinLimit};
   const int G = gridDim.x;
   const int c0 = blockIdx.x * a.cams_per_cta;
   const int c1 = min(ba.num_cameras, c0 + a.cams_per_cta);
   const int j0 = 9 * c0, j1 = 9 * max(c0, c1);
+  const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (G * blockDim.x) >> 5;
 
-  if (a.gate != nullptr && *a.gate != 0.0) {
-    // refinement after a solve that met its tolerance: nothing to do
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      a.result[0] = 0.0; a.result[1] = 0.0; a.result[2] = 0.0; a.result[3] = 0.0;
+  // point pass of this CTA's slices (the balanced CTA schedule of next_cta_slice) with p
+  // from ps (shared memory, T) or V (global memory, float64)
+  auto point_pass = [&](const double* V, int kind) {
+    if (threadIdx.x == 0) slice_counter = 0;
+    __syncthreads();
+    for (int s = next_cta_slice(&slice_counter, ba.num_slices); s >= 0; s = next_cta_slice(&slice_counter, ba.num_slices)) {
+      if (kind == kProdS64) point_pass_slice<T, double, double, true>(ba, V, a.sv, s, lane);
+      else if (a.smem_vectors) point_pass_slice<T, T, T, false>(ba, ps, a.sv, s, lane);
+      else point_pass_slice<T, double, T, true>(ba, V, a.sv, s, lane);
     }
-    return;
-  }
-  // ---- products over the whole grid. Every CTA calls them; V is complete on all CTAs
-  // (a grid barrier precedes the call). out[j0..j1) = (S V) (kS) or (E V) of this
-  // CTA's cameras; ends after the fold, with the partials read.
-  auto product = [&](const double* V, double* out, bool kS) -> bool {
-    if (a.smem_vectors) {
-      for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        ps[j] = (T)ld_cross(V + j);
-        ys[j] = (T)0;
-      }
-      if (threadIdx.x == 0) slice_counter = 0;
-      __syncthreads();
-      if (kS) matvec_slices_cta<T, T, T, false, false>(ba, ps, ys, &slice_counter);
-      else matvec_slices_cta<T, T, T, false, true>(ba, ps, ys, &slice_counter);
-      __syncthreads();
-      T* my = part_y + (size_t)blockIdx.x * n;
-      for (int j = threadIdx.x; j < n; j += blockDim.x) my[j] = ys[j];
-      if (!grid_sync(gb)) return false;
-      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-        double y = 0.0;
-#pragma unroll 4
-        for (int g = 0; g < G; ++g) y += (double)ld_cross(part_y + (size_t)g * n + j);
-        if (kS) y += ba.cam_diag[j] * ld_cross(V + j);
-        out[j] = y;
-      }
-    } else {
-      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) out[j] = 0.0;
-      if (!grid_sync(gb)) return false;
-      if (kS) matvec_slices<T, double, double, true, false>(ba, V, out, gw, nw);
-      else matvec_slices<T, double, double, true, true>(ba, V, out, gw, nw);
-      if (!grid_sync(gb)) return false;
-      if (kS)
-        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) out[j] = ld_cross(out + j) + ba.cam_diag[j] * ld_cross(V + j);
+  };
+  // camera pass over the grid's warps; returns this thread's share of
+  // sum_items V_c . y_item (when with_dot)
+  auto camera_pass_all = [&](const double* V, int kind, bool with_dot) -> double {
+    const double* dp = with_dot ? V : nullptr;
+    if (kind == kProdS64) return camera_pass<T, double, double, true, false>(ba, V, a.sv, a.item_part, dp, gw, nw);
+    if (kind == kProdE) {
+      if (a.smem_vectors) return camera_pass<T, T, T, false, true>(ba, ps, a.sv, a.item_part, dp, gw, nw);
+      return camera_pass<T, double, T, true, true>(ba, V, a.sv, a.item_part, dp, gw, nw);
     }
+    if (a.smem_vectors) return camera_pass<T, T, T, false, false>(ba, ps, a.sv, a.item_part, dp, gw, nw);
+    return camera_pass<T, double, T, true, false>(ba, V, a.sv, a.item_part, dp, gw, nw);
+  };
+  // p (complete in global memory, read through L2) into shared memory as T
+  auto stage_p = [&](const double* V) {
+    if (a.smem_vectors)
+      for (int j = threadIdx.x; j < n; j += blockDim.x) ps[j] = (T)ld_cross(V + j);
+    __syncthreads();
+  };
+
+  // ---- out[j0..j1) = (S V) (kinds S, S64) or (E V) of this CTA's cameras; V complete in
+  // global memory on entry (a grid barrier precedes the call). Two grid barriers.
+  auto product = [&](const double* V, double* out, int kind) -> bool {
+    if (kind != kProdS64) stage_p(V);
+    point_pass(V, kind);
+    if (!grid_sync(gb)) return false;
+    (void)camera_pass_all(V, kind, false);
+    if (!grid_sync(gb)) return false;
+    (void)fold_items(ba, a.item_part, V, out, j0, j1, kind != kProdE);
     __syncthreads();
     return true;
   };
@@ -917,7 +968,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) term[j] = out[j];
     for (int it = 1; it < a.series_terms; ++it) {
       if (!grid_sync(gb)) return false;
-      if (!product(term, w, false)) return false;
+      if (!product(term, w, kProdE)) return false;
       for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(B, w, term, c);
       __syncthreads();
       double v[2] = {0.0, 0.0};
@@ -938,243 +989,255 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     return true;
   };
 
-  // ---- init: x = x0 (0, or the series applied to rhs), r = rhs - S x0, z = M^-1 r,
-  // p = z (written at the first phase A)
-  {
-    double rz = 0.0, rr = 0.0;
-    if (a.init_series) {
-      if (!series(reinterpret_cast<const T*>(a.init_blocks), a.rhs, X, Pbuf + n, AP)) return;
-      if (!grid_sync(gb)) return;
-      if (!product(X, Z, true)) return;
-      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) R[j] = a.rhs[j] - Z[j];
-    } else {
-      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-        X[j] = 0.0;
-        R[j] = a.rhs[j];
-      }
-    }
-    __syncthreads();
-    if (a.precond_series) {
-      if (!series(Minv, R, Z, Pbuf + n, AP)) return;
-    } else {
-      for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
-    }
-    __syncthreads();
-    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-      const double r = (double)R[j], z = (double)Z[j];
-      rz += r * z;
-      rr += r * r;
-    }
-    double v[2] = {rz, rr};
-    block_reduce<2>(v, 0u, red);
-    if (threadIdx.x == 0) { a.part_c[2 * blockIdx.x] = v[0]; a.part_c[2 * blockIdx.x + 1] = v[1]; }
-  }
-  if (!grid_sync(gb)) return;
-  double rz_old, rr;
-  {
-    double t2[2];
-    cta_sum_partials<2>(a.part_c, G, 2, t2, red, bcast);
-    rz_old = t2[0];
-    rr = t2[1];
-  }
-  // the rhs norm is taken in float64 from the float64 rhs
-  double rhs_norm;
-  {
-    double v[1] = {0.0};
-    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) v[0] += a.rhs[j] * a.rhs[j];
-    block_reduce<1>(v, 0u, red);
-    if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
-    if (!grid_sync(gb)) return;
-    double t[1];
-    cta_sum_partials<1>(a.part_b, G, 1, t, red, bcast);
-    rhs_norm = fmax(a.norm_ref != nullptr ? *a.norm_ref : sqrt(t[0]), a.eps);
-  }
-  int iterations = 0;
-  bool success = false;
-  double rnorm = sqrt(rr);
-  double rbest = rnorm;
-  int last_improvement = 0;
-  double beta = 0.0;
-  int cur = 0;
-  if (!(a.min_iterations <= 0 && rnorm <= a.tolerance * rhs_norm)) {
-    for (int k = 0; k < a.max_iterations; ++k) {
-      // ---- phase A: p = z + beta p_old; y = (J_c^T J_c - H_cp W^-1 H_pc) p
-      const int nxt = k == 0 ? 0 : cur ^ 1;
-      double* Pold = Pbuf + (size_t)cur * n;
-      double* Pnew = Pbuf + (size_t)nxt * n;
-      if (a.smem_vectors) {
-#pragma unroll 4
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
-          const double pv = (k == 0) ? ld_cross(Z + j) : ld_cross(Z + j) + beta * ld_cross(Pold + j);
-          ps[j] = (T)pv;
-          ys[j] = (T)0;
-          if (j >= j0 && j < j1) Pnew[j] = pv;
-        }
-        if (threadIdx.x == 0) slice_counter = 0;
-        __syncthreads();
-        matvec_slices_cta<T, T, T>(ba, ps, ys, &slice_counter);
-        __syncthreads();
-        T* my = part_y + (size_t)blockIdx.x * n;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) my[j] = ys[j];
+  // ---- one PCG solve of S X = b (X, R, Z, P, AP: the state vectors). x0 = 0, or the
+  // series applied to b (init); stop when |r| <= tolerance * max(|b|, eps) (norm_ref in
+  // place of |b| when it is >= 0) after min_it iterations. Returns false when a grid
+  // barrier failed.
+  struct CgOut {
+    int iterations;
+    bool success;
+    double rnorm, rhs_norm;
+  };
+  auto cg = [&](const double* b, bool init, double norm_ref, int min_it, CgOut& o) -> bool {
+    double rz_old, rr;
+    // init: x = x0, r = b - S x0, z = M^-1 r, p = z (written at the first phase A)
+    {
+      double rz = 0.0, rr0 = 0.0;
+      if (init) {
+        if (!series(reinterpret_cast<const T*>(a.init_blocks), b, X, Pbuf + n, AP)) return false;
+        if (!grid_sync(gb)) return false;
+        if (!product(X, Z, kProdS)) return false;
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) R[j] = b[j] - Z[j];
       } else {
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-          Pnew[j] = (k == 0) ? Z[j] : Z[j] + beta * Pold[j];
-          AP[j] = 0.0;
+          X[j] = 0.0;
+          R[j] = b[j];
         }
-        if (!grid_sync(gb)) return;
-        matvec_slices<T, double, double, true>(ba, Pnew, AP, gw, nw);
       }
-      cur = nxt;
-      if (!grid_sync(gb)) return;
-      // ---- phase B: Ap = sum of partials + D p ; partial p.Ap
-      {
-        double v[1] = {0.0};
-        const int m = j1 - j0;
-        const int S = (m > 0 && m <= (int)blockDim.x) ? (int)blockDim.x / m : 1;
-        if (a.smem_vectors && m > 0 && m <= (int)blockDim.x) {
-          // the G partial products of my components, summed by S thread groups in parallel
-          double acc = 0.0;
-          const int t = threadIdx.x;
-          if (t < m * S) {
-            const int jj = j0 + t % m;
-#pragma unroll 4
-            for (int g = t / m; g < G; g += S) acc += (double)ld_cross(part_y + (size_t)g * n + jj);
-          }
-          sred[t] = acc;
-          __syncthreads();
-          if (t < m) {
-            double y = 0.0;
-            for (int s2 = 0; s2 < S; ++s2) y += sred[t + m * s2];
-            const int j = j0 + t;
-            const double pj = Pnew[j];
-            y += ba.cam_diag[j] * pj;
-            AP[j] = y;
-            v[0] += pj * y;
-          }
-        } else {
-          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-            double y = 0.0;
-            if (a.smem_vectors) {
-              for (int g = 0; g < G; ++g) y += (double)ld_cross(part_y + (size_t)g * n + j);
-            } else {
-              y = (double)ld_cross(AP + j);
-            }
-            const double pj = Pnew[j];
-            y += ba.cam_diag[j] * pj;
-            AP[j] = y;
-            v[0] += pj * y;
-          }
-        }
-        block_reduce<1>(v, 0u, red);
-        if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
-      }
-      if (!grid_sync(gb)) return;
-      double denom;
-      {
-        double t1[1];
-        cta_sum_partials<1>(a.part_b, G, 1, t1, red, bcast);
-        denom = t1[0];
-      }
-      if (fabs(denom) <= a.eps) {
-        success = rnorm <= a.tolerance * rhs_norm;
-        break;
-      }
-      const double alpha = rz_old / denom;
+      __syncthreads();
       if (a.precond_series) {
-        // the reference's order: x, r; test |r|; only then z = M^-1 r (a series costs
-        // up to series_terms - 1 products)
-        double v[1] = {0.0};
-        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-          X[j] = X[j] + alpha * Pnew[j];
-          const double rj = R[j] - alpha * AP[j];
-          R[j] = rj;
-          v[0] += rj * rj;
+        if (!series(Minv, R, Z, Pbuf + n, AP)) return false;
+      } else {
+        for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+      }
+      __syncthreads();
+      double bb = 0.0;
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const double r = R[j], z = Z[j];
+        rz += r * z;
+        rr0 += r * r;
+        bb += b[j] * b[j];
+      }
+      // r.z, r.r and the float64 |b|^2 in one grid reduction
+      double v[2] = {rz, rr0};
+      block_reduce<2>(v, 0u, red);
+      double vb[1] = {bb};
+      block_reduce<1>(vb, 0u, red);
+      if (threadIdx.x == 0) {
+        a.part_c[2 * blockIdx.x] = v[0];
+        a.part_c[2 * blockIdx.x + 1] = v[1];
+        a.part_b[blockIdx.x] = vb[0];
+      }
+    }
+    if (!grid_sync(gb)) return false;
+    {
+      double t2[2], t1[1];
+      cta_sum_partials<2>(a.part_c, G, 2, t2, red, bcast);
+      cta_sum_partials<1>(a.part_b, G, 1, t1, red, bcast);
+      rz_old = t2[0];
+      rr = t2[1];
+      o.rhs_norm = fmax(norm_ref >= 0.0 ? norm_ref : sqrt(t1[0]), a.eps);
+    }
+    int iterations = 0;
+    bool success = false;
+    double rnorm = sqrt(rr);
+    double rbest = rnorm;
+    int last_improvement = 0;
+    double beta = 0.0;
+    int cur = 0;
+    if (!(min_it <= 0 && rnorm <= a.tolerance * o.rhs_norm)) {
+      for (int k = 0; k < a.max_iterations; ++k) {
+        // ---- phase A: p = z + beta p_old (all cameras, redundantly per CTA: every CTA's
+        // point pass reads any camera); point pass
+        const int nxt = k == 0 ? 0 : cur ^ 1;
+        double* Pold = Pbuf + (size_t)cur * n;
+        double* Pnew = Pbuf + (size_t)nxt * n;
+        if (a.smem_vectors) {
+#pragma unroll 4
+          for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double pv = (k == 0) ? ld_cross(Z + j) : ld_cross(Z + j) + beta * ld_cross(Pold + j);
+            ps[j] = (T)pv;
+            if (j >= j0 && j < j1) Pnew[j] = pv;
+          }
+          __syncthreads();
+        } else {
+          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) Pnew[j] = (k == 0) ? Z[j] : Z[j] + beta * Pold[j];
+          if (!grid_sync(gb)) return false;
         }
-        block_reduce<1>(v, 0u, red);
-        if (threadIdx.x == 0) a.part_s[2 * blockIdx.x] = v[0];
-        if (!grid_sync(gb)) return;
-        double t[2];
-        cta_sum_partials<1>(a.part_s, G, 2, t, red, bcast);
-        rr = t[0];
+        point_pass(Pnew, kProdS);
+        cur = nxt;
+        if (!grid_sync(gb)) return false;
+        // ---- phase B: camera pass; p.Ap = sum_items p_c . y_item + sum_j D_j p_j^2
+        {
+          double v[1] = {camera_pass_all(Pnew, kProdS, true)};
+          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            const double pj = Pnew[j];
+            v[0] += ba.cam_diag[j] * pj * pj;
+          }
+          block_reduce<1>(v, 0u, red);
+          if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
+        }
+        if (!grid_sync(gb)) return false;
+        double denom;
+        {
+          double t1[1];
+          cta_sum_partials<1>(a.part_b, G, 1, t1, red, bcast);
+          denom = t1[0];
+        }
+        if (fabs(denom) <= a.eps) {
+          success = rnorm <= a.tolerance * o.rhs_norm;
+          break;
+        }
+        const double alpha = rz_old / denom;
+        // Ap of this CTA's cameras: their item sums in item order, plus D p
+        (void)fold_items(ba, a.item_part, Pnew, AP, j0, j1, true);
+        __syncthreads();
+        if (a.precond_series) {
+          // the reference's order: x, r; test |r|; only then z = M^-1 r (a series costs
+          // up to series_terms - 1 products)
+          double v[1] = {0.0};
+          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            X[j] = X[j] + alpha * Pnew[j];
+            const double rj = R[j] - alpha * AP[j];
+            R[j] = rj;
+            v[0] += rj * rj;
+          }
+          block_reduce<1>(v, 0u, red);
+          if (threadIdx.x == 0) a.part_s[2 * blockIdx.x] = v[0];
+          if (!grid_sync(gb)) return false;
+          double t[2];
+          cta_sum_partials<1>(a.part_s, G, 2, t, red, bcast);
+          rr = t[0];
+          rnorm = sqrt(rr);
+          iterations = k + 1;
+          if (iterations >= min_it && rnorm <= a.tolerance * o.rhs_norm) {
+            success = true;
+            break;
+          }
+          if (!series(Minv, R, Z, Pbuf + (size_t)(cur ^ 1) * n, AP)) return false;
+          double v2[1] = {0.0};
+          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) v2[0] += R[j] * Z[j];
+          block_reduce<1>(v2, 0u, red);
+          if (threadIdx.x == 0) a.part_c[2 * blockIdx.x] = v2[0];
+          if (!grid_sync(gb)) return false;
+          double t2[1];
+          cta_sum_partials<1>(a.part_c, G, 2, t2, red, bcast);
+          const double rz_new = t2[0];
+          if (fabs(rz_old) <= a.eps) break;
+          if (a.stall_window > 0) {
+            if (rnorm < 0.99 * rbest) { rbest = rnorm; last_improvement = iterations; }
+            else if (iterations - last_improvement >= a.stall_window) break;
+          }
+          beta = rz_new / rz_old;
+          rz_old = rz_new;
+          continue;
+        }
+        // ---- phase C: x += alpha p ; r -= alpha Ap ; z = M^-1 r ; partial r.z, r.r
+        {
+          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            X[j] = X[j] + alpha * Pnew[j];
+            R[j] = R[j] - alpha * AP[j];
+          }
+          __syncthreads();
+          for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+          __syncthreads();
+          double v[2] = {0.0, 0.0};
+          for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            const double r = R[j];
+            v[0] += r * Z[j];
+            v[1] += r * r;
+          }
+          block_reduce<2>(v, 0u, red);
+          if (threadIdx.x == 0) { a.part_c[2 * blockIdx.x] = v[0]; a.part_c[2 * blockIdx.x + 1] = v[1]; }
+        }
+        if (!grid_sync(gb)) return false;
+        double rz_new;
+        {
+          double t2[2];
+          cta_sum_partials<2>(a.part_c, G, 2, t2, red, bcast);
+          rz_new = t2[0];
+          rr = t2[1];
+        }
         rnorm = sqrt(rr);
         iterations = k + 1;
-        if (iterations >= a.min_iterations && rnorm <= a.tolerance * rhs_norm) {
+        if (iterations >= min_it && rnorm <= a.tolerance * o.rhs_norm) {
           success = true;
           break;
         }
-        if (!series(Minv, R, Z, Pbuf + (size_t)(cur ^ 1) * n, AP)) return;
-        double v2[1] = {0.0};
-        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) v2[0] += R[j] * Z[j];
-        block_reduce<1>(v2, 0u, red);
-        if (threadIdx.x == 0) a.part_c[2 * blockIdx.x] = v2[0];
-        if (!grid_sync(gb)) return;
-        double t2[1];
-        cta_sum_partials<1>(a.part_c, G, 2, t2, red, bcast);
-        const double rz_new = t2[0];
         if (fabs(rz_old) <= a.eps) break;
         if (a.stall_window > 0) {
+          // float32 products: the recurrence residual stops shrinking at the rounding floor;
+          // the float64 refinement then judges the iterate by its true residual
           if (rnorm < 0.99 * rbest) { rbest = rnorm; last_improvement = iterations; }
           else if (iterations - last_improvement >= a.stall_window) break;
         }
         beta = rz_new / rz_old;
         rz_old = rz_new;
-        continue;
       }
-      // ---- phase C: x += alpha p ; r -= alpha Ap ; z = M^-1 r ; partial r.z, r.r
-      {
-        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-          X[j] = X[j] + alpha * Pnew[j];
-          R[j] = R[j] - alpha * AP[j];
-        }
-        __syncthreads();
-        for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
-        __syncthreads();
-        double v[2] = {0.0, 0.0};
-        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-          const double r = (double)R[j];
-          v[0] += r * (double)Z[j];
-          v[1] += r * r;
-        }
-        block_reduce<2>(v, 0u, red);
-        if (threadIdx.x == 0) { a.part_c[2 * blockIdx.x] = v[0]; a.part_c[2 * blockIdx.x + 1] = v[1]; }
-      }
-      if (!grid_sync(gb)) return;
-      double rz_new;
-      {
-        double t2[2];
-        cta_sum_partials<2>(a.part_c, G, 2, t2, red, bcast);
-        rz_new = t2[0];
-        rr = t2[1];
-      }
-      rnorm = sqrt(rr);
-      iterations = k + 1;
-      if (iterations >= a.min_iterations && rnorm <= a.tolerance * rhs_norm) {
-        success = true;
-        break;
-      }
-      if (fabs(rz_old) <= a.eps) break;
-      if (a.stall_window > 0) {
-        // float32 products: the recurrence residual stops shrinking at the rounding floor;
-        // the float64 refinement pass then judges the iterate by its true residual
-        if (rnorm < 0.99 * rbest) { rbest = rnorm; last_improvement = iterations; }
-        else if (iterations - last_improvement >= a.stall_window) break;
-      }
-      beta = rz_new / rz_old;
-      rz_old = rz_new;
+    } else {
+      success = true;
     }
-  } else {
-    success = true;
-  }
-  // ---- output
-  for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-    const double xv = (double)X[j];
-    a.x_out[j] = a.accumulate ? a.x_out[j] + xv : xv;
+    o.iterations = iterations;
+    o.success = success;
+    o.rnorm = rnorm;
+    return true;
+  };
+
+  // The solve, then (float32 store) the float64 refinement: r64 = rhs - S x with float64
+  // arithmetic; while |r64| is above the tolerance (relative to the original |rhs|),
+  // solve S dx = r64 in float32 from zero (no series start point) and add dx. With
+  // eta-size tolerances the first solve normally meets the tolerance and no refinement
+  // runs; it matters when the float32 recurrence stalled at its rounding floor. One call
+  // site of cg, so that it is inlined.
+  CgOut o0{0, false, 0.0, 0.0};
+  int refine_iterations = 0;
+  double refine_rnorm = -1.0;
+  const bool refine = sizeof(T) == sizeof(float) && a.max_refinements > 0;
+  for (int pass = 0;; ++pass) {
+    CgOut oc;
+    if (!cg(pass == 0 ? a.rhs : a.r64, pass == 0 && a.init_series != 0, pass == 0 ? -1.0 : o0.rhs_norm,
+            pass == 0 ? a.min_iterations : 0, oc))
+      return;
+    if (pass == 0) {
+      o0 = oc;
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) a.x_out[j] = X[j];
+      if (!refine || o0.success) break;
+    } else {
+      refine_iterations += oc.iterations;
+      for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) a.x_out[j] += X[j];
+    }
+    if (!grid_sync(gb)) return;  // x_out complete
+    if (!product(a.x_out, AP, kProdS64)) return;
+    double v[1] = {0.0};
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+      const double r = a.rhs[j] - AP[j];
+      a.r64[j] = r;
+      v[0] += r * r;
+    }
+    block_reduce<1>(v, 0u, red);
+    if (threadIdx.x == 0) a.part_b[blockIdx.x] = v[0];
+    if (!grid_sync(gb)) return;
+    double t1[1];
+    cta_sum_partials<1>(a.part_b, G, 1, t1, red, bcast);
+    refine_rnorm = sqrt(t1[0]);
+    if (pass == a.max_refinements || refine_rnorm <= a.tolerance * o0.rhs_norm) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.result[0] = (double)iterations;
-    a.result[1] = success ? 1.0 : 0.0;
-    a.result[2] = rnorm;
-    a.result[3] = rhs_norm;
+    ba.stats[CERES_B200_STAT_PCG_ITERS] = (double)(o0.iterations + refine_iterations);
+    ba.stats[CERES_B200_STAT_PCG_SUCCESS] = o0.success ? 1.0 : 0.0;
+    ba.stats[CERES_B200_STAT_PCG_RNORM] = o0.rnorm;
+    ba.stats[CERES_B200_STAT_RHS_NORM] = o0.rhs_norm;
+    ba.stats[CERES_B200_STAT_REFINE_RNORM] = refine_rnorm;
   }
 }
 
@@ -1324,38 +1387,12 @@ __global__ void __launch_bounds__(kWarpBlock, CERES_B200_STEP_MIN_BLOCKS) k_step
   // afterwards (k_add_nonfinite)
 }
 
-__global__ void k_zero_gated(double* __restrict__ y, int n, const double* gate) {
-  if (gate != nullptr && *gate != 0.0) return;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) y[j] = 0.0;
-}
-
-__global__ void k_norm_into(const double* __restrict__ v, int n, double* out, const double* gate) {
-  if (gate != nullptr && *gate != 0.0) return;
-  __shared__ double red[8];
-  double a[1] = {0.0};
-  for (int j = threadIdx.x; j < n; j += blockDim.x) a[0] += v[j] * v[j];
-  block_reduce<1>(a, 0u, red);
-  if (threadIdx.x == 0) *out = sqrt(a[0]);
-}
-
 __global__ void k_add_nonfinite(double* stats, const double* cam_nonfinite) {
   stats[CERES_B200_STAT_NONFINITE] += *cam_nonfinite;
 }
 
 __global__ void k_copy_error(ceres_b200_ba_t ba) {
   ba.stats[CERES_B200_STAT_ERROR] = (double)(ba.counters[kCtrError] | ba.counters[kCtrBarFlag]);
-}
-
-__global__ void k_add_refinement(ceres_b200_ba_t ba, const double* rref) {
-  ba.stats[CERES_B200_STAT_PCG_ITERS] += rref[0];
-}
-
-__global__ void k_copy_result(ceres_b200_ba_t ba, const double* result, double refine_rnorm) {
-  ba.stats[CERES_B200_STAT_PCG_ITERS] = result[0];
-  ba.stats[CERES_B200_STAT_PCG_SUCCESS] = result[1];
-  ba.stats[CERES_B200_STAT_PCG_RNORM] = result[2];
-  ba.stats[CERES_B200_STAT_RHS_NORM] = result[3];
-  ba.stats[CERES_B200_STAT_REFINE_RNORM] = refine_rnorm;
 }
 
 // ======================================================================================
@@ -1521,6 +1558,42 @@ __global__ void __launch_bounds__(1024) k_tri_solve(const double* __restrict__ L
   }
 }
 
+// Column j (= row j: the inverse is symmetric) of (L L^T)^-1 from the Cholesky factor L
+// in the lower triangle of Lm, one CTA per column: L y = e_j (entries above j stay 0),
+// then L^T x = y. The camera covariance of the reduced camera system.
+__global__ void __launch_bounds__(256) k_chol_inverse(const double* __restrict__ Lm, int n, double* __restrict__ out) {
+  __shared__ double yj;
+  __shared__ double red[8];
+  const int col = blockIdx.x;
+  double* x = out + (size_t)col * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (i == col) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int j = col; j < n; ++j) {
+    if (threadIdx.x == 0) {
+      yj = x[j] / Lm[(size_t)j * n + j];
+      x[j] = yj;
+    }
+    __syncthreads();
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) x[i] -= Lm[(size_t)i * n + j] * yj;
+    __syncthreads();
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    double v[1] = {0.0};
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) v[0] += Lm[(size_t)i * n + j] * x[i];
+    block_reduce<1>(v, 0u, red);
+    if (threadIdx.x == 0) x[j] = (x[j] - v[0]) / Lm[(size_t)j * n + j];
+    __syncthreads();
+  }
+}
+
+// Bounded-wait check: two CTAs meet at a grid barrier (the barrier of the persistent
+// PCG), except that CTA absent_cta returns at once. The waiting CTA gives up after
+// gb.limit polls, records CERES_B200_DEVERR_BARRIER in *gb.flag and returns.
+__global__ void k_barrier_probe(GridBarrier gb, int absent_cta) {
+  if ((int)blockIdx.x == absent_cta) return;
+  (void)grid_sync(gb);
+}
+
 // ======================================================================================
 // C ABI
 // ======================================================================================
@@ -1538,6 +1611,12 @@ bool valid(const ceres_b200_ba_t* ba) {
   if (ba->num_cameras > 0 && (!ba->cam_offsets || !ba->cam_const || !ba->cam_diag || !ba->rhs || !ba->precond))
     return false;
   if ((reinterpret_cast<uintptr_t>(ba->jac) & 31) != 0) return false;  // 256-bit record loads
+  if (ba->num_observations > 0) {
+    if (!ba->slot_pos || !ba->cm_jac || !ba->cam_entries || !ba->cam_items || !ba->items || ba->num_items <= 0)
+      return false;
+    if ((reinterpret_cast<uintptr_t>(ba->cm_jac) & 31) != 0) return false;
+  }
+  if (ba->num_items < 0) return false;
   return true;
 }
 
@@ -1555,19 +1634,21 @@ struct PcgLayout {
   int cams_per_cta = 0;
   int smem_vectors = 0;
   size_t dyn_smem = 0;
-  size_t frames = 0, aux = 0, cam_acc = 0, part_y = 0, part_b = 0, part_c = 0, result = 0, x64 = 0, r64 = 0,
-         spse_base = 0, part_s = 0, slice_part = 0, total = 0;
+  size_t frames = 0, aux = 0, cam_acc = 0, sv = 0, item_part = 0, part_b = 0, part_c = 0, r64 = 0, spse_base = 0,
+         part_s = 0, slice_part = 0, total = 0;
 };
 
 template <typename T>
 int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   const DevInfo d = device_info();
   const int n = 9 * ba.num_cameras;
-  const size_t vec_bytes = (size_t)((n + 3) & ~3) * sizeof(T);
-  const size_t static_smem = 2 * (kPcgBlock / 32) * sizeof(double) + 64;
-  L.smem_vectors = (2 * vec_bytes + static_smem <= (size_t)d.max_smem_optin - 1024) ? 1 : 0;
-  L.dyn_smem = L.smem_vectors ? 2 * vec_bytes : 0;
   auto kern = k_pcg<T>;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return CERES_B200_ECUDA;
+  // shared memory: a copy of p in T for the products' camera gathers
+  const size_t vec_bytes = ((size_t)n * sizeof(T) + 15) & ~(size_t)15;
+  L.smem_vectors = (vec_bytes + fa.sharedSizeBytes + 1024 <= (size_t)d.max_smem_optin) ? 1 : 0;
+  L.dyn_smem = L.smem_vectors ? vec_bytes : 0;
   if (L.dyn_smem > 48 * 1024) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.dyn_smem) != cudaSuccess)
       return CERES_B200_ESMEM;
@@ -1587,20 +1668,17 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   off += 256;
   L.cam_acc = off;
   off += ((size_t)(ba.num_cameras > 0 ? ba.num_cameras : 1) * kCamAcc * sizeof(double) + 255) & ~(size_t)255;
-  L.part_y = off;
-  off += L.smem_vectors ? (size_t)L.grid * n * sizeof(T) : 0;
-  off = (off + 255) & ~(size_t)255;
+  L.sv = off;
+  off += ((size_t)(ba.num_points > 0 ? ba.num_points : 1) * 3 * sizeof(double) + 255) & ~(size_t)255;
+  L.item_part = off;
+  off += ((size_t)(ba.num_items > 0 ? ba.num_items : 1) * 9 * sizeof(double) + 255) & ~(size_t)255;
   L.part_b = off;
   off += (size_t)L.grid * sizeof(double);
   L.part_c = off;
   off += (size_t)L.grid * 2 * sizeof(double);
   L.part_s = off;
   off += (size_t)L.grid * 2 * sizeof(double);
-  L.result = off;
-  off += 8 * sizeof(double);
   off = (off + 255) & ~(size_t)255;
-  L.x64 = off;
-  off += (size_t)n * sizeof(double);
   L.r64 = off;
   off += (size_t)n * sizeof(double);
   off = (off + 255) & ~(size_t)255;
@@ -1626,9 +1704,8 @@ struct SeriesOpts {
 };
 
 template <typename T>
-int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int accumulate, int min_it, int max_it,
-               double tol, cudaStream_t st, const PcgLayout& L, char* scratch, double* result, const double* norm_ref,
-               const double* gate, int stall_window, const SeriesOpts& so = SeriesOpts()) {
+int launch_pcg(const ceres_b200_ba_t& ba, int min_it, int max_it, double tol, int max_ref, cudaStream_t st,
+               const PcgLayout& L, char* scratch, const SeriesOpts& so) {
   PcgArgs a;
   a.precond_series = so.precond;
   a.init_series = so.init;
@@ -1636,9 +1713,8 @@ int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int 
   a.series_terms = so.terms;
   a.series_tol = so.tol;
   a.part_s = reinterpret_cast<double*>(scratch + L.part_s);
-  a.rhs = rhs;
-  a.x_out = x_out;
-  a.accumulate = accumulate;
+  a.rhs = ba.rhs;
+  a.x_out = ba.step_cameras;
   a.min_iterations = min_it;
   a.max_iterations = max_it;
   a.tolerance = tol;
@@ -1646,13 +1722,15 @@ int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int 
   a.n = 9 * ba.num_cameras;
   a.cams_per_cta = L.cams_per_cta;
   a.smem_vectors = L.smem_vectors;
-  a.part_y_raw = reinterpret_cast<double*>(scratch + L.part_y);
+  a.sv = reinterpret_cast<double*>(scratch + L.sv);
+  a.item_part = reinterpret_cast<double*>(scratch + L.item_part);
   a.part_b = reinterpret_cast<double*>(scratch + L.part_b);
   a.part_c = reinterpret_cast<double*>(scratch + L.part_c);
-  a.result = result;
-  a.norm_ref = norm_ref;
-  a.gate = gate;
-  a.stall_window = stall_window;
+  a.r64 = reinterpret_cast<double*>(scratch + L.r64);
+  // float32 store: float64 refinement passes inside the launch, and the float32
+  // recurrence stops at its rounding floor so that the refinement can take over
+  a.max_refinements = sizeof(T) == sizeof(float) ? max_ref : 0;
+  a.stall_window = a.max_refinements > 0 ? kStallWindow : 0;
   // barrier words start at zero for every launch
   CB_TRACE("pcg: memset barrier words");
   if (cudaMemsetAsync(&ba.counters[kCtrBarCount], 0, 3 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
@@ -1671,22 +1749,32 @@ int launch_pcg(const ceres_b200_ba_t& ba, const double* rhs, double* x_out, int 
   return CERES_B200_OK;
 }
 
-// y = S x (float64 accumulation; the Jacobian is read in its stored precision T).
-// When rhs and res are given, res = rhs - y as well.
-// ``gate``: when set and *gate != 0 every kernel returns at once (y is then stale).
+// y = S x in float64 arithmetic from the stored Jacobian (precision T): the point pass,
+// the camera pass and the fold of the persistent PCG as three launches. The y = S x
+// test entry point.
 template <typename T>
-int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, const double* rhs, double* res, cudaStream_t st,
-             const double* gate = nullptr) {
+int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, cudaStream_t st) {
   const DevInfo d = device_info();
   const int n = 9 * ba.num_cameras;
-  count_launch();
-  k_zero_gated<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(y, n, gate);
+  PcgLayout L;
+  int rc = pcg_layout<T>(ba, L);
+  if (rc) return rc;
+  if (!ba.scratch || (size_t)ba.scratch_bytes < L.total) return CERES_B200_EINVAL;
+  char* scratch = reinterpret_cast<char*>(ba.scratch);
+  double* sv = reinterpret_cast<double*>(scratch + L.sv);
+  double* part = reinterpret_cast<double*>(scratch + L.item_part);
   if (ba.num_slices > 0) {
     count_launch();
-    k_matvec_points<T><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, x, y, gate);
+    k_point_pass64<T><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, x, sv);
+  }
+  if (ba.num_items > 0) {
+    int g = (ba.num_items * 32 + kWarpBlock - 1) / kWarpBlock;
+    if (g > 8 * d.sms) g = 8 * d.sms;
+    count_launch();
+    k_camera_pass64<T><<<g, kWarpBlock, 0, st>>>(ba, x, sv, part);
   }
   count_launch();
-  k_matvec_diag<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(ba, x, y, rhs, res, gate);
+  k_fold_items<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(ba, part, x, y);
   return check_launch();
 }
 
@@ -1731,47 +1819,14 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
   char* scratch = reinterpret_cast<char*>(ba.scratch);
   const int n = 9 * ba.num_cameras;
   if (n == 0) return CERES_B200_OK;
-  double* result = reinterpret_cast<double*>(scratch + L.result);
-  const bool refine = max_ref > 0 && sizeof(T) == sizeof(float);
-  const int stall = refine ? kStallWindow : 0;
   SeriesOpts so;
   so.precond = precond == CERES_B200_PRECOND_SCHUR_POWER_SERIES ? 1 : 0;
   so.terms = series_terms;
   so.tol = series_tol;
   so.init = series_init ? 1 : 0;
   so.init_blocks = so.precond ? ba.precond : static_cast<const void*>(scratch + L.spse_base);
-  SeriesOpts so_ref = so;  // refinement passes solve for a correction from zero
-  so_ref.init = 0;
-  rc = launch_pcg<T>(ba, ba.rhs, ba.step_cameras, 0, min_it, max_it, tol, st, L, scratch, result, nullptr, nullptr,
-                     stall, so);
+  rc = launch_pcg<T>(ba, min_it, max_it, tol, max_ref, st, L, scratch, so);
   if (rc) return rc;
-  count_launch();
-  k_copy_result<<<1, 1, 0, st>>>(ba, result, -1.0);
-  if (refine) {
-    // float64 refinement: res = rhs - S x with float64 accumulation; while |res| is above
-    // the tolerance (relative to the original |rhs|), solve S dx = res in float32 and add
-    // dx. With eta-size tolerances this normally takes 0 iterations; it matters when the
-    // float32 recurrence stalled at its rounding floor.
-    double* y64 = reinterpret_cast<double*>(scratch + L.x64);
-    double* r64 = reinterpret_cast<double*>(scratch + L.r64);
-    double* rref = result + 4;
-    // every refinement kernel is gated on the float32 solve's success flag: when it met
-    // the tolerance the refinement launches return at once
-    const double* gate = result + 1;
-    for (int it = 0; it < max_ref; ++it) {
-      rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st, gate);
-      if (rc) return rc;
-      rc = launch_pcg<T>(ba, r64, ba.step_cameras, 1, 0, max_it, tol, st, L, scratch, rref, result + 3, gate,
-                         stall, so_ref);
-      if (rc) return rc;
-      count_launch();
-      k_add_refinement<<<1, 1, 0, st>>>(ba, rref);
-    }
-    rc = matvec64<T>(ba, ba.step_cameras, y64, ba.rhs, r64, st, gate);
-    if (rc) return rc;
-    count_launch();
-    k_norm_into<<<1, 256, 0, st>>>(r64, n, ba.stats + CERES_B200_STAT_REFINE_RNORM, gate);
-  }
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(ba);
   return check_launch();
@@ -1840,18 +1895,51 @@ namespace {
 constexpr int kNoAllocPartials = 32768;  // float64 slots: one per evaluation CTA
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocPartials];
 
-// Device address of g_noalloc_partials, looked up once per device. In host code the
-// symbol's name is only a host-side stand-in, so kernels are given this address.
+// Identity of the calling thread's current CUDA context (0 when it cannot be read),
+// through the driver entry points the runtime hands out, so the library needs no link
+// against the driver library.
+unsigned long long current_context_id() {
+  typedef CUresult (*GetCurrentFn)(CUcontext*);
+  typedef CUresult (*GetIdFn)(CUcontext, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q2 == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<GetCurrentFn>(f1);
+      get_id = reinterpret_cast<GetIdFn>(f2);
+    }
+    looked_up = true;
+  }
+  if (!get_current || !get_id) return 0ull;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0ull;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr || get_id(ctx, &id) != CUDA_SUCCESS) return 0ull;
+  return id;
+}
+
+// Device address of g_noalloc_partials, looked up with the device current the first
+// time a context of that device calls (the symbol's host-side name is only a stand-in,
+// so kernels are given this address). The cache remembers the context it was taken in:
+// after a device reset the device gets a new context, the module is loaded again and
+// the address is looked up again.
 double* noalloc_partials(int device, int* rc) {
   static std::mutex mu;
   static double* addr[64] = {nullptr};
+  static unsigned long long ctx_of[64] = {0ull};
   *rc = CERES_B200_OK;
   if (device < 0 || device >= 64) {
     *rc = CERES_B200_EINVAL;
     return nullptr;
   }
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(mu);
-  if (addr[device] == nullptr) {
+  if (addr[device] == nullptr || ctx == 0ull || ctx_of[device] != ctx) {
     void* ptr = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
     if (e != cudaSuccess || ptr == nullptr) {
@@ -1861,6 +1949,7 @@ double* noalloc_partials(int device, int* rc) {
       return nullptr;
     }
     addr[device] = static_cast<double*>(ptr);
+    ctx_of[device] = ctx;
   }
   return addr[device];
 }
@@ -1976,8 +2065,8 @@ int ceres_b200_ba_schur_matvec(const ceres_b200_ba_t* ba, const double* x, doubl
   cudaStream_t st = (cudaStream_t)stream;
   const int n = 9 * ba->num_cameras;
   if (n == 0) return CERES_B200_OK;
-  if (ba->precision == CERES_B200_FP32) return matvec64<float>(*ba, x, y, nullptr, nullptr, st);
-  return matvec64<double>(*ba, x, y, nullptr, nullptr, st);
+  if (ba->precision == CERES_B200_FP32) return matvec64<float>(*ba, x, y, st);
+  return matvec64<double>(*ba, x, y, st);
 }
 
 int ceres_b200_ba_step(const ceres_b200_ba_t* ba, void* stream) {
@@ -2105,6 +2194,57 @@ int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, voi
   }
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
+  return check_launch();
+}
+
+int ceres_b200_debug_barrier_timeout(uint32_t* words, uint32_t spin_limit, void* stream) {
+  if (!words || spin_limit == 0u) return CERES_B200_EINVAL;
+  GridBarrier gb{words, words + 1, words + 2};
+  gb.limit = spin_limit < kSpinLimit ? spin_limit : kSpinLimit;
+  count_launch();
+  k_barrier_probe<<<2, 32, 0, (cudaStream_t)stream>>>(gb, 1);
+  return check_launch();
+}
+
+int ceres_b200_ba_schur_matrix(const ceres_b200_ba_t* ba, double* S, void* stream) {
+  if (!valid(ba) || (ba->num_cameras > 0 && !S)) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = 9 * ba->num_cameras;
+  if (n == 0) return CERES_B200_OK;
+  const DevInfo d = device_info();
+  if (cudaMemsetAsync(S, 0, (size_t)n * n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
+  if (ba->num_slices > 0) {
+    count_launch();
+    if (ba->precision == CERES_B200_FP32)
+      k_schur_explicit<float><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, S, n);
+    else
+      k_schur_explicit<double><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, S, n);
+  }
+  count_launch();
+  k_dense_diag<<<(n + 255) / 256, 256, 0, st>>>(*ba, S, n);
+  return check_launch();
+}
+
+int ceres_b200_dense_spd_inverse(double* A, double* inv, int64_t n64, uint32_t* flags, void* stream) {
+  if (!A || !inv || !flags || n64 < 0 || n64 > (1 << 15)) return CERES_B200_EINVAL;
+  const int n = (int)n64;
+  if (n == 0) return CERES_B200_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevInfo d = device_info();
+  if (cudaMemsetAsync(flags, 0, 3 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_chol_global, 512, 0) != cudaSuccess || per_sm < 1)
+    return CERES_B200_ECOOP;
+  GridBarrier gb{flags, flags + 1, flags + 2};
+  unsigned* errp = flags + 3;
+  int nn = n;
+  void* args[] = {&A, &nn, &gb, &errp};
+  count_launch();
+  if (cudaLaunchCooperativeKernel((const void*)k_chol_global, dim3(d.sms * per_sm), dim3(512), args, 0, st) !=
+      cudaSuccess)
+    return CERES_B200_ECOOP;
+  count_launch();
+  k_chol_inverse<<<n, 256, 0, st>>>(A, n, inv);
   return check_launch();
 }
 

@@ -53,6 +53,10 @@ class Layout:
     cam_entries: torch.Tensor     # int32 [no, 2]  (slot, q)
     lane_point: torch.Tensor      # int64 [32 S]  original point id of each lane, -1 padding
     point_order: torch.Tensor     # int64 [np]   q -> point id for q < np
+    slot_pos: torch.Tensor        # int32 [slots] camera-major position of the slot, -1 padding
+    cam_items: torch.Tensor       # int32 [nc+1] first camera work item of each camera
+    items: torch.Tensor           # int32 [items, 2] (camera, first entry)
+    max_camera_obs: int = 0
 
 
 def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observations: torch.Tensor,
@@ -103,6 +107,7 @@ def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observat
     if no:
         pk = torch.sort(pi * max(num_cameras, 1) + ci).values
         has_dup = bool((pk[1:] == pk[:-1]).any()) if no > 1 else False
+    slot_pos, cam_items, items, max_cam = camera_items(cam_entries if no else cam_entries[:0], cam_counts, num_slots)
     return Layout(
         num_slices=num_slices, num_slots=num_slots,
         max_slice_len=int(slice_len.max()) if num_slices else 0,
@@ -110,8 +115,35 @@ def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observat
         slice_base=slice_base.to(torch.int32).contiguous(), slice_len=slice_len.to(torch.int32).contiguous(),
         slot_cam=slot_cam, slot_obs=slot_obs, slot_of_obs=slot,
         cam_offsets=cam_offsets.to(torch.int32), cam_entries=cam_entries if no else torch.zeros((1, 2), dtype=torch.int32, device=dev),
-        lane_point=lane_point, point_order=order,
+        lane_point=lane_point, point_order=order, slot_pos=slot_pos, cam_items=cam_items, items=items,
+        max_camera_obs=max_cam,
     )
+
+
+def camera_items(cam_entries: torch.Tensor, cam_counts: torch.Tensor, num_slots: int):
+    """The camera-major position of every slot (inverse of cam_entries' slot column,
+    -1 for padding) and the camera work items: each camera's entries cut into runs of
+    at most CAM_ITEM (include/ceres_b200.h). Returns (slot_pos, cam_items, items,
+    largest camera entry count)."""
+    dev = cam_counts.device
+    no = int(cam_entries.shape[0])
+    nc = int(cam_counts.numel())
+    slot_pos = torch.full((max(num_slots, 1),), -1, dtype=torch.int32, device=dev)
+    if no:
+        slot_pos[cam_entries[:, 0].long()] = torch.arange(no, dtype=torch.int32, device=dev)
+    per_cam = (cam_counts + _lib.CAM_ITEM - 1) // _lib.CAM_ITEM
+    cam_items = torch.zeros(nc + 1, dtype=torch.int64, device=dev)
+    cam_items[1:] = torch.cumsum(per_cam, 0)
+    n_items = int(cam_items[-1]) if nc else 0
+    if n_items:
+        item_cam = torch.repeat_interleave(torch.arange(nc, device=dev), per_cam)
+        start = torch.cumsum(cam_counts, 0) - cam_counts
+        first = start[item_cam] + _lib.CAM_ITEM * (torch.arange(n_items, device=dev) - cam_items[item_cam])
+        items = torch.stack([item_cam, first], dim=1).to(torch.int32).contiguous()
+    else:
+        items = torch.zeros((1, 2), dtype=torch.int32, device=dev)
+    max_cam = int(cam_counts.max()) if nc else 0
+    return slot_pos, cam_items.to(torch.int32).contiguous(), items, max_cam
 
 
 class BAEngine:
@@ -170,6 +202,7 @@ class BAEngine:
         self.cand_points = torch.zeros((npq, 3), **f64)
         self.best_points = torch.zeros((npq, 3), **f64)
         self.jac = torch.zeros((nslot, 24), dtype=T, device=dev)
+        self.cm_jac = torch.zeros((max(self.no, 1), 24), dtype=T, device=dev)
         self.res = torch.zeros((nslot, 2), **f64)
         self.point_raw = torch.zeros((npq, 9), **f64)
         self.winv = torch.zeros((npq, 6), dtype=T, device=dev)
@@ -197,6 +230,9 @@ class BAEngine:
         s.cam_offsets, s.cam_entries = _ptr(L.cam_offsets), _ptr(L.cam_entries)
         s.cam_const, s.pt_const = _ptr(self.cam_const), _ptr(self.pt_const)
         s.jac, s.res = _ptr(self.jac), _ptr(self.res)
+        s.slot_pos, s.cm_jac = _ptr(L.slot_pos), _ptr(self.cm_jac)
+        s.cam_items, s.items = _ptr(L.cam_items), _ptr(L.items)
+        s.num_items, s.max_camera_obs = int(L.cam_items[-1]) if self.nc else 0, int(L.max_camera_obs)
         s.point_raw = _ptr(self.point_raw)
         s.winv, s.winv_ga, s.step_points = _ptr(self.winv), _ptr(self.winv_ga), _ptr(self.step_points)
         s.cam_diag, s.precond, s.rhs, s.step_cameras = (_ptr(self.cam_diag), _ptr(self.precond), _ptr(self.rhs),

@@ -165,9 +165,33 @@ class LossFunctionWrapper(LossFunction):
         return (self.rho or TrivialLoss()).device_spec()
 
 
+_BY_NAME = {"TrivialLoss": TrivialLoss, "HuberLoss": HuberLoss, "SoftLOneLoss": SoftLOneLoss, "CauchyLoss": CauchyLoss,
+            "ArctanLoss": ArctanLoss, "TolerantLoss": TolerantLoss, "TukeyLoss": TukeyLoss}
+
+
+def as_loss(loss) -> Optional[LossFunction]:
+    """This module's loss for ``loss``, which may be a loss object of ceres-torch itself
+    (losses.py:13-146: the same class names and fields); None stays None."""
+    if loss is None or isinstance(loss, LossFunction):
+        return loss
+    kind = type(loss).__name__
+    if kind in _BY_NAME:
+        cls = _BY_NAME[kind]
+        return cls() if kind == "TrivialLoss" else cls(*(float(getattr(loss, f)) for f in ("a", "b")
+                                                          if hasattr(loss, f)))
+    if kind == "ScaledLoss":
+        return ScaledLoss(as_loss(loss.rho), float(loss.scale))
+    if kind == "ComposedLoss":
+        return ComposedLoss(as_loss(loss.outer), as_loss(loss.inner))
+    if kind == "LossFunctionWrapper":
+        return LossFunctionWrapper(as_loss(loss.rho))
+    raise NotImplementedError(f"{kind} has no CUDA evaluator")
+
+
 def device_loss(loss: Optional[LossFunction]) -> dict:
-    """Fields of ceres_b200_ba_t describing ``loss`` (None = trivial)."""
-    loss = loss or TrivialLoss()
+    """Fields of ceres_b200_ba_t describing ``loss`` (None = trivial; ceres-torch's own
+    loss objects are accepted)."""
+    loss = as_loss(loss) or TrivialLoss()
     if isinstance(loss, LossFunctionWrapper):
         loss = loss.rho or TrivialLoss()
     scale = 1.0

@@ -22,7 +22,7 @@ from typing import Optional, Sequence
 import numpy as np
 import torch
 
-from .losses import LossFunction, device_loss
+from .losses import LossFunction, as_loss, device_loss
 
 
 # ------------------------------------------------------------------------------------
@@ -361,6 +361,16 @@ class ExtractedBA:
     point_blocks: list
 
 
+def snavely_cost(cost_function) -> "SnavelyReprojectionError | None":
+    """The SnavelyReprojectionError behind a residual block's cost function: the object
+    itself, or the one ceres-torch's Problem wrapped when it was added there
+    (``CallableCostFunction(functor)``, problem.py:167-168 / costs.py:50-62)."""
+    if isinstance(cost_function, SnavelyReprojectionError):
+        return cost_function
+    inner = getattr(cost_function, "functor", None)
+    return inner if isinstance(inner, SnavelyReprojectionError) else None
+
+
 def extract_bundle_adjustment(problem: Problem) -> ExtractedBA:
     """Recognise ``problem`` as Snavely bundle adjustment or raise NotImplementedError."""
     if not problem.residual_blocks:
@@ -375,7 +385,8 @@ def extract_bundle_adjustment(problem: Problem) -> ExtractedBA:
     loss0 = problem.residual_blocks[0].loss_function
     spec0 = device_loss(loss0)
     for rb in problem.residual_blocks:
-        if not isinstance(rb.cost_function, SnavelyReprojectionError) or len(rb.parameter_blocks) != 2:
+        cost = snavely_cost(rb.cost_function)
+        if cost is None or len(rb.parameter_blocks) != 2:
             raise NotImplementedError(
                 "the GPU path solves bundle-adjustment problems whose residual blocks are all "
                 f"SnavelyReprojectionError; found {type(rb.cost_function).__name__}")
@@ -389,7 +400,7 @@ def extract_bundle_adjustment(problem: Problem) -> ExtractedBA:
         pi.append(id(pb))
         if id(pb) not in pt_of:
             pt_of[id(pb)] = -1
-        obs.append(rb.cost_function.observed)
+        obs.append(cost.observed)
     # camera / point numbering follows the problem's parameter-block order
     for b in problem.parameter_blocks:
         if id(b) in cam_of:
@@ -417,7 +428,7 @@ def extract_bundle_adjustment(problem: Problem) -> ExtractedBA:
         observations=torch.tensor(obs, dtype=torch.float64, device=dev),
         camera_index=torch.tensor([cam_of[i] for i in ci], dtype=torch.int64, device=dev),
         point_index=torch.tensor([pt_of[i] for i in pi], dtype=torch.int64, device=dev),
-        loss=loss0,
+        loss=as_loss(loss0),
         camera_constant=torch.tensor([b.constant for b in cam_blocks], dtype=torch.bool, device=dev),
         point_constant=torch.tensor([b.constant for b in pt_blocks], dtype=torch.bool, device=dev),
         camera_blocks=cam_blocks,

@@ -70,6 +70,10 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
     synchronisation) and puts the per-entry-point device times in
     ``summary.kernel_profile``.
     """
+    if not isinstance(options, SolverOptions):
+        from .dropin import options_from
+
+        options = options_from(options)
     options.validate()
     _check_supported(options)
     start = time.perf_counter()
@@ -89,7 +93,8 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
         summary.num_residual_blocks = ba.num_observations
         summary.num_residuals = 2 * ba.num_observations
         extracted = None
-    elif isinstance(problem, Problem):
+    elif isinstance(problem, Problem) or (hasattr(problem, "residual_blocks") and hasattr(problem, "parameter_blocks")):
+        # this package's Problem, or one with ceres-torch's Problem structure
         extracted = extract_bundle_adjustment(problem)
         cams, pts = extracted.cameras, extracted.points
         cam_const, pt_const = extracted.camera_constant, extracted.point_constant

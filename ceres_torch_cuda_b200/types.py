@@ -5,7 +5,7 @@ ceres-torch keeps working. Enum values are the member names, as in ceres-torch.
 """
 from __future__ import annotations
 
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, fields
 from enum import Enum
 from typing import Callable
 
@@ -136,6 +136,19 @@ class SolverOptions:
     gradient_check_numeric_derivative_relative_step_size: float = 1e-6
     update_state_every_iteration: bool = False
     callbacks: list[Callable[[IterationSummary], CallbackReturnType]] = field(default_factory=list)
+
+    def __post_init__(self) -> None:
+        # enum members of another module with the same member names (ceres-torch's own
+        # SolverOptions passed field by field) become this module's members
+        for f in fields(self):
+            default = f.default
+            if isinstance(default, Enum):
+                v = getattr(self, f.name)
+                if not isinstance(v, type(default)):
+                    try:
+                        setattr(self, f.name, type(default)[getattr(v, "name", str(v))])
+                    except KeyError as exc:
+                        raise ValueError(f"{f.name}: {v!r} is not a {type(default).__name__} member") from exc
 
     def _rules(self):
         """(condition, message) pairs; the messages are the ones ceres-torch raises."""

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define CERES_B200_ABI_VERSION 3
+#define CERES_B200_ABI_VERSION 4
 
 /* status codes */
 #define CERES_B200_OK 0
@@ -97,7 +97,15 @@ enum {
  *
  * Jacobian records are 24 scalars per slot (camera row 0 [9], camera row 1
  * [9], point row 0 [3], point row 1 [3]) of float (FP32) or double (FP64).
+ * The evaluation writes each record twice: at its slot (point-major) and at its
+ * camera-major position (cm_jac[e], e the entry's index in cam_entries), so
+ * that the camera-side passes stream their records instead of gathering them.
+ * Camera work items cut every camera's entries into runs of at most
+ * CERES_B200_CAM_ITEM entries; item i = (camera, first entry) covers entries
+ * first .. min(first + CERES_B200_CAM_ITEM, cam_offsets[camera + 1]) - 1, and
+ * cam_items[c] .. cam_items[c + 1] - 1 are camera c's items.
  */
+#define CERES_B200_CAM_ITEM 256
 typedef struct ceres_b200_ba_t {
   int32_t num_cameras;
   int32_t num_observations;  /* real observations (entries of the camera-major list) */
@@ -153,6 +161,14 @@ typedef struct ceres_b200_ba_t {
   void* pcg_z;
   void* pcg_p;                 /* [2][num_cameras][9] double-buffered direction */
   void* pcg_ap;
+
+  /* camera-major copy of the Jacobian store and the camera work items */
+  const int32_t* slot_pos;     /* [num_slots] camera-major position of the slot's observation, -1 padding */
+  void* cm_jac;                /* [num_observations][24] float or double, 32-byte aligned */
+  const int32_t* cam_items;    /* [num_cameras + 1] first item of each camera */
+  const int32_t* items;        /* [num_items][2] (camera, first entry) */
+  int32_t num_items;
+  int32_t max_camera_obs;      /* largest entry count of a camera */
 
   /* scratch owned by the caller */
   void* scratch;               /* per-CTA partial sums; see ceres_b200_scratch_bytes */
@@ -283,6 +299,34 @@ int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, voi
  */
 int ceres_b200_dense_cholesky_solve(double* H, const double* rhs, double* x, int64_t n, uint32_t* flags,
                                     void* stream);
+
+/*
+ * The explicit reduced camera matrix S = H_bb - H_ba H_aa^-1 H_ab + D_c (float64, [n][n]
+ * row-major, n = 9 num_cameras) at the last evaluation and assembly; the block of a
+ * constant camera is the identity. With point_assemble / camera_assemble called with
+ * radius = +inf (no damping), S^-1 is the camera block of (J^T J)^-1: the camera
+ * covariance that covariance.py:86-445 computes from the dense Jacobian's SVD.
+ */
+int ceres_b200_ba_schur_matrix(const ceres_b200_ba_t* ba, double* S, void* stream);
+
+/*
+ * inv = A^-1 for a symmetric positive definite float64 A ([n][n], overwritten by its
+ * Cholesky factor; n <= 32768): cooperative right-looking Cholesky, then one CTA per
+ * column of the inverse. flags: four uint32 (three for the grid barrier, zeroed here;
+ * flags[3] gets CERES_B200_DEVERR_NOT_PD when A is not positive definite, which the
+ * caller zeroes). Used for the camera covariance (covariance.py:86-445).
+ */
+int ceres_b200_dense_spd_inverse(double* A, double* inv, int64_t n, uint32_t* flags, void* stream);
+
+/*
+ * Check of the bounded waits of the cooperative kernels (failure detection without a
+ * GPU fault): two CTAs meet at the grid barrier of ceres_b200_ba_pcg, except that the
+ * second never arrives. The first gives up after spin_limit polls (at most the
+ * library's own limit of 2^24), ORs CERES_B200_DEVERR_BARRIER into words[2] and
+ * returns, so the context stays usable. words: three zero-initialised uint32 (arrival
+ * count, generation, error flag). No counterpart in the reference.
+ */
+int ceres_b200_debug_barrier_timeout(uint32_t* words, uint32_t spin_limit, void* stream);
 
 /* ------------------------------------------------------------------------------------
  * Batched solves: many independent bundle-adjustment problems in one persistent launch.
