@@ -207,7 +207,9 @@ int ceres_b200_ba_evaluate(const ceres_b200_ba_t* ba, int with_jacobian, void* s
  * partials go to a static 256 KB array inside the library (32768 float64 slots,
  * one per evaluation CTA; each loaded GPU keeps it until the process exits). The
  * first call on a device looks up that array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture. Sizes
+ * (cudaGetSymbolAddress) and remembers the context it was taken in; a later call in
+ * a new context of that device (after a device reset) looks it up again. Make the
+ * first call in each context before any stream capture. Sizes
  * that need more slots return CERES_B200_ETOOBIG. Calls share the array: two
  * calls that overlap on the GPU race. No memory is allocated or freed.
  * This entry point has no counterpart in the reference.

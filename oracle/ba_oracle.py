@@ -819,3 +819,80 @@ def schur_visibility(prob: OracleProblem):
     if not any(sets):
         return None
     return tuple(tuple(sorted(s)) for s in sets)
+
+
+# --------------------------------------------------------------------------------------
+# Covariance (covariance.py:86-445, DENSE_SVD path)
+# --------------------------------------------------------------------------------------
+@dataclass
+class OracleCovariance:
+    success: bool
+    message: str
+    rank: int
+    nullity: int
+    tangent: np.ndarray          # [n, n] covariance of the active tangent columns
+    cam_col: np.ndarray          # camera -> first column (-1 constant)
+    pt_col: np.ndarray           # point -> first column (-1 constant)
+
+    def block(self, kind_a: str, a: int, kind_b: str, b: int) -> np.ndarray:
+        """Ambient covariance block (Euclidean blocks: the tangent block; constant blocks:
+        zeros), as get_covariance_block (covariance.py:270-282) returns it."""
+        sa = self._slice(kind_a, a)
+        sb = self._slice(kind_b, b)
+        na, nb = (9 if kind_a == "camera" else 3), (9 if kind_b == "camera" else 3)
+        if sa is None or sb is None:
+            return np.zeros((na, nb))
+        return self.tangent[sa, sb].copy()
+
+    def _slice(self, kind: str, i: int):
+        c = (self.cam_col if kind == "camera" else self.pt_col)[i]
+        if c < 0:
+            return None
+        return slice(c, c + (9 if kind == "camera" else 3))
+
+
+def covariance(prob: OracleProblem, cameras, points, *, apply_loss: bool = True, null_space_rank: int = 0,
+               min_reciprocal_condition_number: float = 1e-14) -> OracleCovariance:
+    """covariance.py:139-246: the dense Jacobian of the active blocks (corrected by the
+    loss when apply_loss, covariance.py:122-125), its SVD, singular values above
+    20 (m + n) eps s_max kept (:414-417), the retained spectrum checked against
+    min_reciprocal_condition_number (:216-224), covariance V diag(1/s^2) V^T (:202-203);
+    a rank-deficient Jacobian with null_space_rank 0 is a failure (:206-214)."""
+    if apply_loss:
+        ev = evaluate(prob, cameras, points)
+        Jc, Jp = ev.Jc, ev.Jp
+    else:
+        _, Jc, Jp = snavely_residuals_and_jacobians(cameras, points, prob.observations, prob.camera_index,
+                                                     prob.point_index)
+        Jc = Jc * (~prob.camera_constant[prob.camera_index])[:, None, None]
+        Jp = Jp * (~prob.point_constant[prob.point_index])[:, None, None]
+    nca, npa = prob.active_cams.size, prob.active_pts.size
+    n = 9 * nca + 3 * npa
+    cam_col = np.where(prob.cam_col >= 0, 9 * prob.cam_col, -1)
+    pt_col = np.where(prob.pt_col >= 0, 9 * nca + 3 * prob.pt_col, -1)
+    no = prob.observations.shape[0]
+    J = np.zeros((2 * no, n))
+    for o in range(no):
+        c, q = prob.camera_index[o], prob.point_index[o]
+        if cam_col[c] >= 0:
+            J[2 * o:2 * o + 2, cam_col[c]:cam_col[c] + 9] = Jc[o]
+        if pt_col[q] >= 0:
+            J[2 * o:2 * o + 2, pt_col[q]:pt_col[q] + 3] = Jp[o]
+    _, S, Vh = np.linalg.svd(J, full_matrices=False)
+    threshold = 20.0 * (J.shape[0] + J.shape[1]) * EPS64 * S.max()
+    keep = S > threshold
+    ratios = (S / max(S.max(), TINY64)) ** 2
+    if null_space_rank == -1:
+        keep &= ratios >= min_reciprocal_condition_number
+    elif null_space_rank > 0:
+        keep = keep.copy()
+        keep[-null_space_rank:] = False
+    inv_s2 = np.where(keep, 1.0 / np.where(keep, S * S, 1.0), 0.0)
+    tangent = (Vh.T * inv_s2) @ Vh
+    rank = int(keep.sum())
+    success, message = True, "Computed covariance with dense SVD."
+    if null_space_rank == 0 and rank < J.shape[1]:
+        success, message = False, "Jacobian is rank deficient."
+    elif np.any(ratios[keep] < min_reciprocal_condition_number):
+        success, message = False, "Retained covariance spectrum is below min_reciprocal_condition_number."
+    return OracleCovariance(success, message, rank, max(0, J.shape[1] - rank), tangent, cam_col, pt_col)

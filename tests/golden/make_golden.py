@@ -1,8 +1,8 @@
 """Generate golden fixtures by running the ceres-torch reference itself.
 
-Run in a container that has the reference checked out (read-only is fine):
+Run where the reference is checked out (read-only is fine), naming its root:
 
-    python tests/golden/make_golden.py --reference /root/reference [--big]
+    python tests/golden/make_golden.py --reference <ceres-torch checkout> [--big]
 
 Each fixture is an ``.npz`` holding the inputs (seeded synthetic BA problem),
 what ceres-torch's own ``Problem.evaluate`` returns at the initial point
@@ -193,9 +193,65 @@ def make_rotation(tc, out=HERE):
     print("rotation.npz written", flush=True)
 
 
+def make_covariance(tc, ex, name, data, *, constant_cameras, out=HERE, point_blocks=5):
+    """Solve with the reference (DENSE_SCHUR, its default tolerances), then its own
+    Covariance (covariance.py:86-445, DENSE_SVD, default options) of every free camera
+    pair, the first ``point_blocks`` points and camera-point pairs at the solution."""
+    problem, cams, pts = _build(tc, ex, data, constant_cameras)
+    t0 = time.time()
+    summary = tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.DENSE_SCHUR), problem)
+    blocks = problem.parameter_blocks
+    cam_blocks, pt_blocks = blocks[:data.num_cameras], blocks[data.num_cameras:]
+    free = [i for i in range(data.num_cameras) if i not in constant_cameras]
+    chosen_pts = list(range(min(point_blocks, data.num_points)))
+    pairs = [(cam_blocks[i], cam_blocks[j]) for a, i in enumerate(free) for j in free[a:]]
+    pairs += [(pt_blocks[q], pt_blocks[q]) for q in chosen_pts]
+    pairs += [(cam_blocks[free[0]], pt_blocks[q]) for q in chosen_pts] if free else []
+    cov = tc.Covariance()
+    ok = cov.compute(pairs, problem)
+    cc = np.zeros((len(free), len(free), 9, 9))
+    pp = np.zeros((len(chosen_pts), 3, 3))
+    cp = np.zeros((len(chosen_pts), 9, 3))
+    if ok:
+        for a, i in enumerate(free):
+            for b, j in enumerate(free):
+                cc[a, b] = cov.get_covariance_block(cam_blocks[i], cam_blocks[j]).numpy()
+        for k, q in enumerate(chosen_pts):
+            pp[k] = cov.get_covariance_block(pt_blocks[q], pt_blocks[q]).numpy()
+            if free:
+                cp[k] = cov.get_covariance_block(cam_blocks[free[0]], pt_blocks[q]).numpy()
+    meta = {"name": name, "loss": list(data.loss), "constant_cameras": list(constant_cameras), "free_cameras": free,
+            "points": chosen_pts, "success": bool(cov.summary.success), "message": cov.summary.message,
+            "rank": int(cov.summary.rank), "nullity": int(cov.summary.nullity),
+            "tangent_dimension": int(cov.summary.tangent_dimension), "final_cost": float(summary.final_cost),
+            "seconds": time.time() - t0}
+    np.savez_compressed(out / f"{name}.npz", meta=json.dumps(meta), cameras=data.cameras, points=data.points,
+                        observations=data.observations, camera_index=data.camera_index,
+                        point_index=data.point_index, solved_cameras=cams.numpy(), solved_points=pts.numpy(),
+                        cov_cameras=cc, cov_points=pp, cov_camera_point=cp)
+    print(f"{name}: success={cov.summary.success} rank={cov.summary.rank} ({meta['seconds']:.1f} s)", flush=True)
+
+
+def make_bal(ex, name, data, out=HERE):
+    """BAL text of ``data`` (the format BALProblem.from_text reads,
+    examples/simple_bundle_adjuster.py:33-70) and what the reference parser returns."""
+    lines = [f"{data.num_cameras} {data.num_points} {data.num_observations}"]
+    for c, q, o in zip(data.camera_index.tolist(), data.point_index.tolist(), data.observations.tolist()):
+        lines.append(f"{c} {q} {o[0]!r} {o[1]!r}")
+    lines += [repr(float(v)) for v in data.cameras.reshape(-1)]
+    lines += [repr(float(v)) for v in data.points.reshape(-1)]
+    text = "\n".join(lines) + "\n"
+    bal = ex.BALProblem.from_text(text)
+    np.savez_compressed(out / f"{name}.npz", meta=json.dumps({"name": name}), text=np.array(text),
+                        camera_indices=np.array(bal.camera_indices, dtype=np.int64),
+                        point_indices=np.array(bal.point_indices, dtype=np.int64),
+                        observations=bal.observations.numpy(), cameras=bal.cameras.numpy(), points=bal.points.numpy())
+    print(f"{name}: {bal.num_cameras} cameras, {bal.num_points} points, {bal.num_observations} observations", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of a ceres-torch checkout (src/, examples/)")
     ap.add_argument("--big", action="store_true", help="also run config0 at full size (minutes)")
     ap.add_argument("--only", default="")
     args = ap.parse_args()
@@ -241,6 +297,17 @@ def main():
         si = S.make_small_ba(5, 40, 3, seed=9)
         make_case(tc, ex, "ba_spse_init", si, solver="ITERATIVE_SCHUR",
                   spse=dict(use_spse_initialization=True, max_num_spse_iterations=3))
+    if want("ba_covariance"):
+        cv = S.make_small_ba(6, 40, 4, seed=10)
+        make_covariance(tc, ex, "ba_covariance", cv, constant_cameras=(0, 1))
+    if want("ba_covariance_cauchy"):
+        cvc = S.make_small_ba(5, 40, 4, seed=11, loss=("cauchy", 2.0), outlier_fraction=0.05)
+        make_covariance(tc, ex, "ba_covariance_cauchy", cvc, constant_cameras=(0, 2))
+    if want("ba_covariance_gauge"):
+        cvg = S.make_small_ba(4, 30, 3, seed=12)
+        make_covariance(tc, ex, "ba_covariance_gauge", cvg, constant_cameras=())
+    if want("bal_text"):
+        make_bal(ex, "bal_text", S.make_small_ba(7, 60, 3, seed=13))
     if args.big and want("config0_dense"):
         make_case(tc, ex, "config0_dense", S.ba_config(0), solver="DENSE_SCHUR")
     if args.big and want("config1_small"):

@@ -69,6 +69,8 @@ def test_stats_indices_match_header():
         m = re.search(rf"{name}\s*=\s*(\d+)", text)
         assert m and int(m.group(1)) == idx, name
     assert _lib.NSTATS * 8 <= _lib.CTL_COUNTERS and _lib.CTL_COUNTERS + 16 * 4 <= _lib.CTL_BYTES
+    m = re.search(r"#define CERES_B200_CAM_ITEM (\d+)", text)
+    assert m and int(m.group(1)) == _lib.CAM_ITEM
 
 
 def test_invalid_arguments_are_rejected_without_a_gpu(lib):

@@ -38,6 +38,20 @@ def _check_invariants(L, ci, pi, obs, nc, npts):
         assert (np.diff(slot[idx]) > 0).all()
     ent = L.cam_entries.numpy()
     off = L.cam_offsets.numpy()
+    # camera-major positions: the inverse of the entries' slot column, -1 on padding
+    pos = L.slot_pos.numpy()
+    if len(ent):
+        np.testing.assert_array_equal(pos[ent[:, 0]], np.arange(len(ent)))
+    assert (pos >= 0).sum() == len(ent)
+    # camera work items cover each camera's entries in order, in runs of at most CAM_ITEM
+    from ceres_torch_cuda_b200 import _lib
+
+    items, ci_off = L.items.numpy(), L.cam_items.numpy()
+    for c in range(nc):
+        firsts = items[ci_off[c]:ci_off[c + 1]]
+        assert (firsts[:, 0] == c).all()
+        np.testing.assert_array_equal(firsts[:, 1], np.arange(off[c], off[c + 1], _lib.CAM_ITEM))
+    assert L.max_camera_obs == (int(np.diff(off).max()) if nc else 0)
     assert off[-1] == len(ci)
     for c in range(nc):
         e = ent[off[c]:off[c + 1]]
@@ -56,6 +70,20 @@ def test_layout_visibility_is_bit_exact_with_reference(name):
     const = set(d["meta"]["constant_cameras"])
     ent = L.cam_entries.numpy()
     off = L.cam_offsets.numpy()
+    # camera-major positions: the inverse of the entries' slot column, -1 on padding
+    pos = L.slot_pos.numpy()
+    if len(ent):
+        np.testing.assert_array_equal(pos[ent[:, 0]], np.arange(len(ent)))
+    assert (pos >= 0).sum() == len(ent)
+    # camera work items cover each camera's entries in order, in runs of at most CAM_ITEM
+    from ceres_torch_cuda_b200 import _lib
+
+    items, ci_off = L.items.numpy(), L.cam_items.numpy()
+    for c in range(nc):
+        firsts = items[ci_off[c]:ci_off[c + 1]]
+        assert (firsts[:, 0] == c).all()
+        np.testing.assert_array_equal(firsts[:, 1], np.arange(off[c], off[c + 1], _lib.CAM_ITEM))
+    assert L.max_camera_obs == (int(np.diff(off).max()) if nc else 0)
     lane_point = L.lane_point.numpy()
     vis = [np.unique(lane_point[ent[off[c]:off[c + 1], 1]]) for c in range(nc) if c not in const]
     np.testing.assert_array_equal(np.concatenate(vis), d["visibility_flat"])

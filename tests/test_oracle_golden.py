@@ -128,3 +128,53 @@ def test_lm_solve_matches_reference(name):
     np.testing.assert_array_equal(lin, trace[:, 7].astype(int))
     costs = np.array([it.cost for it in r.iterations])
     np.testing.assert_allclose(costs, trace[:, 1], rtol=1e-9)
+
+
+@pytest.mark.parametrize("name", ["ba_covariance", "ba_covariance_cauchy", "ba_covariance_gauge"])
+def test_oracle_covariance_matches_reference(name):
+    """The oracle's dense-SVD covariance (covariance.py:86-445) against the reference's own
+    Covariance at the reference's solution: success, rank and every stored block."""
+    d = G.load(name)
+    meta = d["meta"]
+    nc = d["cameras"].shape[0]
+    p = O.OracleProblem(d["solved_cameras"], d["solved_points"], d["observations"], d["camera_index"],
+                        d["point_index"], G.loss_spec(meta["loss"]),
+                        camera_constant=G.constant_mask(nc, meta["constant_cameras"]))
+    c = O.covariance(p, p.cameras, p.points)
+    assert (c.success, c.message, c.rank, c.nullity) == (meta["success"], meta["message"], meta["rank"], meta["nullity"])
+    if not c.success:
+        return
+    free, pts = meta["free_cameras"], meta["points"]
+    for a, i in enumerate(free):
+        for b, j in enumerate(free):
+            np.testing.assert_allclose(c.block("camera", i, "camera", j), d["cov_cameras"][a, b], rtol=1e-8,
+                                       atol=1e-10 * np.abs(d["cov_cameras"]).max())
+    for k, q in enumerate(pts):
+        np.testing.assert_allclose(c.block("point", q, "point", q), d["cov_points"][k], rtol=1e-8,
+                                   atol=1e-10 * np.abs(d["cov_points"]).max())
+        np.testing.assert_allclose(c.block("camera", free[0], "point", q), d["cov_camera_point"][k], rtol=1e-8,
+                                   atol=1e-10 * np.abs(d["cov_camera_point"]).max())
+
+
+def test_bal_text_parse_matches_reference():
+    """BundleAdjustmentProblem.from_bal_text (one vectorised conversion) against the
+    reference's BALProblem.from_text (examples/simple_bundle_adjuster.py:33-70) on the
+    same text: identical indices, observations and parameters."""
+    import torch
+
+    from ceres_torch_cuda_b200 import BundleAdjustmentProblem
+
+    z = np.load(G.GOLDEN / "bal_text.npz")
+    text = str(z["text"])
+    ba = BundleAdjustmentProblem.from_bal_text(text, device="cpu")
+    np.testing.assert_array_equal(ba.camera_index.numpy(), z["camera_indices"])
+    np.testing.assert_array_equal(ba.point_index.numpy(), z["point_indices"])
+    np.testing.assert_array_equal(ba.observations.numpy(), z["observations"])
+    np.testing.assert_array_equal(ba.cameras.numpy(), z["cameras"])
+    np.testing.assert_array_equal(ba.points.numpy(), z["points"])
+    assert ba.cameras.dtype == torch.float64
+    # the reference's error cases: trailing values, truncated input
+    with pytest.raises(ValueError, match="trailing"):
+        BundleAdjustmentProblem.from_bal_text(text + " 1.0", device="cpu")
+    with pytest.raises(ValueError, match="truncated"):
+        BundleAdjustmentProblem.from_bal_text(text.rsplit("\n", 2)[0], device="cpu")
