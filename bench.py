@@ -149,9 +149,54 @@ def loss_of(tc, data):
 
 
 # --------------------------------------------------------------------------------------
-# CPU baseline: the float64 numpy oracle (a restatement of the reference algorithm)
+# CPU baseline: the float64 numpy oracle (a restatement of the reference algorithm) and
+# the reference's own Problem.evaluate
 # --------------------------------------------------------------------------------------
-def cpu_sample(full_obs: int, small: bool = False) -> dict:
+# LM iterations of the float64 solve of the 6.0M-observation problem to C*(1+1e-6), as the
+# GPU arm measures them (``fp64.iterations_to_tol`` of its line); the float64 oracle takes
+# the same iterations. Used only by the reference arm, which runs without a GPU.
+FULL_PROBLEM_FP64_ITERATIONS = 79
+
+
+def host_info() -> dict:
+    """The host the CPU figures ran on: logical CPUs, the ones this process may use, the
+    BLAS threads numpy runs with, torch's intra-op threads and the CPU model."""
+    info: dict = {"os_cpu_count": os.cpu_count()}
+    try:
+        info["affinity_cpus"] = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        info["affinity_cpus"] = None
+    try:
+        from threadpoolctl import threadpool_info
+
+        pools = threadpool_info()
+        info["blas_threads"] = max((p.get("num_threads", 1) for p in pools), default=1)
+        info["blas"] = sorted({p.get("internal_api", "?") for p in pools})
+    except Exception as exc:  # noqa: BLE001 - informational only
+        info["blas_threads"] = None
+        info["blas_error"] = str(exc)
+    try:
+        import torch
+
+        info["torch_threads"] = torch.get_num_threads()
+    except Exception:  # noqa: BLE001
+        info["torch_threads"] = None
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                info["cpu_model"] = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return info
+
+
+def cpu_sample(full_obs: int, full_iterations: int, small: bool = False) -> dict:
+    """The oracle's LM solve of a smaller ring problem (same generator and loss), timed
+    per LM iteration and scaled to the full problem: seconds per iteration x (full
+    observations / sample observations) x the full problem's LM iterations to the
+    target. One LM iteration of the oracle is linear in the observations (evaluation,
+    Schur assembly and PCG products all stream them)."""
     from ceres_torch_cuda_b200 import synthetic as S
     from oracle import ba_oracle as O
 
@@ -162,11 +207,66 @@ def cpu_sample(full_obs: int, small: bool = False) -> dict:
     r = O.solve(p, O.OracleOptions(linear_solver_type="ITERATIVE_SCHUR", preconditioner_type="SCHUR_JACOBI",
                                    explicit_schur_limit=0))
     dt = time.perf_counter() - t0
+    its = max(len(r.iterations) - 1, 1)  # iteration 0 is the initial evaluation
+    per_it = dt / its
     scale = full_obs / d.num_observations
-    return {"seconds": dt, "value": dt * scale, "obs": d.num_observations, "iterations": len(r.iterations),
-            "sample": (f"float64 numpy oracle, full LM solve of a ring BA with {nc} cameras / {npts} points / "
-                       f"{d.num_observations} observations (Cauchy 2, ITERATIVE_SCHUR + SCHUR_JACOBI), "
-                       f"{dt:.1f} s scaled by the observation ratio x{scale:.1f}")}
+    host = host_info()
+    return {"seconds": dt, "value": per_it * scale * full_iterations, "obs": d.num_observations, "iterations": its,
+            "seconds_per_iteration": per_it, "host": host,
+            "sample": (f"float64 numpy oracle (restated reference algorithm, mostly single-threaded numpy), full LM "
+                       f"solve of a ring BA with {nc} cameras / {npts} points / {d.num_observations} observations "
+                       f"(Cauchy 2, ITERATIVE_SCHUR + SCHUR_JACOBI): {dt:.1f} s for {its} LM iterations, "
+                       f"{per_it:.3f} s per iteration x {scale:.1f} (observation ratio) x {full_iterations} "
+                       f"(LM iterations of the full problem to the target)")}
+
+
+def reference_evaluate_datum(num_cameras: int = 16, num_points: int = 125) -> dict | None:
+    """The reference's own Problem.evaluate (problem.py:377-413) on a configuration-0
+    problem cut to ``num_points`` points (4 observations each), built the way its BAL
+    example builds it (one autodiff residual block per observation), timed once on the
+    host's CPU threads: seconds per observation of a Jacobian evaluation. None when the
+    reference package is not installed in baseline/_ref."""
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "ceres_torch" / "__init__.py").exists():
+        return None
+    if str(ref) not in sys.path:
+        sys.path.append(str(ref))
+    try:
+        import ceres_torch as ct
+        import torch
+
+        from ceres_torch_cuda_b200 import synthetic as S
+    except Exception as exc:  # noqa: BLE001 - reported, not fatal
+        return {"error": f"import: {exc}"}
+    d = S.make_uniform_ba(num_cameras, num_points, 4, seed=100)
+    cams = torch.tensor(d.cameras)
+    pts = torch.tensor(d.points)
+    problem = ct.Problem()
+    cb = [cams[i] for i in range(num_cameras)]
+    pb = [pts[i] for i in range(num_points)]
+    for c in cb:
+        problem.AddParameterBlock(c)
+    for q in pb:
+        problem.AddParameterBlock(q)
+        problem.SetParameterBlockOrderingGroup(q, 0)
+
+    def project(camera, point):
+        p = ct.angle_axis_rotate_point(camera[:3], point) + camera[3:6]
+        xp, yp = -p[0] / p[2], -p[1] / p[2]
+        r2 = xp * xp + yp * yp
+        return camera[6] * (1.0 + r2 * (camera[7] + camera[8] * r2)) * torch.stack([xp, yp])
+
+    for c, q, o in zip(d.camera_index.tolist(), d.point_index.tolist(), d.observations):
+        ob = torch.tensor(o)
+        problem.AddResidualBlock(ct.AutoDiffCostFunction(lambda cam, pt, ob=ob: project(cam, pt) - ob, [9, 3], 2),
+                                 None, [cb[c], pb[q]])
+    t0 = time.perf_counter()
+    problem.evaluate()
+    dt = time.perf_counter() - t0
+    return {"seconds": dt, "observations": d.num_observations, "seconds_per_observation": dt / d.num_observations,
+            "torch_threads": torch.get_num_threads(),
+            "what": f"ceres_torch Problem.evaluate with Jacobian, {num_cameras} cameras / {num_points} points / "
+                    f"{d.num_observations} observations (configuration 0 model), float64 on CPU"}
 
 
 def run_reference(args):
@@ -176,19 +276,22 @@ def run_reference(args):
     data = make_workload(args)
     full_obs = data.num_observations
     for _ in range(args.warmup):
-        cpu_sample(full_obs, small=True)
+        cpu_sample(full_obs, FULL_PROBLEM_FP64_ITERATIONS, small=True)
     vals, samples = [], []
     for _ in range(args.steps):
-        s = cpu_sample(full_obs)
+        s = cpu_sample(full_obs, FULL_PROBLEM_FP64_ITERATIONS)
         vals.append(s["value"])
         samples.append(s)
     v = statistics.median(vals)
+    host = samples[-1]["host"]
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median(s["seconds"] for s in samples),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": data.description, "observations": full_obs, "parallelism": "replicas"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": samples[-1]["sample"]},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": host.get("blas_threads") or 1, "kind": "port",
+                         "sample": samples[-1]["sample"], "extrapolated": True, "host": host,
+                         "reference_evaluate": reference_evaluate_datum()},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -302,7 +405,9 @@ def run_ours(args):
         value, e2e = reduce_max([value, e2e], dev)
 
     if rank == 0:
-        cpu = cpu_sample(data.num_observations) if not args.no_cpu_baseline else None
+        fp64_iterations = max(len(fp64_runs[-1][0].iterations) - 1, 1)
+        cpu = cpu_sample(data.num_observations, fp64_iterations) if not args.no_cpu_baseline else None
+        ref_eval = reference_evaluate_datum() if not args.no_cpu_baseline else None
         peaks = {}
         pk = ROOT / "MEASURED_PEAKS.json"
         if pk.exists():
@@ -341,17 +446,33 @@ def run_ours(args):
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"},
             "kernels_timed_region": live,
             "kernels_isolated": prof["table"],
-            "cpu_baseline": None if cpu is None else {"value": cpu["value"], "unit": UNIT, "cores": 1, "kind": "port",
-                                                      "sample": cpu["sample"]},
+            "cpu_baseline": None if cpu is None else {
+                "value": cpu["value"], "unit": UNIT, "cores": cpu["host"].get("blas_threads") or 1, "kind": "port",
+                "sample": cpu["sample"], "extrapolated": True, "host": cpu["host"], "reference_evaluate": ref_eval},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in), "d2h_bytes_per_step": int(bytes_out)},
             "gpu_launches": launches,
             "clocks": clocks,
         }
+        if world == 1 and not args.no_side_blocks:
+            line["serving"] = _side_block(lambda: serving_result(args.rate, args.serving_duration))
+            line["batched"] = _side_block(lambda: batched_result(args, args.batch_instances, 1, 1))
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _side_block(fn) -> dict:
+    """The served-stream (configuration 4) or batched (configuration 3) measurement
+    carried in the default line; its failure is reported in the block."""
+    t0 = time.perf_counter()
+    try:
+        out = fn()
+    except Exception as exc:  # noqa: BLE001 - the main measurement stands on its own
+        return {"error": f"{type(exc).__name__}: {exc}"}
+    out["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 # DRAM traffic of the PCG kernel from one ncu capture (--set full of k_pcg<float> on
@@ -485,15 +606,19 @@ def _batched_problems(tc, datas):
 
 
 def run_batched(args):
-    """Configuration 3: 4,096 independent instances solved in one persistent launch.
-    value = instances per second of the launch (inputs in HBM); e2e = solve_batch from
-    host arrays (upload, layout, launch, results back)."""
+    print(json.dumps(batched_result(args, max(1, int(4096 * args.scale)), args.steps, args.warmup)), flush=True)
+    return 0
+
+
+def batched_result(args, count: int, steps: int, warmup: int) -> dict:
+    """Configuration 3: ``count`` independent instances (4,096 at full size) solved in one
+    persistent launch. value = instances per second of the launch (inputs in HBM); e2e =
+    solve_batch from host arrays (upload, layout, launch, results back)."""
     import torch
 
     import ceres_torch_cuda_b200 as tc
     from ceres_torch_cuda_b200 import synthetic as S
 
-    count = max(1, int(4096 * args.scale))
     datas = S.make_batched_instances(count, seed=3)
     opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
                             preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI, max_num_iterations=50)
@@ -502,7 +627,7 @@ def run_batched(args):
     res = {}
     for prec in ("mixed", "fp64"):
         times, finals = [], None
-        for k in range(args.warmup + args.steps):
+        for k in range(warmup + steps):
             solver = tc.BatchSolver(base, opts, precision=prec)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -510,14 +635,14 @@ def run_batched(args):
             solver.launch(*shape)
             e1.record()
             torch.cuda.synchronize()
-            if k >= args.warmup:
+            if k >= warmup:
                 times.append(e0.elapsed_time(e1))
             finals = solver.summaries()
         res[prec] = {"ms": statistics.median(times), "summaries": finals}
     mixed, fp64 = res["mixed"]["summaries"], res["fp64"]["summaries"]
     rel = [abs(m.final_cost - f.final_cost) / max(f.final_cost, 1e-300) for m, f in zip(mixed, fp64)]
     e2e = []
-    for _ in range(max(1, args.steps)):
+    for _ in range(max(1, steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ps = _batched_problems(tc, datas)
@@ -528,7 +653,7 @@ def run_batched(args):
     nobs = sum(d.num_observations for d in datas)
     line = {
         "metric": "batched BA solves/s (configuration 3, one persistent launch)", "value": count / (ms / 1e3),
-        "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "unit": "solves/s", "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32+f64", "data": "synthetic",
         "config": {"workload": f"config3 {count} instances nc~U(3..32) np~U(50..2000) track~U(3..8)",
                    "instances": count, "observations": nobs, "cta_shape": list(shape), "cluster_size": 1,
@@ -541,11 +666,15 @@ def run_batched(args):
                                               2 * 8 * d.num_observations for d in datas)),
                 "d2h_bytes_per_step": int(sum(d.cameras.nbytes + d.points.nbytes for d in datas))},
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_serving(args):
+    print(json.dumps(serving_result(args.rate, args.duration)), flush=True)
+    return 0
+
+
+def serving_result(rate: float, duration: float) -> dict:
     """Configuration 4: a Poisson stream of solve requests through the continuous-batching
     server; value = p99 latency (ms) at the offered rate, mixed precision; the float64
     server is run on the same stream."""
@@ -555,8 +684,7 @@ def run_serving(args):
     from ceres_torch_cuda_b200 import synthetic as S
     from ceres_torch_cuda_b200.serving import BAServer, run_stream
 
-    rate = args.rate
-    count = max(16, int(rate * args.duration))
+    count = max(16, int(rate * duration))
     arrivals, datas = S.make_serving_requests(count, seed=4, rate_hz=rate)
     opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
                             preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI, max_num_iterations=50)
@@ -594,8 +722,7 @@ def run_serving(args):
         "e2e": {"value": m["p99_ms"], "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "note": "requests are device-resident at submission; latency = submission to solution on device"},
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def main():
@@ -609,6 +736,12 @@ def main():
     ap.add_argument("--duration", type=float, default=2.0, help="configuration 4: seconds of arrivals")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-side-blocks", action="store_true",
+                    help="default run: leave out the served-stream and batched blocks")
+    ap.add_argument("--serving-duration", type=float, default=10.0,
+                    help="default run: seconds of Poisson arrivals for the served-stream block")
+    ap.add_argument("--batch-instances", type=int, default=4096,
+                    help="default run: instances of the batched block")
     ap.add_argument("--kernel-pass", action="store_true",
                     help="run one LM iteration's kernels twice (for profiler captures) and exit")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
