@@ -208,8 +208,9 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
           for (int j = 0; j < 3; ++j) o.jp[0][j] = o.jp[1][j] = 0.0;
         }
         store_rec(jac, slot, o);
-        // the camera-major copy (the camera-side passes stream it in camera order)
-        store_rec(reinterpret_cast<T*>(ba.cm_jac), (size_t)ba.slot_pos[slot], o);
+        // the camera-major copy, when the caller keeps one (the camera-side passes then
+        // stream it in camera order instead of gathering records by slot)
+        if (ba.cm_jac != nullptr) store_rec(reinterpret_cast<T*>(ba.cm_jac), (size_t)ba.slot_pos[slot], o);
         double a[3], b[3];
 #pragma unroll
         for (int m = 0; m < 3; ++m) { a[m] = (double)(T)o.jp[0][m]; b[m] = (double)(T)o.jp[1][m]; }
@@ -328,7 +329,7 @@ __global__ void __launch_bounds__(kWarpBlock) k_point_assemble(ceres_b200_ba_t b
 // Schur diagonal block before damping), the camera column sums, the gradient and
 // the reduced rhs over the camera's observations, then forms the preconditioner.
 // ======================================================================================
-constexpr int kCamBlock = 128;
+constexpr int kCamBlock = 256;  // 4 warp pairs per camera
 constexpr int kCamAcc = 45 + 9 + 9 + 9;  // V (upper), colsum, g, h
 
 __device__ __forceinline__ int tri9(int j, int l) {  // upper-triangle index, j <= l
@@ -351,13 +352,17 @@ struct CamObs {
   double wg[3];
 };
 
-// The record comes from the camera-major copy (entry e: consecutive threads read
-// consecutive records); residual and point blocks are gathered by slot and point.
+// The record comes from the camera-major copy when there is one (entry e: consecutive
+// threads read consecutive records), else from its slot; residual and point blocks are
+// gathered by slot and point.
 template <typename T>
-__device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ cm,
-                                             const T* __restrict__ winv, int e, int2 ent, CamObs<T>& o) {
+__device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ jac,
+                                             const T* __restrict__ cm, const T* __restrict__ winv, int e, int2 ent,
+                                             CamObs<T>& o) {
   o.ent = ent;
-  load_rec(cm, (size_t)e, o.rv);
+  if (cm != nullptr) load_rec(cm, (size_t)e, o.rv);
+  else if constexpr (sizeof(T) == 4) load_rec128(jac, (size_t)ent.x, o.rv);
+  else load_rec(jac, (size_t)ent.x, o.rv);
   o.r = reinterpret_cast<const double2*>(ba.res)[ent.x];
 #pragma unroll
   for (int i = 0; i < 6; ++i) o.wi[i] = winv[6 * (size_t)ent.y + i];
@@ -365,38 +370,48 @@ __device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T*
   for (int i = 0; i < 3; ++i) o.wg[i] = ba.winv_ga[3 * (size_t)ent.y + i];
 }
 
-// Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
-// into acc_out[c][72] (float64). kHbb: the camera block is the Hbb block sum Jc^T Jc
-// (M = I below) instead of the Schur block; the base of SCHUR_POWER_SERIES_EXPANSION.
-template <typename T, bool kDup, bool kHbb = false>
-__global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba, double* __restrict__ acc_out) {
+// Sums of one half of the 72: rows R0..R1-1 of the Schur block's upper triangle and the
+// column sums, gradient and rhs entries J0..J1-1 (36 float64 each).
+template <int H> struct CamHalf {
+  static constexpr int R0 = H == 0 ? 0 : 3, R1 = H == 0 ? 3 : 9;
+  static constexpr int J0 = H == 0 ? 0 : 4, J1 = H == 0 ? 4 : 9;
+  static constexpr int NJ = J1 - J0;
+  static constexpr int NV = H == 0 ? 24 : 21;  // sum over the rows of 9 - r
+  // position of upper-triangle entry (r, l) among this half's entries
+  static __device__ __forceinline__ constexpr int v_index(int r, int l) {
+    return (r - R0) * 9 - ((r * (r - 1)) / 2 - (R0 * (R0 - 1)) / 2) + (l - r);
+  }
+};
+
+// One warp's half of a camera's sums over the observations of its warp pair (wp):
+// entries e0 + 32 wp + lane + 128 k. Lane sums reduced over the warp go to
+// sred[index * 4 + wp].
+template <typename T, bool kDup, bool kHbb, int H>
+__device__ __forceinline__ void camera_reduce_half(const ceres_b200_ba_t& ba, int c, bool cconst, int wp, int lane,
+                                                   double* __restrict__ sred) {
   using A = double;
-  __shared__ double sred[kCamAcc * (kCamBlock / 32)];
-  const int c = blockIdx.x;
+  using HF = CamHalf<H>;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ cm = reinterpret_cast<const T*>(ba.cm_jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  A av[54];      // Schur block (upper triangle, 45), column sums (9)
-  double ag[18]; // gradient (9), reduced rhs (9)
+  A v[HF::NV];
+  double cs[HF::NJ], g[HF::NJ], h[HF::NJ];
 #pragma unroll
-  for (int i = 0; i < 54; ++i) av[i] = (A)0;
+  for (int i = 0; i < HF::NV; ++i) v[i] = 0.0;
 #pragma unroll
-  for (int i = 0; i < 18; ++i) ag[i] = 0.0;
-  const bool cconst = ba.cam_const[c] != 0;
+  for (int i = 0; i < HF::NJ; ++i) { cs[i] = 0.0; g[i] = 0.0; h[i] = 0.0; }
   const int e0 = ba.cam_offsets[c], e1 = ba.cam_offsets[c + 1];
   if (!cconst) {
     const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);
-    const int stride = blockDim.x;
-    const int first = e0 + threadIdx.x;
+    constexpr int stride = kCamBlock / 2;
+    const int first = e0 + 32 * wp + lane;
     // entries are read two observations ahead, so each observation waits for one
-    // gather (its data) instead of two (entry, then data): 0.43 -> 0.39 ms on the
-    // 6.0M-observation problem (float32 store). Holding the next observation's data in
-    // registers as well spilled and ran slower.
+    // gather (its data) instead of two (entry, then data)
     int2 en1 = first < e1 ? ents[first] : make_int2(0, 0);
     int2 en2 = first + stride < e1 ? ents[first + stride] : make_int2(0, 0);
     for (int e = first; e < e1; e += stride) {
       CamObs<T> cur;
-      cam_obs_load(ba, cm, winv, e, en1, cur);
+      cam_obs_load(ba, jac, cm, winv, e, en1, cur);
       en1 = en2;
       en2 = e + 2 * stride < e1 ? ents[e + 2 * stride] : make_int2(0, 0);
       const size_t slot = (size_t)cur.ent.x;
@@ -421,25 +436,26 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
       const A B00 = P0[0] * jp0[0] + P0[1] * jp0[1] + P0[2] * jp0[2];
       const A B01 = P0[0] * jp1[0] + P0[1] * jp1[1] + P0[2] * jp1[2];
       const A B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
-      const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
-      const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
       const A M00 = kHbb ? (A)1 : (A)1 - B00, M01 = kHbb ? (A)0 : -B01, M11 = kHbb ? (A)1 : (A)1 - B11;
-      A K0[9], K1[9];
+      if (HF::NJ > 0) {
+        const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
+        const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
 #pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        const A c0 = (A)rv[j], c1 = (A)rv[9 + j];
-        K0[j] = M00 * c0 + M01 * c1;
-        K1[j] = M01 * c0 + M11 * c1;
-        av[45 + j] += c0 * c0 + c1 * c1;
-        const double d0 = (double)rv[j], d1 = (double)rv[9 + j];
-        ag[j] += d0 * r.x + d1 * r.y;
-        ag[9 + j] += d0 * (r.x + a0) + d1 * (r.y + a1);
+        for (int j = HF::J0; j < HF::J1; ++j) {
+          const double d0 = (double)rv[j], d1 = (double)rv[9 + j];
+          cs[j - HF::J0] += d0 * d0 + d1 * d1;
+          g[j - HF::J0] += d0 * r.x + d1 * r.y;
+          h[j - HF::J0] += d0 * (r.x + a0) + d1 * (r.y + a1);
+        }
       }
 #pragma unroll
-      for (int j = 0; j < 9; ++j)
+      for (int l = HF::R0; l < 9; ++l) {
+        const A c0 = (A)rv[l], c1 = (A)rv[9 + l];
+        const A k0 = M00 * c0 + M01 * c1, k1 = M01 * c0 + M11 * c1;
 #pragma unroll
-        for (int l = j; l < 9; ++l) av[tri9(j, l)] += (A)rv[j] * K0[l] + (A)rv[9 + j] * K1[l];
-
+        for (int rr = HF::R0; rr < HF::R1; ++rr)
+          if (rr <= l) v[HF::v_index(rr, l)] += (A)rv[rr] * k0 + (A)rv[9 + rr] * k1;
+      }
       if (kDup && !kHbb) {
         // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
         const int sidx = q >> 5, ln = q & 31;
@@ -455,33 +471,57 @@ __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba,
           const A C10 = P1[0] * (A)rk[18] + P1[1] * (A)rk[19] + P1[2] * (A)rk[20];
           const A C11 = P1[0] * (A)rk[21] + P1[1] * (A)rk[22] + P1[2] * (A)rk[23];
 #pragma unroll
-          for (int j = 0; j < 9; ++j) {
-            const A t0 = (A)rv[j] * C00 + (A)rv[9 + j] * C10;
-            const A t1 = (A)rv[j] * C01 + (A)rv[9 + j] * C11;
+          for (int rr = HF::R0; rr < HF::R1; ++rr) {
+            const A t0 = (A)rv[rr] * C00 + (A)rv[9 + rr] * C10;
+            const A t1 = (A)rv[rr] * C01 + (A)rv[9 + rr] * C11;
 #pragma unroll
-            for (int l = j; l < 9; ++l) av[tri9(j, l)] -= t0 * (A)rk[l] + t1 * (A)rk[9 + l];
+            for (int l = rr; l < 9; ++l) v[HF::v_index(rr, l)] -= t0 * (A)rk[l] + t1 * (A)rk[9 + l];
           }
         }
       }
     }
   }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-  for (int i = 0; i < 54; ++i) {
-    const double v = warp_sum((double)av[i]);
-    if (lane == 0) sred[i * nw + wid] = v;
-  }
+  for (int rr = HF::R0; rr < HF::R1; ++rr)
 #pragma unroll
-  for (int i = 0; i < 18; ++i) {
-    const double v = warp_sum(ag[i]);
-    if (lane == 0) sred[(54 + i) * nw + wid] = v;
+    for (int l = rr; l < 9; ++l) {
+      const double s = warp_sum(v[HF::v_index(rr, l)]);
+      if (lane == 0) sred[tri9(rr, l) * 4 + wp] = s;
+    }
+#pragma unroll
+  for (int j = HF::J0; j < HF::J1; ++j) {
+    const double a = warp_sum(cs[j - HF::J0]), b = warp_sum(g[j - HF::J0]), d = warp_sum(h[j - HF::J0]);
+    if (lane == 0) {
+      sred[(45 + j) * 4 + wp] = a;
+      sred[(54 + j) * 4 + wp] = b;
+      sred[(63 + j) * 4 + wp] = d;
+    }
   }
+}
+
+// Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
+// into acc_out[c][72] (float64). The 8 warps form 4 pairs; both warps of a pair read
+// the same observations (the second read mostly hits L1) and each keeps half of the
+// sums (36 float64 accumulators instead of 72: 16 warps per SM instead of 8). The four
+// pairs' sums are added in pair order. kHbb: the camera block is the Hbb block sum
+// Jc^T Jc (M = I below) instead of the Schur block; the base of
+// SCHUR_POWER_SERIES_EXPANSION.
+// CTAs per SM the camera reduction is compiled for: 2 (128 registers) with the float32
+// store; the float64 store's records need more registers, 1 (no spills).
+template <typename T> struct CamMinBlocks { static constexpr int v = sizeof(T) == 4 ? 2 : 1; };
+
+template <typename T, bool kDup, bool kHbb = false>
+__global__ void __launch_bounds__(kCamBlock, CamMinBlocks<T>::v) k_camera_reduce(ceres_b200_ba_t ba,
+                                                                                double* __restrict__ acc_out) {
+  __shared__ double sred[kCamAcc * 4];
+  const int c = blockIdx.x;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool cconst = ba.cam_const[c] != 0;
+  if (w & 1) camera_reduce_half<T, kDup, kHbb, 1>(ba, c, cconst, w >> 1, lane, sred);
+  else camera_reduce_half<T, kDup, kHbb, 0>(ba, c, cconst, w >> 1, lane, sred);
   __syncthreads();
-  for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x) {
-    double sum = 0.0;
-    for (int w = 0; w < nw; ++w) sum += sred[i * nw + w];
-    acc_out[(size_t)c * kCamAcc + i] = sum;
-  }
+  for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x)
+    acc_out[(size_t)c * kCamAcc + i] = ((sred[4 * i] + sred[4 * i + 1]) + sred[4 * i + 2]) + sred[4 * i + 3];
 }
 
 // Phase 2: one warp per camera forms the damping, the reduced rhs, the gradient stats
@@ -696,7 +736,16 @@ __device__ __forceinline__ int camera_pass_item(const ceres_b200_ba_t& ba, const
   const int c = it.x, e0 = it.y;
   const int e1 = min(e0 + CERES_B200_CAM_ITEM, ba.cam_offsets[c + 1]);
   const T* __restrict__ cm = reinterpret_cast<const T*>(ba.cm_jac);
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);
+  // the record of entry e: streamed from the camera-major copy, or gathered by slot
+  auto load = [&](int e, T rv[kRec], int& q) {
+    const int2 en = ents[e];
+    q = en.y;
+    if (cm != nullptr) load_rec(cm, (size_t)e, rv);
+    else if constexpr (sizeof(T) == 4) load_rec128(jac, (size_t)en.x, rv);
+    else load_rec(jac, (size_t)en.x, rv);
+  };
   A pc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
@@ -727,17 +776,15 @@ __device__ __forceinline__ int camera_pass_item(const ceres_b200_ba_t& ba, const
     T rv[kUnroll][kRec];
     int q[kUnroll];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      load_rec(cm, (size_t)(e + 32 * u), rv[u]);
-      q[u] = ents[e + 32 * u].y;
-    }
+    for (int u = 0; u < kUnroll; ++u) load(e + 32 * u, rv[u], q[u]);
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) one(rv[u], q[u]);
   }
   for (; e < e1; e += 32) {
     T rv[kRec];
-    load_rec(cm, (size_t)e, rv);
-    one(rv, ents[e].y);
+    int q;
+    load(e, rv, q);
+    one(rv, q);
   }
 #pragma unroll
   for (int j = 0; j < 9; ++j) y[j] = warp_sum_any(y[j]);
@@ -1612,9 +1659,8 @@ bool valid(const ceres_b200_ba_t* ba) {
     return false;
   if ((reinterpret_cast<uintptr_t>(ba->jac) & 31) != 0) return false;  // 256-bit record loads
   if (ba->num_observations > 0) {
-    if (!ba->slot_pos || !ba->cm_jac || !ba->cam_entries || !ba->cam_items || !ba->items || ba->num_items <= 0)
-      return false;
-    if ((reinterpret_cast<uintptr_t>(ba->cm_jac) & 31) != 0) return false;
+    if (!ba->cam_entries || !ba->cam_items || !ba->items || ba->num_items <= 0) return false;
+    if (ba->cm_jac && (!ba->slot_pos || (reinterpret_cast<uintptr_t>(ba->cm_jac) & 31) != 0)) return false;
   }
   if (ba->num_items < 0) return false;
   return true;

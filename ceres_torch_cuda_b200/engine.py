@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import os
 import time
 from dataclasses import dataclass
 
@@ -152,7 +153,7 @@ class BAEngine:
     def __init__(self, cameras: torch.Tensor, points: torch.Tensor, observations: torch.Tensor,
                  camera_index: torch.Tensor, point_index: torch.Tensor, *, loss=None,
                  camera_constant: torch.Tensor | None = None, point_constant: torch.Tensor | None = None,
-                 precision: str = "fp64", layout: Layout | None = None):
+                 precision: str = "fp64", layout: Layout | None = None, camera_copy: bool | None = None):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         if cameras.device.type != "cuda":
@@ -202,7 +203,11 @@ class BAEngine:
         self.cand_points = torch.zeros((npq, 3), **f64)
         self.best_points = torch.zeros((npq, 3), **f64)
         self.jac = torch.zeros((nslot, 24), dtype=T, device=dev)
-        self.cm_jac = torch.zeros((max(self.no, 1), 24), dtype=T, device=dev)
+        # camera-major copy of the Jacobian store (the camera-side passes stream it instead
+        # of gathering records by slot); CERES_B200_CAMERA_COPY=0 leaves it out
+        self.camera_copy = os.environ.get("CERES_B200_CAMERA_COPY", "1") != "0" if camera_copy is None \
+            else bool(camera_copy)
+        self.cm_jac = torch.zeros((max(self.no, 1), 24), dtype=T, device=dev) if self.camera_copy else None
         self.res = torch.zeros((nslot, 2), **f64)
         self.point_raw = torch.zeros((npq, 9), **f64)
         self.winv = torch.zeros((npq, 6), dtype=T, device=dev)

@@ -97,9 +97,10 @@ enum {
  *
  * Jacobian records are 24 scalars per slot (camera row 0 [9], camera row 1
  * [9], point row 0 [3], point row 1 [3]) of float (FP32) or double (FP64).
- * The evaluation writes each record twice: at its slot (point-major) and at its
- * camera-major position (cm_jac[e], e the entry's index in cam_entries), so
- * that the camera-side passes stream their records instead of gathering them.
+ * When cm_jac is set, the evaluation writes each record twice: at its slot
+ * (point-major) and at its camera-major position (cm_jac[e], e the entry's index
+ * in cam_entries), and the camera-side passes stream the copy; with cm_jac null
+ * they gather the records by slot.
  * Camera work items cut every camera's entries into runs of at most
  * CERES_B200_CAM_ITEM entries; item i = (camera, first entry) covers entries
  * first .. min(first + CERES_B200_CAM_ITEM, cam_offsets[camera + 1]) - 1, and
@@ -164,7 +165,7 @@ typedef struct ceres_b200_ba_t {
 
   /* camera-major copy of the Jacobian store and the camera work items */
   const int32_t* slot_pos;     /* [num_slots] camera-major position of the slot's observation, -1 padding */
-  void* cm_jac;                /* [num_observations][24] float or double, 32-byte aligned */
+  void* cm_jac;                /* [num_observations][24] float or double, 32-byte aligned, or null */
   const int32_t* cam_items;    /* [num_cameras + 1] first item of each camera */
   const int32_t* items;        /* [num_items][2] (camera, first entry) */
   int32_t num_items;
