@@ -120,3 +120,78 @@ def test_batch_with_loss_and_constant_camera():
     for r, g, pb, ps in zip(ref, got, batch, singles):
         np.testing.assert_allclose(g.final_cost, r.final_cost, rtol=1e-8)
         np.testing.assert_array_equal(pb.cameras[0].cpu().numpy(), ps.cameras[0].cpu().numpy())
+
+
+def _oracle_solve(d, loss_spec=("trivial",), max_iterations=30):
+    from oracle import ba_oracle as O
+    p = O.OracleProblem(d.cameras, d.points, d.observations, d.camera_index, d.point_index, loss_spec)
+    return O.solve(p, O.OracleOptions(linear_solver_type="ITERATIVE_SCHUR", preconditioner_type="SCHUR_JACOBI",
+                                      max_num_iterations=max_iterations))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_matches_the_reference_fixtures(precision):
+    """Each batched problem against the reference's own recorded solve of it (ceres-torch's
+    float64 tc.solve, ITERATIVE_SCHUR + SCHUR_JACOBI, default tolerances): the same
+    termination, iteration count within +-2 and final cost within 1e-8 (float64) or 1e-6
+    (mixed) relative. Problems sharing a loss form one batch."""
+    import ceres_torch_cuda_b200 as tc
+    from tests import _golden as G
+
+    groups = {("trivial",): ["ba_small_iterative"], ("cauchy", 2.0): ["ba_cauchy", "config2_small"],
+              ("huber", 1.0): ["config1_small"]}
+    rtol = 1e-8 if precision == "fp64" else 1e-6
+    for spec, names in groups.items():
+        loss = None if spec[0] == "trivial" else (tc.CauchyLoss if spec[0] == "cauchy" else tc.HuberLoss)(spec[1])
+        ds = [G.load(n) for n in names]
+        probs = [tc.BundleAdjustmentProblem.from_arrays(d["cameras"], d["points"], d["observations"],
+                                                        d["camera_index"], d["point_index"], loss=loss) for d in ds]
+        opts = tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
+                                preconditioner_type=tc.PreconditionerType.SCHUR_JACOBI,
+                                max_num_iterations=ds[0]["meta"]["max_num_iterations"])
+        got = tc.solve_batch(opts, probs, precision=precision)
+        for name, d, g in zip(names, ds, got):
+            meta = d["meta"]
+            assert g.termination_type.value == meta["termination"], (name, g.message)
+            assert abs(len(g.iterations) - meta["num_iterations"]) <= 2, (name, len(g.iterations))
+            np.testing.assert_allclose(g.final_cost, meta["final_cost"], rtol=rtol, err_msg=name)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_of_configuration3_size_instances_matches_the_oracle(precision):
+    """Eight instances drawn like configuration 3 at its full size range (3-32 cameras,
+    up to 2,000 points, tracks of 3-8) in one launch against the float64 oracle:
+    final cost within 1e-8 (float64) or 1e-6 (mixed) relative, iteration count within
+    +-2."""
+    import ceres_torch_cuda_b200 as tc
+
+    datas = S.make_batched_instances(8, seed=33, max_points=2000)
+    assert max(d.num_points for d in datas) > 1000 and max(d.num_cameras for d in datas) > 16
+    got = tc.solve_batch(_options(), _problems(datas), precision=precision)
+    rtol = 1e-8 if precision == "fp64" else 1e-6
+    for d, g in zip(datas, got):
+        ref = _oracle_solve(d)
+        np.testing.assert_allclose(g.final_cost, ref.final_cost, rtol=rtol)
+        assert abs(len(g.iterations) - len(ref.iterations)) <= 2
+
+
+@pytest.mark.gpu
+def test_batch_autotune_shapes_give_the_same_float64_results():
+    """Every CTA shape the autotuner chooses from gives the same float64 solves (final
+    cost 1e-10 relative), and autotune returns one of them."""
+    import ceres_torch_cuda_b200 as tc
+    from ceres_torch_cuda_b200 import batch as B
+
+    datas = S.make_batched_instances(4, seed=44, max_points=200)
+    results = {}
+    for shape in B.SHAPES:
+        solver = tc.BatchSolver(_problems(datas), _options(), precision="fp64")
+        solver.launch(*shape)
+        results[shape] = [s.final_cost for s in solver.summaries()]
+    first = next(iter(results.values()))
+    for shape, costs in results.items():
+        np.testing.assert_allclose(costs, first, rtol=1e-10, err_msg=str(shape))
+    chosen = B.autotune(_options(), _problems(datas), precision="fp64")
+    assert tuple(chosen) in {tuple(s) for s in B.SHAPES}

@@ -59,3 +59,19 @@ def test_server_respects_memory_budget_and_stream_replay():
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
     for r in stats["requests_list"]:
         assert r.summary.termination_type in (tc.TerminationType.CONVERGENCE, tc.TerminationType.NO_CONVERGENCE)
+
+
+def test_mixed_server_results_equal_alone():
+    """Mixed precision in the served mix: each request's result equals the same request
+    solved alone in its own launch (final cost within 1e-6 relative, iteration count
+    within +-2), with several batches overlapping on the GPU."""
+    tc, opts, _, probs = _setup(count=12, seed=8)
+    from ceres_torch_cuda_b200.serving import BAServer
+    server = BAServer(opts, precision="mixed", max_inflight=3, max_batch=3, cluster_size=1, min_batch=1)
+    reqs = [server.submit(p) for p in probs()]
+    server.drain()
+    assert server.peak_inflight >= 2
+    alone = [tc.solve_batch(opts, [p], precision="mixed", cluster_size=1)[0] for p in probs()]
+    for r, a in zip(reqs, alone):
+        np.testing.assert_allclose(r.summary.final_cost, a.final_cost, rtol=1e-6)
+        assert abs(len(r.summary.iterations) - len(a.iterations)) <= 2
