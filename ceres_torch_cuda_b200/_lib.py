@@ -32,7 +32,7 @@ DEVERR_BARRIER = 2
 DEVERR_NOT_PD = 4
 
 LOSS_TRIVIAL, LOSS_HUBER, LOSS_SOFTLONE, LOSS_CAUCHY, LOSS_ARCTAN, LOSS_TOLERANT, LOSS_TUKEY = range(7)
-PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_SCHUR_JACOBI, PRECOND_SCHUR_POWER_SERIES = range(4)
+PRECOND_IDENTITY, PRECOND_JACOBI, PRECOND_SCHUR_JACOBI, PRECOND_SCHUR_POWER_SERIES, PRECOND_CLUSTER = range(5)
 PRECOND_FLAG_SPSE_BASE = 0x100  # camera_assemble: also build the Hbb blocks of the SPSE initial point
 FP64, FP32 = 0, 1
 CAM_ITEM = 256  # CERES_B200_CAM_ITEM: entries per camera work item
@@ -115,6 +115,21 @@ class BatchStruct(ctypes.Structure):
 
 _PB = ctypes.POINTER(BatchStruct)
 
+
+class ClusterStruct(ctypes.Structure):
+    """ceres_b200_clusters_t: the visibility-cluster preconditioner's index arrays and
+    storage (device pointers)."""
+    _fields_ = [
+        ("num_components", c_int32), ("num_pairs", c_int32), ("max_dim", c_int32), ("tridiagonal", c_int32),
+        ("num_elements", c_int64),
+        ("pairs", c_void_p), ("entries", c_void_p), ("cam_comp", c_void_p), ("cam_pos", c_void_p),
+        ("cam_cluster", c_void_p), ("comp_cams", c_void_p), ("comp_cam_off", c_void_p), ("comp_base", c_void_p),
+        ("comp_piv", c_void_p), ("inv", c_void_p), ("piv", c_void_p), ("flags", c_void_p),
+    ]
+
+
+_PC = ctypes.POINTER(ClusterStruct)
+
 # name -> (restype, argtypes); every symbol include/ceres_b200.h declares
 SIGNATURES = {
     "ceres_b200_abi_version": (c_int32, []),
@@ -138,6 +153,9 @@ SIGNATURES = {
     "ceres_b200_debug_barrier_timeout": (c_int32, [c_void_p, ctypes.c_uint32, c_void_p]),
     "ceres_b200_ba_schur_matrix": (c_int32, [_P, c_void_p, c_void_p]),
     "ceres_b200_dense_spd_inverse": (c_int32, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]),
+    "ceres_b200_clusters_struct_bytes": (c_int32, []),
+    "ceres_b200_ba_cluster_factor": (c_int32, [_P, _PC, c_void_p]),
+    "ceres_b200_ba_pcg_cluster": (c_int32, [_P, _PC, c_int32, c_int32, c_double, c_int32, c_void_p]),
 }
 
 _LIB: ctypes.CDLL | None = None
@@ -173,6 +191,8 @@ def load(*, build_if_missing: bool = False) -> ctypes.CDLL:
         raise NativeLibraryError("ceres_b200_ba_t layout differs between the library and this binding")
     if lib.ceres_b200_batch_struct_bytes() != ctypes.sizeof(BatchStruct):
         raise NativeLibraryError("ceres_b200_batch_t layout differs between the library and this binding")
+    if lib.ceres_b200_clusters_struct_bytes() != ctypes.sizeof(ClusterStruct):
+        raise NativeLibraryError("ceres_b200_clusters_t layout differs between the library and this binding")
     _LIB = lib
     return lib
 

@@ -69,9 +69,10 @@ struct Prob {
 struct Smem {
   double* red;    // [8 * kMaxWarps]
   double* part;   // [8]: this CTA's partial sums for cluster reductions
-  void* ps;       // [9 * max_cameras] T: the PCG direction (all cameras)
-  void* ys;       // [9 * max_cameras] T: this CTA's product accumulator
-  double* y64;    // [9 * max_cameras]: float64 product accumulator (refinement)
+  double* ps;     // [9 * max_cameras]: the PCG direction (all cameras)
+  double* ys;     // [9 * max_cameras]: this CTA's product accumulator
+  double* y64;    // the refinement's product accumulator (the same memory as ys: the
+                  // refinement runs between PCG solves)
 };
 
 // Reduce NV values over the cluster (sum, or max where max_mask has the bit) and hand
@@ -548,9 +549,12 @@ __device__ PcgOut cl_pcg(const ceres_b200_batch_t& B, const Prob& P, const Ctx& 
   double* AP = B.pcg + 5 * N + o;
   const T* Minv = reinterpret_cast<const T*>(B.precond) + 81 * (size_t)P.cam0;
   const double* D = B.cam_diag + o;
-  T* ps = reinterpret_cast<T*>(S.ps);
-  T* ys = reinterpret_cast<T*>(S.ys);
-  const double eps = Eps<T>::v();
+  // the products stream the store in T and compute in float64 (float32 arithmetic adds
+  // errors of 1e-7 |U| |p| per product that swamp the small eigenvalues of S once the
+  // LM damping has decayed, and costs the same time)
+  double* ps = S.ps;
+  double* ys = S.ys;
+  const double eps = kEps64;  // float64 vectors and arithmetic in both precisions
 
   for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) { Xv[j] = 0.0; R[j] = ldx(rhs + j); }
   __syncthreads();
@@ -581,18 +585,18 @@ __device__ PcgOut cl_pcg(const ceres_b200_batch_t& B, const Prob& P, const Ctx& 
       // every CTA builds the whole direction in shared memory; the owner stores its part
       for (int j = threadIdx.x; j < n; j += blockDim.x) {
         const double pv = (k == 0) ? ldx(Z + j) : ldx(Z + j) + beta * ldx(Pold + j);
-        ps[j] = (T)pv;
-        ys[j] = (T)0;
+        ps[j] = pv;
+        ys[j] = 0.0;
         if (j >= j0 && j < j1) Pnew[j] = pv;
       }
       cur = nxt;
       __syncthreads();
-      cl_schur_product<T, T, T, false>(B, P, X, ps, ys);
+      cl_schur_product<T, double, double, false>(B, P, X, ps, ys);
       csync();  // every CTA's product accumulator is complete
       double v1[1] = {0.0};
       for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
         double y = 0.0;
-        for (int r = 0; r < X.G; ++r) y += (double)remote(ys, r)[j];
+        for (int r = 0; r < X.G; ++r) y += remote(ys, r)[j];
         y += ldx(D + j) * Pnew[j];
         AP[j] = y;
         v1[0] += Pnew[j] * y;
@@ -980,9 +984,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_batch_solve(ceres_b200
   Smem S;
   S.red = red;
   S.part = part;
-  S.y64 = reinterpret_cast<double*>(smem_raw);
-  S.ps = smem_raw + (sizeof(T) == sizeof(float) ? vec * sizeof(double) : 0);
-  S.ys = reinterpret_cast<unsigned char*>(S.ps) + vec * sizeof(T);
+  S.ps = reinterpret_cast<double*>(smem_raw);
+  S.ys = S.ps + vec;
+  S.y64 = S.ys;
   for (;;) {
     if (X.rank == 0 && threadIdx.x == 0) next = (int)atomicAdd(B.queue, 1u);
     csync();
@@ -1046,7 +1050,7 @@ int ceres_b200_batch_solve(const ceres_b200_batch_t* batch, int threads_per_cta,
   BatchKernel kern = f32 ? batch_kernel<float>(threads, ctas) : batch_kernel<double>(threads, ctas);
   if (!kern) return CERES_B200_EINVAL;
   const size_t vec = (size_t)((9 * B.max_cameras + 3) & ~3);
-  const size_t smem = f32 ? vec * (sizeof(double) + 2 * sizeof(float)) : vec * 2 * sizeof(double);
+  const size_t smem = vec * 2 * sizeof(double);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return CERES_B200_ECUDA;
   int sms = 0, optin = 0;

@@ -220,8 +220,11 @@ k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ fram
         W[3] += a[1] * a[1] + b[1] * b[1];
         W[4] += a[1] * a[2] + b[1] * b[2];
         W[5] += a[2] * a[2] + b[2] * b[2];
+        // the gradient J_p^T r from the float64 Jacobian before rounding: with the float32
+        // store, a gradient summed from rounded values moves the point where the step
+        // vanishes along weakly determined directions (a point's depth)
 #pragma unroll
-        for (int m = 0; m < 3; ++m) g[m] += a[m] * o.r[0] + b[m] * o.r[1];
+        for (int m = 0; m < 3; ++m) g[m] += o.jp[0][m] * o.r[0] + o.jp[1][m] * o.r[1];
       }
     }
     if (kJac) {
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(kWarpBlock) k_point_assemble(ceres_b200_ba_t b
 // Schur diagonal block before damping), the camera column sums, the gradient and
 // the reduced rhs over the camera's observations, then forms the preconditioner.
 // ======================================================================================
-constexpr int kCamBlock = 256;  // 4 warp pairs per camera
+constexpr int kCamBlock = 128;
 constexpr int kCamAcc = 45 + 9 + 9 + 9;  // V (upper), colsum, g, h
 
 __device__ __forceinline__ int tri9(int j, int l) {  // upper-triangle index, j <= l
@@ -370,43 +373,33 @@ __device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T*
   for (int i = 0; i < 3; ++i) o.wg[i] = ba.winv_ga[3 * (size_t)ent.y + i];
 }
 
-// Sums of one half of the 72: rows R0..R1-1 of the Schur block's upper triangle and the
-// column sums, gradient and rhs entries J0..J1-1 (36 float64 each).
-template <int H> struct CamHalf {
-  static constexpr int R0 = H == 0 ? 0 : 3, R1 = H == 0 ? 3 : 9;
-  static constexpr int J0 = H == 0 ? 0 : 4, J1 = H == 0 ? 4 : 9;
-  static constexpr int NJ = J1 - J0;
-  static constexpr int NV = H == 0 ? 24 : 21;  // sum over the rows of 9 - r
-  // position of upper-triangle entry (r, l) among this half's entries
-  static __device__ __forceinline__ constexpr int v_index(int r, int l) {
-    return (r - R0) * 9 - ((r * (r - 1)) / 2 - (R0 * (R0 - 1)) / 2) + (l - r);
-  }
-};
-
-// One warp's half of a camera's sums over the observations of its warp pair (wp):
-// entries e0 + 32 wp + lane + 128 k. Lane sums reduced over the warp go to
-// sred[index * 4 + wp].
-template <typename T, bool kDup, bool kHbb, int H>
-__device__ __forceinline__ void camera_reduce_half(const ceres_b200_ba_t& ba, int c, bool cconst, int wp, int lane,
-                                                   double* __restrict__ sred) {
+// Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
+// into acc_out[c][72] (float64). kHbb: the camera block is the Hbb block sum Jc^T Jc
+// (M = I below) instead of the Schur block; the base of SCHUR_POWER_SERIES_EXPANSION.
+template <typename T, bool kDup, bool kHbb = false>
+__global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba, double* __restrict__ acc_out) {
   using A = double;
-  using HF = CamHalf<H>;
+  __shared__ double sred[kCamAcc * (kCamBlock / 32)];
+  const int c = blockIdx.x;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ cm = reinterpret_cast<const T*>(ba.cm_jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  A v[HF::NV];
-  double cs[HF::NJ], g[HF::NJ], h[HF::NJ];
+  A av[54];      // Schur block (upper triangle, 45), column sums (9)
+  double ag[18]; // gradient (9), reduced rhs (9)
 #pragma unroll
-  for (int i = 0; i < HF::NV; ++i) v[i] = 0.0;
+  for (int i = 0; i < 54; ++i) av[i] = (A)0;
 #pragma unroll
-  for (int i = 0; i < HF::NJ; ++i) { cs[i] = 0.0; g[i] = 0.0; h[i] = 0.0; }
+  for (int i = 0; i < 18; ++i) ag[i] = 0.0;
+  const bool cconst = ba.cam_const[c] != 0;
   const int e0 = ba.cam_offsets[c], e1 = ba.cam_offsets[c + 1];
   if (!cconst) {
     const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);
-    constexpr int stride = kCamBlock / 2;
-    const int first = e0 + 32 * wp + lane;
+    const int stride = blockDim.x;
+    const int first = e0 + threadIdx.x;
     // entries are read two observations ahead, so each observation waits for one
-    // gather (its data) instead of two (entry, then data)
+    // gather (its data) instead of two (entry, then data): 0.43 -> 0.39 ms on the
+    // 6.0M-observation problem (float32 store). Holding the next observation's data in
+    // registers as well spilled and ran slower.
     int2 en1 = first < e1 ? ents[first] : make_int2(0, 0);
     int2 en2 = first + stride < e1 ? ents[first + stride] : make_int2(0, 0);
     for (int e = first; e < e1; e += stride) {
@@ -436,26 +429,25 @@ __device__ __forceinline__ void camera_reduce_half(const ceres_b200_ba_t& ba, in
       const A B00 = P0[0] * jp0[0] + P0[1] * jp0[1] + P0[2] * jp0[2];
       const A B01 = P0[0] * jp1[0] + P0[1] * jp1[1] + P0[2] * jp1[2];
       const A B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
+      const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
+      const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
       const A M00 = kHbb ? (A)1 : (A)1 - B00, M01 = kHbb ? (A)0 : -B01, M11 = kHbb ? (A)1 : (A)1 - B11;
-      if (HF::NJ > 0) {
-        const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
-        const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
+      A K0[9], K1[9];
 #pragma unroll
-        for (int j = HF::J0; j < HF::J1; ++j) {
-          const double d0 = (double)rv[j], d1 = (double)rv[9 + j];
-          cs[j - HF::J0] += d0 * d0 + d1 * d1;
-          g[j - HF::J0] += d0 * r.x + d1 * r.y;
-          h[j - HF::J0] += d0 * (r.x + a0) + d1 * (r.y + a1);
-        }
+      for (int j = 0; j < 9; ++j) {
+        const A c0 = (A)rv[j], c1 = (A)rv[9 + j];
+        K0[j] = M00 * c0 + M01 * c1;
+        K1[j] = M01 * c0 + M11 * c1;
+        av[45 + j] += c0 * c0 + c1 * c1;
+        const double d0 = (double)rv[j], d1 = (double)rv[9 + j];
+        ag[j] += d0 * r.x + d1 * r.y;
+        ag[9 + j] += d0 * (r.x + a0) + d1 * (r.y + a1);
       }
 #pragma unroll
-      for (int l = HF::R0; l < 9; ++l) {
-        const A c0 = (A)rv[l], c1 = (A)rv[9 + l];
-        const A k0 = M00 * c0 + M01 * c1, k1 = M01 * c0 + M11 * c1;
+      for (int j = 0; j < 9; ++j)
 #pragma unroll
-        for (int rr = HF::R0; rr < HF::R1; ++rr)
-          if (rr <= l) v[HF::v_index(rr, l)] += (A)rv[rr] * k0 + (A)rv[9 + rr] * k1;
-      }
+        for (int l = j; l < 9; ++l) av[tri9(j, l)] += (A)rv[j] * K0[l] + (A)rv[9 + j] * K1[l];
+
       if (kDup && !kHbb) {
         // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
         const int sidx = q >> 5, ln = q & 31;
@@ -471,57 +463,33 @@ __device__ __forceinline__ void camera_reduce_half(const ceres_b200_ba_t& ba, in
           const A C10 = P1[0] * (A)rk[18] + P1[1] * (A)rk[19] + P1[2] * (A)rk[20];
           const A C11 = P1[0] * (A)rk[21] + P1[1] * (A)rk[22] + P1[2] * (A)rk[23];
 #pragma unroll
-          for (int rr = HF::R0; rr < HF::R1; ++rr) {
-            const A t0 = (A)rv[rr] * C00 + (A)rv[9 + rr] * C10;
-            const A t1 = (A)rv[rr] * C01 + (A)rv[9 + rr] * C11;
+          for (int j = 0; j < 9; ++j) {
+            const A t0 = (A)rv[j] * C00 + (A)rv[9 + j] * C10;
+            const A t1 = (A)rv[j] * C01 + (A)rv[9 + j] * C11;
 #pragma unroll
-            for (int l = rr; l < 9; ++l) v[HF::v_index(rr, l)] -= t0 * (A)rk[l] + t1 * (A)rk[9 + l];
+            for (int l = j; l < 9; ++l) av[tri9(j, l)] -= t0 * (A)rk[l] + t1 * (A)rk[9 + l];
           }
         }
       }
     }
   }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-  for (int rr = HF::R0; rr < HF::R1; ++rr)
-#pragma unroll
-    for (int l = rr; l < 9; ++l) {
-      const double s = warp_sum(v[HF::v_index(rr, l)]);
-      if (lane == 0) sred[tri9(rr, l) * 4 + wp] = s;
-    }
-#pragma unroll
-  for (int j = HF::J0; j < HF::J1; ++j) {
-    const double a = warp_sum(cs[j - HF::J0]), b = warp_sum(g[j - HF::J0]), d = warp_sum(h[j - HF::J0]);
-    if (lane == 0) {
-      sred[(45 + j) * 4 + wp] = a;
-      sred[(54 + j) * 4 + wp] = b;
-      sred[(63 + j) * 4 + wp] = d;
-    }
+  for (int i = 0; i < 54; ++i) {
+    const double v = warp_sum((double)av[i]);
+    if (lane == 0) sred[i * nw + wid] = v;
   }
-}
-
-// Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
-// into acc_out[c][72] (float64). The 8 warps form 4 pairs; both warps of a pair read
-// the same observations (the second read mostly hits L1) and each keeps half of the
-// sums (36 float64 accumulators instead of 72: 16 warps per SM instead of 8). The four
-// pairs' sums are added in pair order. kHbb: the camera block is the Hbb block sum
-// Jc^T Jc (M = I below) instead of the Schur block; the base of
-// SCHUR_POWER_SERIES_EXPANSION.
-// CTAs per SM the camera reduction is compiled for: 2 (128 registers) with the float32
-// store; the float64 store's records need more registers, 1 (no spills).
-template <typename T> struct CamMinBlocks { static constexpr int v = sizeof(T) == 4 ? 2 : 1; };
-
-template <typename T, bool kDup, bool kHbb = false>
-__global__ void __launch_bounds__(kCamBlock, CamMinBlocks<T>::v) k_camera_reduce(ceres_b200_ba_t ba,
-                                                                                double* __restrict__ acc_out) {
-  __shared__ double sred[kCamAcc * 4];
-  const int c = blockIdx.x;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool cconst = ba.cam_const[c] != 0;
-  if (w & 1) camera_reduce_half<T, kDup, kHbb, 1>(ba, c, cconst, w >> 1, lane, sred);
-  else camera_reduce_half<T, kDup, kHbb, 0>(ba, c, cconst, w >> 1, lane, sred);
+#pragma unroll
+  for (int i = 0; i < 18; ++i) {
+    const double v = warp_sum(ag[i]);
+    if (lane == 0) sred[(54 + i) * nw + wid] = v;
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x)
-    acc_out[(size_t)c * kCamAcc + i] = ((sred[4 * i] + sred[4 * i + 1]) + sred[4 * i + 2]) + sred[4 * i + 3];
+  for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x) {
+    double sum = 0.0;
+    for (int w = 0; w < nw; ++w) sum += sred[i * nw + w];
+    acc_out[(size_t)c * kCamAcc + i] = sum;
+  }
 }
 
 // Phase 2: one warp per camera forms the damping, the reduced rhs, the gradient stats
@@ -867,6 +835,23 @@ __global__ void k_fold_items(ceres_b200_ba_t ba, const double* __restrict__ part
 // Cooperative persistent PCG (linear.py:1216-1256) on the reduced camera system, with
 // the float64 refinement of the float32 store in the same launch.
 // ======================================================================================
+// Device view of ceres_b200_clusters_t (the visibility-cluster preconditioner).
+struct ClusterArgs {
+  int num_components, num_pairs, max_dim, tridiagonal;
+  const int2* pairs;
+  const int2* entries;
+  const int* cam_comp;
+  const int* cam_pos;
+  const int* cam_cluster;
+  const int* comp_cams;
+  const int* comp_cam_off;
+  const long long* comp_base;
+  const long long* comp_piv;
+  double* inv;
+  double* piv;
+  unsigned* flags;
+};
+
 struct PcgArgs {
   const double* rhs;   // [n] right-hand side (float64)
   double* x_out;       // [n] solution (float64)
@@ -874,7 +859,7 @@ struct PcgArgs {
   double tolerance, eps;
   int n;               // 9 * num_cameras
   int cams_per_cta;
-  int smem_vectors;    // 1: a copy of p (in T) in shared memory for the product
+  int smem_vectors;    // 1: a copy of p in shared memory for the product
   double* sv;          // [num_points][3] point-pass results s_q
   double* item_part;   // [num_items][9] camera-pass item sums
   double* part_b;      // [G]
@@ -889,6 +874,9 @@ struct PcgArgs {
   int series_terms;        // max_num_spse_iterations (>= 1)
   double series_tol;       // spse_tolerance
   double* part_s;          // [G][2] partials of the series norms and of |r|^2
+  // CLUSTER_JACOBI / CLUSTER_TRIDIAGONAL: z = M^-1 r with the component inverses of cl
+  int cluster;
+  ClusterArgs cl;
 };
 
 constexpr int kPcgBlock = 512;
@@ -908,6 +896,32 @@ __device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const 
 #pragma unroll
     for (int j = 0; j < 9; ++j) s += (double)M[i * 9 + j] * rr[j];
     z[9 * (size_t)c + i] = s;
+  }
+}
+
+// z_j = (M^-1 r)_j for the entries j in [j0, j1) (whole cameras): one warp per entry,
+// the lanes over the columns of the camera's component (a fixed shuffle tree sums them,
+// so the result does not depend on the schedule). r is complete in global memory (a
+// grid barrier precedes the call). Cameras outside every component get z = 0.
+__device__ __forceinline__ void cluster_apply(const ClusterArgs& cl, const double* __restrict__ r,
+                                              double* __restrict__ z, int j0, int j1) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  for (int j = j0 + (threadIdx.x >> 5); j < j1; j += nwarps) {
+    const int c = j / 9, m = j - 9 * c;
+    const int comp = cl.cam_comp[c];
+    double acc = 0.0;
+    if (comp >= 0) {
+      const int cam0 = cl.comp_cam_off[comp];
+      const int dim = 9 * (cl.comp_cam_off[comp + 1] - cam0);
+      const double* __restrict__ row = cl.inv + cl.comp_base[comp] + (size_t)(9 * cl.cam_pos[c] + m) * dim;
+      for (int col = lane; col < dim; col += 32) {
+        const int k = col / 9;
+        acc += row[col] * ld_cross(r + 9 * (size_t)cl.comp_cams[cam0 + k] + (col - 9 * k));
+      }
+      acc = warp_sum(acc);
+    }
+    if (lane == 0) z[j] = acc;
   }
 }
 
@@ -946,9 +960,14 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   __shared__ double bcast[4];
   __shared__ int slice_counter;
   const int n = a.n;
-  T* ps = reinterpret_cast<T*>(smem_raw);
-  // PCG state vectors are float64 in both precisions; the products S p and E p stream
-  // the Jacobian store in T with T arithmetic.
+  double* ps = reinterpret_cast<double*>(smem_raw);
+  // PCG state vectors are float64 in both precisions, and so is the arithmetic of the
+  // products S p and E p: they stream the Jacobian store in T (half the bytes when T is
+  // float) and compute in float64. Float32 arithmetic would cost the same time (the
+  // passes are bound by the store's bytes) but adds errors of 1e-7 |U| |p| to each
+  // product, which swamp the small eigenvalues of S once the LM damping has decayed:
+  // the steps then stop converging in the weakly determined directions and the solve
+  // ends above the float64 minimum.
   double* __restrict__ X = reinterpret_cast<double*>(ba.pcg_x);
   double* __restrict__ R = reinterpret_cast<double*>(ba.pcg_r);
   double* __restrict__ Z = reinterpret_cast<double*>(ba.pcg_z);
@@ -970,27 +989,26 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     if (threadIdx.x == 0) slice_counter = 0;
     __syncthreads();
     for (int s = next_cta_slice(&slice_counter, ba.num_slices); s >= 0; s = next_cta_slice(&slice_counter, ba.num_slices)) {
-      if (kind == kProdS64) point_pass_slice<T, double, double, true>(ba, V, a.sv, s, lane);
-      else if (a.smem_vectors) point_pass_slice<T, T, T, false>(ba, ps, a.sv, s, lane);
-      else point_pass_slice<T, double, T, true>(ba, V, a.sv, s, lane);
+      if (kind != kProdS64 && a.smem_vectors) point_pass_slice<T, double, double, false>(ba, ps, a.sv, s, lane);
+      else point_pass_slice<T, double, double, true>(ba, V, a.sv, s, lane);
     }
   };
   // camera pass over the grid's warps; returns this thread's share of
   // sum_items V_c . y_item (when with_dot)
   auto camera_pass_all = [&](const double* V, int kind, bool with_dot) -> double {
     const double* dp = with_dot ? V : nullptr;
-    if (kind == kProdS64) return camera_pass<T, double, double, true, false>(ba, V, a.sv, a.item_part, dp, gw, nw);
     if (kind == kProdE) {
-      if (a.smem_vectors) return camera_pass<T, T, T, false, true>(ba, ps, a.sv, a.item_part, dp, gw, nw);
-      return camera_pass<T, double, T, true, true>(ba, V, a.sv, a.item_part, dp, gw, nw);
+      if (a.smem_vectors) return camera_pass<T, double, double, false, true>(ba, ps, a.sv, a.item_part, dp, gw, nw);
+      return camera_pass<T, double, double, true, true>(ba, V, a.sv, a.item_part, dp, gw, nw);
     }
-    if (a.smem_vectors) return camera_pass<T, T, T, false, false>(ba, ps, a.sv, a.item_part, dp, gw, nw);
-    return camera_pass<T, double, T, true, false>(ba, V, a.sv, a.item_part, dp, gw, nw);
+    if (kind != kProdS64 && a.smem_vectors)
+      return camera_pass<T, double, double, false, false>(ba, ps, a.sv, a.item_part, dp, gw, nw);
+    return camera_pass<T, double, double, true, false>(ba, V, a.sv, a.item_part, dp, gw, nw);
   };
   // p (complete in global memory, read through L2) into shared memory as T
   auto stage_p = [&](const double* V) {
     if (a.smem_vectors)
-      for (int j = threadIdx.x; j < n; j += blockDim.x) ps[j] = (T)ld_cross(V + j);
+      for (int j = threadIdx.x; j < n; j += blockDim.x) ps[j] = ld_cross(V + j);
     __syncthreads();
   };
 
@@ -1064,6 +1082,9 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
       __syncthreads();
       if (a.precond_series) {
         if (!series(Minv, R, Z, Pbuf + n, AP)) return false;
+      } else if (a.cluster) {
+        if (!grid_sync(gb)) return false;  // r of every camera
+        cluster_apply(a.cl, R, Z, j0, j1);
       } else {
         for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
       }
@@ -1113,7 +1134,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
 #pragma unroll 4
           for (int j = threadIdx.x; j < n; j += blockDim.x) {
             const double pv = (k == 0) ? ld_cross(Z + j) : ld_cross(Z + j) + beta * ld_cross(Pold + j);
-            ps[j] = (T)pv;
+            ps[j] = pv;
             if (j >= j0 && j < j1) Pnew[j] = pv;
           }
           __syncthreads();
@@ -1195,8 +1216,13 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
             X[j] = X[j] + alpha * Pnew[j];
             R[j] = R[j] - alpha * AP[j];
           }
-          __syncthreads();
-          for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+          if (a.cluster) {
+            if (!grid_sync(gb)) return false;  // r of every camera
+            cluster_apply(a.cl, R, Z, j0, j1);
+          } else {
+            __syncthreads();
+            for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(Minv, R, Z, c);
+          }
           __syncthreads();
           double v[2] = {0.0, 0.0};
           for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
@@ -1642,6 +1668,194 @@ __global__ void k_barrier_probe(GridBarrier gb, int absent_cta) {
 }
 
 // ======================================================================================
+// Visibility-cluster preconditioner (linear.py:1032-1085): S kept on the cluster block
+// pairs, one dense matrix per component, inverted by the symmetric sweep operator.
+// ======================================================================================
+// One warp per kept pair (a, b), a <= b, writes the 9 x 9 block S_ab and its transpose
+// into the component's matrix. A diagonal block is camera_assemble's damped Schur block
+// (V_a from its camera sums, plus D_a): the block SCHUR_JACOBI inverts. An off-diagonal
+// block is -sum over the points q seen by both cameras of G_a,q W_q^-1 G_b,q^T, with
+// G_c,q = sum of Jc^T Jp over camera c's observations of q (float64 arithmetic on the
+// store); the shared points are taken in point order, so the block does not depend on
+// the schedule. Lane l holds entries l, l + 32, l + 64 of the block (row-major); the
+// 9 x 3 products go through the warp's shared memory. With pass 1 (the rebuild after a
+// kept matrix that was not positive definite) the blocks between different clusters
+// are halved (linear.py:1059-1072).
+constexpr int kClusterWarps = kWarpBlock / 32;
+
+template <typename T>
+__global__ void __launch_bounds__(kWarpBlock) k_cluster_assemble(ceres_b200_ba_t ba, ClusterArgs cl,
+                                                                 const double* __restrict__ cam_acc, int pass) {
+  if (pass == 1 && *reinterpret_cast<volatile unsigned*>(cl.flags) == 0u) return;
+  __shared__ double sg[kClusterWarps][3][27];  // G_a, G_b, G_a W^-1 of the current point
+  const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
+  const int2* __restrict__ ents = cl.entries;
+  double* Ga = sg[wid][0];
+  double* Gb = sg[wid][1];
+  double* Ha = sg[wid][2];
+  const int gi = lane / 3, gk = lane - 3 * (lane / 3);  // lane < 27: G entry (row gi, column gk)
+  // G[gi][gk] over the observations [e0, e1) of one camera and one point
+  auto group_g = [&](int e0, int e1) -> double {
+    double g = 0.0;
+    if (lane < 27) {
+      for (int e = e0; e < e1; ++e) {
+        const T* rv = jac + (size_t)kRec * (size_t)ents[e].x;
+        g += (double)rv[gi] * (double)rv[18 + gk] + (double)rv[9 + gi] * (double)rv[21 + gk];
+      }
+    }
+    return g;
+  };
+  for (int pi = gw; pi < cl.num_pairs; pi += nw) {
+    const int2 pr = cl.pairs[pi];
+    const int a = pr.x, b = pr.y;
+    const int comp = cl.cam_comp[a];
+    if (comp < 0 || cl.cam_comp[b] != comp) continue;  // uniform in the warp
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (a != b) {
+      const int ea0 = ba.cam_offsets[a], ea1 = ba.cam_offsets[a + 1];
+      const int eb0 = ba.cam_offsets[b], eb1 = ba.cam_offsets[b + 1];
+      for (int base = ea0; base < ea1; base += 32) {
+        // lane: the entry base + lane; the first entry of a point group looks the point
+        // up in b's list (sorted by point lane)
+        const int e = base + lane;
+        int q = -1, lo = eb1;
+        bool hit = false;
+        if (e < ea1) {
+          q = ents[e].y;
+          if (e == ea0 || ents[e - 1].y != q) {
+            int l = eb0, h = eb1;
+            while (l < h) {
+              const int mid = (l + h) >> 1;
+              if (ents[mid].y < q) l = mid + 1;
+              else h = mid;
+            }
+            lo = l;
+            hit = lo < eb1 && ents[lo].y == q;
+          }
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, hit);
+        while (mask) {
+          const int src = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const int qs = __shfl_sync(0xffffffffu, q, src);
+          const int ga = __shfl_sync(0xffffffffu, e, src);
+          const int gb = __shfl_sync(0xffffffffu, lo, src);
+          int ga1 = ga + 1, gb1 = gb + 1;
+          while (ga1 < ea1 && ents[ga1].y == qs) ++ga1;
+          while (gb1 < eb1 && ents[gb1].y == qs) ++gb1;
+          const double va = group_g(ga, ga1), vb = group_g(gb, gb1);
+          if (lane < 27) { Ga[lane] = va; Gb[lane] = vb; }
+          __syncwarp();
+          if (lane < 27) {  // (G_a W^-1)[gi][gk], W^-1 symmetric (6 values)
+            const T* w = winv + 6 * (size_t)qs;
+            const int c0 = gk == 0 ? 0 : (gk == 1 ? 1 : 2);
+            const int c1 = gk == 0 ? 1 : (gk == 1 ? 3 : 4);
+            const int c2 = gk == 0 ? 2 : (gk == 1 ? 4 : 5);
+            Ha[lane] = Ga[3 * gi] * (double)w[c0] + Ga[3 * gi + 1] * (double)w[c1] + Ga[3 * gi + 2] * (double)w[c2];
+          }
+          __syncwarp();
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            const int idx = lane + 32 * m;
+            if (idx < 81) {
+              const int i = idx / 9, j = idx - 9 * (idx / 9);
+              acc[m] -= Ha[3 * i] * Gb[3 * j] + Ha[3 * i + 1] * Gb[3 * j + 1] + Ha[3 * i + 2] * Gb[3 * j + 2];
+            }
+          }
+          __syncwarp();
+        }
+      }
+    }
+    const int dim = 9 * (cl.comp_cam_off[comp + 1] - cl.comp_cam_off[comp]);
+    double* __restrict__ M = cl.inv + cl.comp_base[comp];
+    const int pa = cl.cam_pos[a], pb = cl.cam_pos[b];
+    const double scale = (pass == 1 && cl.tridiagonal && cl.cam_cluster[a] != cl.cam_cluster[b]) ? 0.5 : 1.0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int idx = lane + 32 * m;
+      if (idx >= 81) continue;
+      const int i = idx / 9, j = idx - 9 * (idx / 9);
+      double v = acc[m];
+      if (a == b) {
+        if (i > j) continue;  // from the upper triangle of the camera sums: exactly symmetric
+        v = cam_acc[(size_t)a * kCamAcc + tri9(i, j)] + (i == j ? ba.cam_diag[9 * (size_t)a + i] : 0.0);
+      }
+      v *= scale;
+      M[(size_t)(9 * pa + i) * dim + 9 * pb + j] = v;
+      M[(size_t)(9 * pb + j) * dim + 9 * pa + i] = v;
+    }
+  }
+}
+
+// Zero the component matrices (pass 1: only when the first matrix was not positive definite).
+__global__ void k_cluster_zero(ClusterArgs cl, long long num_elements, int pass) {
+  if (pass == 1 && *reinterpret_cast<volatile unsigned*>(cl.flags) == 0u) return;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < num_elements;
+       e += (long long)gridDim.x * blockDim.x)
+    cl.inv[e] = 0.0;
+}
+
+// In-place inversion of every component matrix by the symmetric sweep operator, all
+// components at once, pivot k of each in step k, a grid barrier per step. Sweeping pivot
+// k with d = a_kk: a_kk <- -1/d, a_ik <- a_ik / d, a_kj <- a_kj / d, a_ij <- a_ij - a_ik a_kj / d.
+// The matrix stays symmetric, so column k is row k, and row k is read from a copy made
+// in the previous step (piv, two rows per component, alternating), which lets every
+// element be updated in place in one step. After the last pivot the matrix is -A^-1;
+// the epilogue negates it. The pivots d are those of A's LDL^T factorisation: all are
+// positive exactly when A is positive definite (the test torch.linalg.cholesky makes,
+// linear.py:1141-1145); a non-positive pivot sets flags[pass], a zero or non-finite one
+// flags[2]. Pass 1 runs only when pass 0 found its matrix not positive definite.
+__global__ void __launch_bounds__(256) k_cluster_sweep(ClusterArgs cl, GridBarrier gb, int pass) {
+  if (pass == 1 && *reinterpret_cast<volatile unsigned*>(cl.flags) == 0u) return;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nthreads = (long long)gridDim.x * blockDim.x;
+  for (int c = 0; c < cl.num_components; ++c) {
+    const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
+    const double* M = cl.inv + cl.comp_base[c];
+    double* pv = cl.piv + cl.comp_piv[c];
+    for (long long j = tid; j < dim; j += nthreads) pv[j] = M[j];
+  }
+  if (!grid_sync(gb)) return;
+  for (int k = 0; k < cl.max_dim; ++k) {
+    for (int c = 0; c < cl.num_components; ++c) {
+      const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
+      if (dim <= k) continue;
+      double* __restrict__ M = cl.inv + cl.comp_base[c];
+      const double* __restrict__ pk = cl.piv + cl.comp_piv[c] + (size_t)(k & 1) * dim;
+      double* __restrict__ pn = cl.piv + cl.comp_piv[c] + (size_t)((k + 1) & 1) * dim;
+      const double d = ld_cross(pk + k);
+      const double rd = 1.0 / d;
+      const unsigned udim = (unsigned)dim, n2 = udim * udim;  // dim <= 16384 (checked on the host)
+      for (unsigned e = (unsigned)tid; e < n2; e += (unsigned)nthreads) {
+        const int i = (int)(e / udim), j = (int)(e - (unsigned)i * udim);
+        double v;
+        if (i == k) v = (j == k) ? -rd : ld_cross(pk + j) * rd;
+        else if (j == k) v = ld_cross(pk + i) * rd;
+        else v = M[e] - ld_cross(pk + i) * ld_cross(pk + j) * rd;
+        M[e] = v;
+        if (i == k + 1) pn[j] = v;
+      }
+      if (tid == 0) {
+        if (!(d > 0.0)) atomicOr(cl.flags + pass, 1u);
+        if (d == 0.0 || !isfinite(d)) atomicOr(cl.flags + 2, 1u);
+      }
+    }
+    if (!grid_sync(gb)) return;
+  }
+  for (int c = 0; c < cl.num_components; ++c) {
+    const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
+    double* M = cl.inv + cl.comp_base[c];
+    const long long n2 = (long long)dim * dim;
+    for (long long e = tid; e < n2; e += nthreads) M[e] = -M[e];
+  }
+}
+
+// ======================================================================================
 // C ABI
 // ======================================================================================
 namespace {
@@ -1664,6 +1878,40 @@ bool valid(const ceres_b200_ba_t* ba) {
   }
   if (ba->num_items < 0) return false;
   return true;
+}
+
+// The cluster struct against the problem: pointers present, sizes consistent. The index
+// arrays themselves are the host builder's (clustering.py) and are not re-checked here.
+bool valid_clusters(const ceres_b200_ba_t& ba, const ceres_b200_clusters_t* cl) {
+  if (!cl) return false;
+  if (cl->num_components < 1 || cl->num_pairs < cl->num_components || cl->max_dim < 9 || cl->max_dim % 9 != 0)
+    return false;
+  if (cl->max_dim > 16384 || cl->max_dim > 9 * ba.num_cameras || cl->num_elements < 81) return false;
+  if (!cl->pairs || !cl->entries || !cl->cam_comp || !cl->cam_pos || !cl->cam_cluster || !cl->comp_cams ||
+      !cl->comp_cam_off || !cl->comp_base || !cl->comp_piv || !cl->inv || !cl->piv || !cl->flags)
+    return false;
+  return true;
+}
+
+ClusterArgs cluster_args(const ceres_b200_clusters_t& c) {
+  ClusterArgs a;
+  a.num_components = c.num_components;
+  a.num_pairs = c.num_pairs;
+  a.max_dim = c.max_dim;
+  a.tridiagonal = c.tridiagonal;
+  a.pairs = reinterpret_cast<const int2*>(c.pairs);
+  a.entries = reinterpret_cast<const int2*>(c.entries);
+  a.cam_comp = c.cam_comp;
+  a.cam_pos = c.cam_pos;
+  a.cam_cluster = c.cam_cluster;
+  a.comp_cams = c.comp_cams;
+  a.comp_cam_off = c.comp_cam_off;
+  a.comp_base = reinterpret_cast<const long long*>(c.comp_base);
+  a.comp_piv = reinterpret_cast<const long long*>(c.comp_piv);
+  a.inv = c.inv;
+  a.piv = c.piv;
+  a.flags = c.flags;
+  return a;
 }
 
 int check_launch() {
@@ -1691,8 +1939,8 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   auto kern = k_pcg<T>;
   cudaFuncAttributes fa;
   if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return CERES_B200_ECUDA;
-  // shared memory: a copy of p in T for the products' camera gathers
-  const size_t vec_bytes = ((size_t)n * sizeof(T) + 15) & ~(size_t)15;
+  // shared memory: a float64 copy of p for the products' camera gathers
+  const size_t vec_bytes = ((size_t)n * sizeof(double) + 15) & ~(size_t)15;
   L.smem_vectors = (vec_bytes + fa.sharedSizeBytes + 1024 <= (size_t)d.max_smem_optin) ? 1 : 0;
   L.dyn_smem = L.smem_vectors ? vec_bytes : 0;
   if (L.dyn_smem > 48 * 1024) {
@@ -1751,8 +1999,10 @@ struct SeriesOpts {
 
 template <typename T>
 int launch_pcg(const ceres_b200_ba_t& ba, int min_it, int max_it, double tol, int max_ref, cudaStream_t st,
-               const PcgLayout& L, char* scratch, const SeriesOpts& so) {
+               const PcgLayout& L, char* scratch, const SeriesOpts& so, const ClusterArgs* cl = nullptr) {
   PcgArgs a;
+  a.cluster = cl != nullptr ? 1 : 0;
+  if (cl != nullptr) a.cl = *cl;
   a.precond_series = so.precond;
   a.init_series = so.init;
   a.init_blocks = so.init_blocks;
@@ -1764,7 +2014,7 @@ int launch_pcg(const ceres_b200_ba_t& ba, int min_it, int max_it, double tol, in
   a.min_iterations = min_it;
   a.max_iterations = max_it;
   a.tolerance = tol;
-  a.eps = (double)Eps<T>::v();
+  a.eps = kEps64;  // the PCG vectors and arithmetic are float64 in both precisions
   a.n = 9 * ba.num_cameras;
   a.cams_per_cta = L.cams_per_cta;
   a.smem_vectors = L.smem_vectors;
@@ -1855,7 +2105,7 @@ void camera_assemble_impl(const ceres_b200_ba_t& ba, const PcgLayout& L, char* s
 
 template <typename T>
 int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, double tol, int max_ref, cudaStream_t st,
-             int series_terms = 1, double series_tol = 0.0, int series_init = 0) {
+             int series_terms = 1, double series_tol = 0.0, int series_init = 0, const ClusterArgs* cl = nullptr) {
   PcgLayout L;
   CB_TRACE("pcg: layout");
   int rc = pcg_layout<T>(ba, L);
@@ -1871,7 +2121,7 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
   so.tol = series_tol;
   so.init = series_init ? 1 : 0;
   so.init_blocks = so.precond ? ba.precond : static_cast<const void*>(scratch + L.spse_base);
-  rc = launch_pcg<T>(ba, min_it, max_it, tol, max_ref, st, L, scratch, so);
+  rc = launch_pcg<T>(ba, min_it, max_it, tol, max_ref, st, L, scratch, so, cl);
   if (rc) return rc;
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(ba);
@@ -2060,8 +2310,9 @@ int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, doub
                                   int jacobi_scaling, int preconditioner, void* stream) {
   if (!valid(ba) || !ba->scratch) return CERES_B200_EINVAL;
   const int flags = preconditioner & ~0xff;
-  const int pc = preconditioner & 0xff;
-  if (pc < CERES_B200_PRECOND_IDENTITY || pc > CERES_B200_PRECOND_SCHUR_POWER_SERIES) return CERES_B200_EINVAL;
+  int pc = preconditioner & 0xff;
+  if (pc < CERES_B200_PRECOND_IDENTITY || pc > CERES_B200_PRECOND_CLUSTER) return CERES_B200_EINVAL;
+  if (pc == CERES_B200_PRECOND_CLUSTER) pc = CERES_B200_PRECOND_IDENTITY;  // built by cluster_factor
   if ((flags & ~CERES_B200_PRECOND_FLAG_SPSE_BASE) != 0) return CERES_B200_EINVAL;
   if (ba->num_cameras == 0) return CERES_B200_OK;
   PcgLayout L;
@@ -2241,6 +2492,62 @@ int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, voi
   count_launch();
   k_copy_error<<<1, 1, 0, st>>>(*ba);
   return check_launch();
+}
+
+int ceres_b200_clusters_struct_bytes(void) { return (int)sizeof(ceres_b200_clusters_t); }
+
+int ceres_b200_ba_cluster_factor(const ceres_b200_ba_t* ba, const ceres_b200_clusters_t* cl, void* stream) {
+  if (!valid(ba) || !valid_clusters(*ba, cl) || !ba->scratch) return CERES_B200_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  const DevInfo d = device_info();
+  const ClusterArgs c = cluster_args(*cl);
+  // the camera sums of the last camera_assemble, in the scratch
+  PcgLayout L;
+  const int lrc = ba->precision == CERES_B200_FP32 ? pcg_layout<float>(*ba, L) : pcg_layout<double>(*ba, L);
+  if (lrc) return lrc;
+  if ((size_t)ba->scratch_bytes < L.total) return CERES_B200_EINVAL;
+  const double* cam_acc = reinterpret_cast<const double*>(reinterpret_cast<const char*>(ba->scratch) + L.cam_acc);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cluster_sweep, 256, 0) != cudaSuccess || per_sm < 1)
+    return CERES_B200_ECOOP;
+  const int sweep_grid = d.sms * (per_sm < 4 ? per_sm : 4);
+  int pair_grid = (cl->num_pairs * 32 + kWarpBlock - 1) / kWarpBlock;
+  if (pair_grid > 16 * d.sms) pair_grid = 16 * d.sms;
+  int zero_grid = (int)((cl->num_elements + 255) / 256);
+  if (zero_grid > 8 * d.sms) zero_grid = 8 * d.sms;
+  if (cudaMemsetAsync(cl->flags, 0, 8 * sizeof(uint32_t), st) != cudaSuccess) return CERES_B200_ECUDA;
+  for (int pass = 0; pass < (cl->tridiagonal ? 2 : 1); ++pass) {
+    ClusterArgs cp = c;
+    int pp = pass;
+    GridBarrier gb{cl->flags + 3, cl->flags + 4, cl->flags + 5};
+    long long ne = cl->num_elements;
+    count_launch(2);
+    k_cluster_zero<<<zero_grid, 256, 0, st>>>(c, ne, pass);
+    if (ba->precision == CERES_B200_FP32)
+      k_cluster_assemble<float><<<pair_grid, kWarpBlock, 0, st>>>(*ba, c, cam_acc, pass);
+    else
+      k_cluster_assemble<double><<<pair_grid, kWarpBlock, 0, st>>>(*ba, c, cam_acc, pass);
+    void* args[] = {&cp, &gb, &pp};
+    count_launch();
+    if (cudaLaunchCooperativeKernel((const void*)k_cluster_sweep, dim3(sweep_grid), dim3(256), args, 0, st) !=
+        cudaSuccess)
+      return CERES_B200_ECOOP;
+  }
+  return check_launch();
+}
+
+int ceres_b200_ba_pcg_cluster(const ceres_b200_ba_t* ba, const ceres_b200_clusters_t* cl, int min_iterations,
+                              int max_iterations, double tolerance, int max_refinements, void* stream) {
+  if (!valid(ba) || !valid_clusters(*ba, cl) || max_iterations < 0 || min_iterations < 0 || max_refinements < 0)
+    return CERES_B200_EINVAL;
+  if (!ba->pcg_x || !ba->pcg_r || !ba->pcg_z || !ba->pcg_p || !ba->pcg_ap || !ba->step_cameras) return CERES_B200_EINVAL;
+  const ClusterArgs c = cluster_args(*cl);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ba->precision == CERES_B200_FP32)
+    return pcg_impl<float>(*ba, CERES_B200_PRECOND_CLUSTER, min_iterations, max_iterations, tolerance,
+                           max_refinements, st, 1, 0.0, 0, &c);
+  return pcg_impl<double>(*ba, CERES_B200_PRECOND_CLUSTER, min_iterations, max_iterations, tolerance,
+                          max_refinements, st, 1, 0.0, 0, &c);
 }
 
 int ceres_b200_debug_barrier_timeout(uint32_t* words, uint32_t spin_limit, void* stream) {

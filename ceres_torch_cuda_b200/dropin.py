@@ -32,7 +32,8 @@ from .linear import OptionalBackendUnavailable as _OwnUnavailable
 from .types import SolverOptions, SolverSummary
 
 SCHUR_SOLVERS = ("ITERATIVE_SCHUR", "SPARSE_SCHUR", "DENSE_SCHUR")
-GPU_PRECONDITIONERS = ("IDENTITY", "JACOBI", "SCHUR_JACOBI", "SCHUR_POWER_SERIES_EXPANSION")
+GPU_PRECONDITIONERS = ("IDENTITY", "JACOBI", "SCHUR_JACOBI", "SCHUR_POWER_SERIES_EXPANSION", "CLUSTER_JACOBI",
+                       "CLUSTER_TRIDIAGONAL")
 
 
 def options_from(options: Any) -> SolverOptions:

@@ -28,7 +28,10 @@ _PRECOND = {
     PreconditionerType.JACOBI: _lib.PRECOND_JACOBI,
     PreconditionerType.SCHUR_JACOBI: _lib.PRECOND_SCHUR_JACOBI,
     PreconditionerType.SCHUR_POWER_SERIES_EXPANSION: _lib.PRECOND_SCHUR_POWER_SERIES,
+    PreconditionerType.CLUSTER_JACOBI: _lib.PRECOND_CLUSTER,
+    PreconditionerType.CLUSTER_TRIDIAGONAL: _lib.PRECOND_CLUSTER,
 }
+_CLUSTER_MAX_DIM = 16384  # 9 x cameras of the largest component (the sweep's 32-bit element index)
 
 PRECISIONS = ("fp64", "mixed")
 
@@ -178,6 +181,8 @@ class BAEngine:
             raise ValueError("observations must be finite")
         self.layout = layout or build_layout(camera_index.to(dev), point_index.to(dev), observations.to(dev),
                                              self.nc, self.np)
+        self._index = (camera_index, point_index, point_constant)
+        self.clusters: ClusterPlan | None = None
         L = self.layout
         self.np_pad = 32 * L.num_slices
         T = torch.float32 if precision == "mixed" else torch.float64
@@ -330,6 +335,21 @@ class BAEngine:
                    float(options.max_lm_diagonal), int(options.jacobi_scaling))
         self._call("ceres_b200_ba_camera_assemble", float(radius), float(options.min_lm_diagonal),
                    float(options.max_lm_diagonal), int(options.jacobi_scaling), int(precond) | flags)
+        if precond == _lib.PRECOND_CLUSTER:
+            if self.clusters is None:
+                raise RuntimeError("setup_clusters() first")
+            self._call("ceres_b200_ba_cluster_factor", ctypes.byref(self.clusters.struct))
+
+    def setup_clusters(self, tridiagonal: bool, clustering: str = "CANONICAL_VIEWS") -> bool:
+        """Cluster the active cameras by visibility (linear.py:953-990) and allocate the
+        preconditioner's storage. False when the reference would not use the clusters:
+        fewer than two active cameras, or no camera sees an active point (it then uses
+        SCHUR_JACOBI's blocks, linear.py:498-528)."""
+        self.clusters = ClusterPlan.build(self, tridiagonal, clustering)
+        return self.clusters is not None
+
+    def cluster_flags(self) -> np.ndarray:
+        return self.clusters.flags.cpu().numpy().view(np.uint32).copy()
 
     def pcg(self, precond: int, min_iterations: int, max_iterations: int, tolerance: float,
             max_refinements: int = 0, spse_terms: int = 0, spse_tolerance: float = 0.0,
@@ -338,7 +358,10 @@ class BAEngine:
         or ``spse_init`` the series options apply (``spse_terms`` = max_num_spse_iterations);
         ``spse_init`` needs the SPSE base blocks from ``assemble(..., spse_base=True)``
         unless the preconditioner is the power series itself."""
-        if precond == _lib.PRECOND_SCHUR_POWER_SERIES or spse_init:
+        if precond == _lib.PRECOND_CLUSTER:
+            self._call("ceres_b200_ba_pcg_cluster", ctypes.byref(self.clusters.struct), int(min_iterations),
+                       int(max_iterations), float(tolerance), int(max_refinements))
+        elif precond == _lib.PRECOND_SCHUR_POWER_SERIES or spse_init:
             self._call("ceres_b200_ba_pcg_spse", int(precond), int(min_iterations), int(max_iterations),
                        float(tolerance), int(max_refinements), int(spse_terms), float(spse_tolerance), int(bool(spse_init)))
         else:
@@ -385,6 +408,91 @@ class BAEngine:
         r = self.res[slots]
         J = self.jac[slots].to(torch.float64)
         return r, J[:, :18].reshape(-1, 2, 9), J[:, 18:].reshape(-1, 2, 3)
+
+
+class ClusterPlan:
+    """Device arrays of the visibility-cluster preconditioner of one engine
+    (ceres_b200_clusters_t): the kept camera block pairs, the components they link, the
+    cameras' point lists by point lane, and the storage of the component inverses."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @classmethod
+    def build(cls, eng: "BAEngine", tridiagonal: bool, clustering: str) -> "ClusterPlan | None":
+        from . import clustering as C
+
+        dev = eng.device
+        active = np.flatnonzero(eng.cam_const[:eng.nc].cpu().numpy() == 0)
+        if active.size < 2:
+            return None
+        ci_t, pi_t, pconst = eng._index
+        ci = ci_t.detach().cpu().numpy().astype(np.int64)
+        pi = pi_t.detach().cpu().numpy().astype(np.int64)
+        col = np.full(eng.nc, -1, dtype=np.int64)
+        col[active] = np.arange(active.size)
+        keep = col[ci] >= 0
+        if pconst is not None:
+            keep &= ~pconst.detach().cpu().numpy().astype(bool)[pi]
+        if not keep.any():
+            return None
+        incidence = C.incidence_from_observations(active.size, col[ci[keep]], pi[keep])
+        st = C.cluster_structure(tridiagonal=tridiagonal, clustering=clustering, incidence=incidence)
+        comps = st.components()
+        dims = np.array([9 * g.size for g in comps], dtype=np.int64)
+        if int(dims.max()) > _CLUSTER_MAX_DIM:
+            raise NotImplementedError(
+                f"a visibility-cluster component of {int(dims.max()) // 9} cameras: the GPU preconditioner "
+                f"inverts components of up to {_CLUSTER_MAX_DIM // 9} cameras")
+        member = st.membership
+        pairs = []
+        cam_comp = np.full(eng.nc, -1, dtype=np.int32)
+        cam_pos = np.zeros(eng.nc, dtype=np.int32)
+        cam_cluster = np.full(eng.nc, -1, dtype=np.int32)
+        cam_cluster[active] = member
+        for k, g in enumerate(comps):
+            cams = active[g]
+            cam_comp[cams] = k
+            cam_pos[cams] = np.arange(g.size)
+            kg = member[g]
+            same = kg[:, None] == kg[None, :]
+            nb = st.neighbors[kg]                                   # [m][2]
+            linked = (nb[:, None, :] == kg[None, :, None]).any(axis=2)
+            a, b = np.nonzero(np.triu(same | linked))
+            pairs.append(np.stack([cams[a], cams[b]], axis=1))
+        pairs = np.concatenate(pairs).astype(np.int32)
+        comp_cams = np.concatenate([active[g] for g in comps]).astype(np.int32)
+        comp_cam_off = np.concatenate([[0], np.cumsum([g.size for g in comps])]).astype(np.int32)
+        comp_base = np.concatenate([[0], np.cumsum(dims * dims)]).astype(np.int64)
+        comp_piv = np.concatenate([[0], np.cumsum(2 * dims)]).astype(np.int64)
+        # every camera's observations by point lane (the pair kernel looks points up)
+        L = eng.layout
+        ents = L.cam_entries[:eng.no].to(torch.int64)
+        counts = (L.cam_offsets[1:] - L.cam_offsets[:-1]).to(torch.int64)
+        owner = torch.repeat_interleave(torch.arange(eng.nc, device=dev), counts)
+        order = torch.argsort(owner * max(eng.np_pad, 1) + ents[:, 1], stable=True)
+        entries = ents[order].to(torch.int32).contiguous() if eng.no else L.cam_entries
+        t = lambda a: torch.as_tensor(a).to(dev).contiguous()  # noqa: E731
+        plan = cls(structure=st, components=comps, pairs=t(pairs), entries=entries, cam_comp=t(cam_comp),
+                   cam_pos=t(cam_pos), cam_cluster=t(cam_cluster), comp_cams=t(comp_cams),
+                   comp_cam_off=t(comp_cam_off), comp_base=t(comp_base), comp_piv=t(comp_piv),
+                   inv=torch.zeros(int(comp_base[-1]), dtype=torch.float64, device=dev),
+                   piv=torch.zeros(int(comp_piv[-1]), dtype=torch.float64, device=dev),
+                   flags=torch.zeros(8, dtype=torch.int32, device=dev), tridiagonal=bool(tridiagonal))
+        s = _lib.ClusterStruct()
+        s.num_components, s.num_pairs = len(comps), int(pairs.shape[0])
+        s.max_dim, s.tridiagonal, s.num_elements = int(dims.max()), int(bool(tridiagonal)), int(comp_base[-1])
+        for name in ("pairs", "entries", "cam_comp", "cam_pos", "cam_cluster", "comp_cams", "comp_cam_off",
+                     "comp_base", "comp_piv", "inv", "piv", "flags"):
+            setattr(s, name, _ptr(getattr(plan, name)))
+        plan.struct = s
+        return plan
+
+    def matrices(self) -> list[torch.Tensor]:
+        """The component inverses (views into the storage), after cluster_factor."""
+        base = self.comp_base.cpu().numpy()
+        return [self.inv[int(base[k]):int(base[k + 1])].view(9 * g.size, 9 * g.size)
+                for k, g in enumerate(self.components)]
 
 
 # ======================================================================================
@@ -466,7 +574,8 @@ def linear_solver_kind(options: SolverOptions) -> str:
         if options.preconditioner_type not in _PRECOND:
             raise NotImplementedError(
                 f"ITERATIVE_SCHUR with {options.preconditioner_type.value} is not implemented on the GPU path "
-                "(IDENTITY, JACOBI, SCHUR_JACOBI and SCHUR_POWER_SERIES_EXPANSION are)")
+                "(IDENTITY, JACOBI, SCHUR_JACOBI, SCHUR_POWER_SERIES_EXPANSION, CLUSTER_JACOBI and "
+                "CLUSTER_TRIDIAGONAL are)")
         return "iterative"
     raise NotImplementedError(f"{lst.value} is not a Schur solver; the GPU path implements DENSE_SCHUR, "
                               "SPARSE_SCHUR and ITERATIVE_SCHUR")
@@ -485,6 +594,12 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
     """
     kind = linear_solver_kind(options)
     precond = _PRECOND.get(options.preconditioner_type, _lib.PRECOND_SCHUR_JACOBI)
+    if precond == _lib.PRECOND_CLUSTER:
+        # the visibility clusters of the active cameras (linear.py:498-521); without them the
+        # reference uses the SCHUR_JACOBI blocks
+        tri = options.preconditioner_type is PreconditionerType.CLUSTER_TRIDIAGONAL
+        if kind != "iterative" or not engine.setup_clusters(tri, options.visibility_clustering_type.name):
+            precond = _lib.PRECOND_SCHUR_JACOBI
     spse_init = kind == "iterative" and bool(options.use_spse_initialization)
     spse_base = spse_init and precond != _lib.PRECOND_SCHUR_POWER_SERIES
     refinements = max_refinements if engine.precision == "mixed" else 0

@@ -225,6 +225,29 @@ def make_ring_ba(
                    meta={"seed": seed})
 
 
+def make_sequence_ba(num_cameras: int, num_points: int, window: int, *, seed: int = 0, loss=("trivial",),
+                     closed: bool = False) -> BAData:
+    """A capture sequence: the ring cameras of ``make_ring_ba``, and each point seen by
+    ``window`` consecutive cameras from a uniform start (wrapping round the ring when
+    ``closed``), so that the camera visibility graph is banded and the visibility
+    clusters are runs of neighbouring cameras."""
+    rng = np.random.default_rng(seed)
+    window = min(int(window), num_cameras)
+    true_cams = np.zeros((num_cameras, 9))
+    true_cams[:, 1] = 2.0 * np.pi * np.arange(num_cameras) / num_cameras
+    true_cams[:, 0:3] += rng.normal(0.0, 0.01, size=(num_cameras, 3))
+    true_cams[:, 3:6] = np.array([0.0, 0.0, 10.0]) + rng.normal(0.0, 0.1, size=(num_cameras, 3))
+    true_cams[:, 6] = 500.0
+    true_cams[:, 7:9] = rng.normal(0.0, 1e-3, size=(num_cameras, 2))
+    true_pts = rng.uniform(-3.0, 3.0, size=(num_points, 3))
+    span = num_cameras if closed else num_cameras - window + 1
+    start = rng.integers(0, span, size=num_points)
+    cam = ((start[:, None] + np.arange(window)[None, :]) % num_cameras).reshape(-1).astype(np.int64)
+    pt = np.repeat(np.arange(num_points, dtype=np.int64), window)
+    return _finish(rng, true_cams, true_pts, cam, pt, loss, f"sequence nc={num_cameras} np={num_points} w={window}",
+                   meta={"seed": seed})
+
+
 def make_small_ba(num_cameras: int, num_points: int, track: int, *, seed: int = 0, loss=("trivial",),
                   outlier_fraction: float = 0.0) -> BAData:
     """Small instance with the configs[0] camera/point model (tests, fixtures)."""

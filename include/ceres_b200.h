@@ -52,7 +52,11 @@ enum {
   CERES_B200_PRECOND_SCHUR_JACOBI = 2,
   /* SCHUR_POWER_SERIES_EXPANSION (linear.py:482-497): blocks of the damped Hbb,
    * series in ceres_b200_ba_pcg_spse; single-problem path only */
-  CERES_B200_PRECOND_SCHUR_POWER_SERIES = 3
+  CERES_B200_PRECOND_SCHUR_POWER_SERIES = 3,
+  /* CLUSTER_JACOBI / CLUSTER_TRIDIAGONAL (linear.py:1032-1085): the inverse of S kept on
+   * the visibility cluster pairs, built by ceres_b200_ba_cluster_factor and applied by
+   * ceres_b200_ba_pcg_cluster; camera_assemble treats it as IDENTITY */
+  CERES_B200_PRECOND_CLUSTER = 4
 };
 /* or-ed into camera_assemble's preconditioner: also build the Hbb blocks of the
  * SPSE initial point (use_spse_initialization, linear.py:745-756) in the scratch */
@@ -320,6 +324,61 @@ int ceres_b200_ba_schur_matrix(const ceres_b200_ba_t* ba, double* S, void* strea
  * caller zeroes). Used for the camera covariance (covariance.py:86-445).
  */
 int ceres_b200_dense_spd_inverse(double* A, double* inv, int64_t n, uint32_t* flags, void* stream);
+
+/*
+ * Visibility-cluster preconditioner of the reduced camera system (CLUSTER_JACOBI and
+ * CLUSTER_TRIDIAGONAL, linear.py:498-521 and :1032-1085). The host clusters the cameras
+ * (linear.py:842-1028) and passes the kept camera block pairs; the kept matrix is block
+ * diagonal over the connected groups of cameras ("components") that the pairs link.
+ * All pointers are device memory; the struct itself is read on the host.
+ */
+typedef struct ceres_b200_clusters {
+  int32_t num_components;
+  int32_t num_pairs;           /* kept camera block pairs (a, b), a <= b */
+  int32_t max_dim;             /* largest component dimension (9 x its cameras) */
+  int32_t tridiagonal;         /* 1: CLUSTER_TRIDIAGONAL (halve the blocks between
+                                * clusters when the kept matrix is not positive definite) */
+  int64_t num_elements;        /* comp_base[num_components]: length of inv */
+  const int32_t* pairs;        /* [num_pairs][2] camera ids a <= b */
+  const int32_t* entries;      /* [num_observations][2] (slot, point lane) of every camera,
+                                * camera-major (offsets cam_offsets), by point lane within a camera */
+  const int32_t* cam_comp;     /* [num_cameras] component of the camera, -1 for one outside */
+  const int32_t* cam_pos;      /* [num_cameras] position of the camera in its component */
+  const int32_t* cam_cluster;  /* [num_cameras] cluster of the camera */
+  const int32_t* comp_cams;    /* the cameras of the components, component after component */
+  const int32_t* comp_cam_off; /* [num_components + 1] */
+  const int64_t* comp_base;    /* [num_components + 1] first element of the component's
+                                * matrix in inv (row-major, dim x dim) */
+  const int64_t* comp_piv;     /* [num_components + 1] first element of its two pivot rows in piv */
+  double* inv;                 /* [comp_base[num_components]] the kept matrices, then their inverses */
+  double* piv;                 /* [comp_piv[num_components]] pivot rows of the sweep */
+  uint32_t* flags;             /* [8], zeroed by cluster_factor: [0] the kept matrix was not
+                                * positive definite, [1] nor was the halved one, [2] a zero
+                                * pivot, [3..5] grid barrier words ([5]: CERES_B200_DEVERR_BARRIER
+                                * when a barrier wait gave up) */
+} ceres_b200_clusters_t;
+
+/* sizeof(ceres_b200_clusters_t) as compiled into the library (binding check). */
+int ceres_b200_clusters_struct_bytes(void);
+
+/*
+ * Builds the kept matrices of S at the current assembly (float64 arithmetic on the
+ * Jacobian store, deterministic: one warp per block pair, shared points in point order)
+ * and inverts them with the symmetric sweep operator in one cooperative launch (all
+ * components at once, a grid barrier per pivot). Non-positive pivots set flags[0]; with
+ * tridiagonal set, the matrices are rebuilt with the blocks between different clusters
+ * halved and inverted again (flags[1] when that one is not positive definite either,
+ * where the reference falls back to a general solve of the same matrix, which the
+ * sweep's inverse equals). A zero pivot sets flags[2]. Call after camera_assemble.
+ */
+int ceres_b200_ba_cluster_factor(const ceres_b200_ba_t* ba, const ceres_b200_clusters_t* cl, void* stream);
+
+/*
+ * ceres_b200_ba_pcg with z = M^-1 r from the inverses of ceres_b200_ba_cluster_factor
+ * (one grid barrier more per iteration: z of a camera needs r of its whole component).
+ */
+int ceres_b200_ba_pcg_cluster(const ceres_b200_ba_t* ba, const ceres_b200_clusters_t* cl, int min_iterations,
+                              int max_iterations, double tolerance, int max_refinements, void* stream);
 
 /*
  * Check of the bounded waits of the cooperative kernels (failure detection without a

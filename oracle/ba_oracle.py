@@ -31,6 +31,10 @@ ceres-torch project root):
   block of S; JACOBI = clamped diagonal; IDENTITY; SCHUR_POWER_SERIES_EXPANSION = the series
   of linear.py:59-67 on the SCHUR_JACOBI factors of Hbb, linear.py:482-497) and the SPSE initial
   point of linear.py:745-756.
+* cluster preconditioners      linear.py:498-521 and :1032-1085 (S kept on the visibility cluster
+  block pairs, Cholesky, the halved retry of CLUSTER_TRIDIAGONAL, the general-solve fallback of
+  :1366-1370), with the clustering of linear.py:842-1028 (visibility graph, SINGLE_LINKAGE,
+  CANONICAL_VIEWS, cluster graph, degree-2 maximum spanning forest) restated loop for loop.
 * ``solve``                     solver.py:35-357 (trust-region LM), with :798-802 (model
   decrease), :805-820 (LM radius), :823-861 (step evaluator), :1165-1175 (convergence tests),
   :661-676 (restore best state), :714-785 (parameter order, num_eliminate, visibility).
@@ -462,6 +466,45 @@ class _Preconditioner:
         return self.dinv * r
 
 
+class _ClusterPreconditioner:
+    """linear.py:1032-1085 and :53-59: S kept on the cluster block pairs, Cholesky-
+    factored; CLUSTER_TRIDIAGONAL whose kept matrix is not positive definite halves the
+    blocks between different clusters and tries again; a matrix that still fails is
+    solved as a general square system (linear.py:1366-1370)."""
+
+    def __init__(self, S: np.ndarray, st: "OracleClusterStructure", tridiagonal: bool):
+        n = S.shape[0] // 9
+        member = np.asarray(st.membership)
+        keep = np.zeros((n, n), dtype=bool)
+        for a, b in st.block_pairs:
+            keep[a, b] = keep[b, a] = True
+        mask = np.kron(keep, np.ones((9, 9), dtype=bool))
+        M = np.where(mask, S, 0.0)
+        self.factor, self.chol = self._factor(M)
+        if not self.chol and tridiagonal:
+            cross = np.kron(keep & (member[:, None] != member[None, :]), np.ones((9, 9), dtype=bool))
+            scaled = np.where(cross, 0.5 * M, M)
+            f, ok = self._factor(scaled)
+            self.factor, self.chol = (f, True) if ok else (scaled, False)
+
+    @staticmethod
+    def _factor(M):
+        try:
+            return np.linalg.cholesky(M), True
+        except np.linalg.LinAlgError:
+            return M, False
+
+    def apply(self, r: np.ndarray) -> np.ndarray:
+        v = r.reshape(-1)
+        if self.chol:
+            y = np.linalg.solve(self.factor, v)
+            return np.linalg.solve(self.factor.T, y).reshape(r.shape)
+        try:
+            return np.linalg.solve(self.factor, v).reshape(r.shape)
+        except np.linalg.LinAlgError:
+            return np.linalg.lstsq(self.factor, v, rcond=None)[0].reshape(r.shape)
+
+
 class _PowerSeries:
     """SCHUR_POWER_SERIES_EXPANSION (linear.py:482-497, applied at :59-67):
     z = sum_i (B E)^i B r with B the SCHUR_JACOBI factors of the damped Hbb blocks and
@@ -559,6 +602,12 @@ def solve_step(prob, ev, radius, opts, *, explicit_limit=1800):
             mv = lambda v: schur_matvec(sys, v)  # noqa: E731
         if opts.preconditioner_type == "SCHUR_POWER_SERIES_EXPANSION":
             prec = _PowerSeries(sys, opts.max_num_spse_iterations, opts.spse_tolerance)
+        elif (opts.preconditioner_type in ("CLUSTER_JACOBI", "CLUSTER_TRIDIAGONAL") and sys.n_cam > 1
+              and schur_visibility(prob) is not None):
+            # linear.py:498-521: the visibility clusters of the retained (camera) blocks
+            st = cluster_structure(schur_visibility(prob), tridiagonal=opts.preconditioner_type == "CLUSTER_TRIDIAGONAL",
+                                   clustering=opts.visibility_clustering_type)
+            prec = _ClusterPreconditioner(schur_dense(sys), st, opts.preconditioner_type == "CLUSTER_TRIDIAGONAL")
         else:
             prec = _Preconditioner(opts.preconditioner_type, schur_diag_blocks(sys))
         x0 = None
@@ -598,6 +647,7 @@ class OracleOptions:
     max_num_spse_iterations: int = 5
     spse_tolerance: float = 0.1
     use_spse_initialization: bool = False
+    visibility_clustering_type: str = "CANONICAL_VIEWS"
 
 
 @dataclass
@@ -896,3 +946,195 @@ def covariance(prob: OracleProblem, cameras, points, *, apply_loss: bool = True,
     elif np.any(ratios[keep] < min_reciprocal_condition_number):
         success, message = False, "Retained covariance spectrum is below min_reciprocal_condition_number."
     return OracleCovariance(success, message, rank, max(0, J.shape[1] - rank), tangent, cam_col, pt_col)
+
+
+# --------------------------------------------------------------------------------------
+# Visibility clustering (linear.py:842-1153), a loop-for-loop restatement
+# --------------------------------------------------------------------------------------
+def _norm_vis(visibility):
+    out = []
+    for pts in visibility:
+        st = set()
+        for p in pts:
+            p = int(p)
+            if p < 0:
+                raise ValueError("visibility point ids must be non-negative")
+            st.add(p)
+        out.append(frozenset(st))
+    return tuple(out)
+
+
+def visibility_graph(visibility) -> dict:
+    """linear.py:842-862."""
+    vis = _norm_vis(visibility)
+    cams_of: dict = {}
+    for c, pts in enumerate(vis):
+        for p in pts:
+            cams_of.setdefault(p, []).append(c)
+    counts: dict = {}
+    for cams in cams_of.values():
+        cams = sorted(cams)
+        for i, a in enumerate(cams):
+            for b in cams[i + 1:]:
+                counts[(a, b)] = counts.get((a, b), 0) + 1
+    edges = {(c, c): 1.0 for c in range(len(vis))}
+    for (a, b), k in counts.items():
+        denom = math.sqrt(float(len(vis[a]) * len(vis[b])))
+        if denom > 0.0:
+            edges[(a, b)] = float(k) / denom
+    return dict(sorted(edges.items()))
+
+
+def _flatten_membership(membership: dict, n: int) -> tuple:
+    """linear.py:1108-1118."""
+    index: dict = {}
+    out = []
+    for v in range(n):
+        key = membership.get(v, -1)
+        if key < 0:
+            key = v
+        if key not in index:
+            index[key] = len(index)
+        out.append(index[key])
+    return tuple(out)
+
+
+def _find(parent: dict, v: int) -> int:
+    root = v
+    while parent[root] != root:
+        root = parent[root]
+    while parent[v] != v:
+        parent[v], v = root, parent[v]
+    return root
+
+
+def single_linkage_clustering(visibility, min_similarity: float = 0.9) -> tuple:
+    """linear.py:865-893."""
+    graph = visibility_graph(visibility)
+    n = len(_norm_vis(visibility))
+    parent = {v: v for v in range(n)}
+    for (a, b), w in graph.items():
+        if a >= b or w < min_similarity:
+            continue
+        ra, rb = _find(parent, a), _find(parent, b)
+        if ra == rb:
+            continue
+        if ra < rb:
+            parent[rb] = ra
+        else:
+            parent[ra] = rb
+    return _flatten_membership({v: _find(parent, v) for v in range(n)}, n)
+
+
+def canonical_views_clustering(visibility, min_views=3, size_penalty_weight=3.0, similarity_penalty_weight=0.0,
+                               view_score_weight=0.0) -> tuple:
+    """linear.py:896-950."""
+    graph = visibility_graph(visibility)
+    n = len(_norm_vis(visibility))
+
+    def nbrs(v):
+        out = set()
+        for a, b in graph:
+            if a == v:
+                out.add(b)
+            if b == v:
+                out.add(a)
+        return sorted(out)
+
+    def w(a, b):
+        return graph.get((a, b) if a <= b else (b, a), 0.0)
+
+    valid = set(range(n))
+    centers: list = []
+    center_of: dict = {}
+    sim_of: dict = {}
+    while valid:
+        best_diff = -float("inf")
+        best_view = min(valid)
+        for cand in sorted(valid):
+            diff = view_score_weight
+            for nb in nbrs(cand):
+                old = sim_of.get(nb, 0.0)
+                new = w(nb, cand)
+                if new > old:
+                    diff += new - old
+            diff -= size_penalty_weight
+            for c in centers:
+                diff -= similarity_penalty_weight * w(c, cand)
+            if diff > best_diff:
+                best_diff, best_view = diff, cand
+        if best_diff <= 0.0 and len(centers) >= min_views:
+            break
+        centers.append(best_view)
+        valid.remove(best_view)
+        for nb in nbrs(best_view):
+            old = sim_of.get(nb, 0.0)
+            new = w(nb, best_view)
+            if new > old:
+                center_of[nb] = best_view
+                sim_of[nb] = new
+    idx = {c: i for i, c in enumerate(centers)}
+    return _flatten_membership({v: idx[center_of[v]] if v in center_of else -1 for v in range(n)}, n)
+
+
+def degree2_forest(num_vertices: int, weighted_edges: dict) -> tuple:
+    """linear.py:993-1028."""
+    parent = {v: v for v in range(num_vertices)}
+    degree = {v: 0 for v in range(num_vertices)}
+    edges = []
+    for (a, b), wt in weighted_edges.items():
+        if a == b:
+            continue
+        edges.append((float(wt), (a, b) if a < b else (b, a)))
+    forest = []
+    for _, (a, b) in sorted(edges, reverse=True):
+        if degree[a] == 2 or degree[b] == 2:
+            continue
+        ra, rb = _find(parent, a), _find(parent, b)
+        if ra == rb:
+            continue
+        forest.append((a, b))
+        degree[a] += 1
+        degree[b] += 1
+        if rb < ra:
+            ra, rb = rb, ra
+        parent[rb] = ra
+    return tuple(sorted(forest))
+
+
+@dataclass(frozen=True)
+class OracleClusterStructure:
+    membership: tuple
+    num_clusters: int
+    cluster_pairs: tuple
+    block_pairs: tuple
+
+
+def cluster_structure(visibility, *, tridiagonal: bool, clustering: str = "CANONICAL_VIEWS") -> OracleClusterStructure:
+    """linear.py:953-990 with the cluster graph of linear.py:1121-1134."""
+    vis = _norm_vis(visibility)
+    if clustering == "SINGLE_LINKAGE":
+        membership = single_linkage_clustering(vis)
+    elif clustering == "CANONICAL_VIEWS":
+        membership = canonical_views_clustering(vis)
+    else:
+        raise ValueError(f"Unknown visibility clustering type: {clustering}")
+    k = max(membership) + 1 if membership else 0
+    pairs = {(i, i) for i in range(k)}
+    if tridiagonal and k > 1:
+        seen = [set() for _ in range(k)]
+        for c, pts in enumerate(vis):
+            seen[membership[c]].update(pts)
+        cg = {}
+        for a in range(k):
+            for b in range(a + 1, k):
+                m = len(seen[a] & seen[b])
+                if m:
+                    cg[(a, b)] = float(m)
+        pairs.update(degree2_forest(k, dict(sorted(cg.items()))))
+    blocks = []
+    for a in range(len(membership)):
+        for b in range(a, len(membership)):
+            if tuple(sorted((membership[a], membership[b]))) in pairs:
+                blocks.append((a, b))
+    return OracleClusterStructure(membership, k, tuple(sorted(pairs)), tuple(blocks))

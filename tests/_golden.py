@@ -19,6 +19,10 @@ BA_CASES = [
     "ba_spse",
     "ba_spse_cauchy",
     "ba_spse_init",
+    "ba_cluster_jacobi",
+    "ba_cluster_tridiagonal",
+    "ba_cluster_single_linkage",
+    "ba_cluster_uniform",
 ]
 BIG_CASES = ["config0_dense", "config1_small", "config2_small"]
 

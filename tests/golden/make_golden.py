@@ -107,16 +107,22 @@ def _evaluate_blocks(tc, problem, data, constant_cameras):
 
 
 def make_case(tc, ex, name, data, *, solver, preconditioner="SCHUR_JACOBI", constant_cameras=(), max_iter=50, out=HERE,
-              spse=None):
+              spse=None, clustering=None):
+    """``spse``: further SolverOptions fields (stored in meta["spse"], which the tests pass
+    back); ``clustering``: the visibility_clustering_type name (stored there as a string)."""
     t0 = time.time()
     problem, cams, pts = _build(tc, ex, data, constant_cameras)
     blocks = _evaluate_blocks(tc, problem, data, constant_cameras)
     spse = dict(spse or {})
+    extra = dict(spse)
+    if clustering is not None:
+        extra["visibility_clustering_type"] = getattr(tc.VisibilityClusteringType, clustering)
+        spse["visibility_clustering_type"] = clustering
     opts = tc.SolverOptions(
         max_num_iterations=max_iter,
         linear_solver_type=getattr(tc.LinearSolverType, solver),
         preconditioner_type=getattr(tc.PreconditionerType, preconditioner),
-        **spse,
+        **extra,
     )
     summary = tc.solve(opts, problem)
     trace = np.array([[it.iteration, it.cost, it.cost_change, it.gradient_max_norm, it.step_norm,
@@ -232,6 +238,49 @@ def make_covariance(tc, ex, name, data, *, constant_cameras, out=HERE, point_blo
     print(f"{name}: success={cov.summary.success} rank={cov.summary.rank} ({meta['seconds']:.1f} s)", flush=True)
 
 
+def _visibility(nc, camera_index, point_index):
+    vis = [set() for _ in range(nc)]
+    for c, p in zip(np.asarray(camera_index).tolist(), np.asarray(point_index).tolist()):
+        vis[c].add(int(p))
+    return [sorted(v) for v in vis]
+
+
+def make_clustering(tc, out=HERE):
+    """The reference's visibility clustering (linear.py:842-1028) on visibility lists of
+    capture sequences, uniform problems and hand-made edge cases, for both clustering
+    types and both cluster preconditioners: membership, cluster pairs, kept block pairs
+    and the two similarity graphs."""
+    from ceres_torch.linear import build_visibility_cluster_structure
+
+    cases = {}
+    for nc, npts, w, closed, seed in ((12, 200, 3, False, 5), (10, 150, 4, True, 6), (16, 300, 3, False, 7),
+                                      (30, 600, 4, False, 8), (40, 500, 2, True, 9)):
+        d = S.make_sequence_ba(nc, npts, w, seed=seed, closed=closed)
+        cases[f"sequence_{nc}_{w}{'_closed' if closed else ''}"] = _visibility(nc, d.camera_index, d.point_index)
+    for nc, npts, t, seed in ((8, 60, 3, 1), (20, 300, 4, 2), (6, 10, 2, 3), (25, 80, 2, 4)):
+        d = S.make_small_ba(nc, npts, t, seed=seed)
+        cases[f"uniform_{nc}_{npts}_{t}"] = _visibility(nc, d.camera_index, d.point_index)
+    cases["edge_empty_and_duplicates"] = [[0, 1, 2, 2], [2, 3], [], [0, 1, 2], [5], [5, 6]]
+    cases["edge_identical_views"] = [[0, 1, 2], [0, 1, 2], [0, 1, 2], [7, 8], [7, 8], [9]]
+    cases["edge_single_camera"] = [[0, 1, 2]]
+    cases["edge_disjoint"] = [[0], [1], [2], [3]]
+    results = {}
+    for cname, vis in cases.items():
+        for pre in ("CLUSTER_JACOBI", "CLUSTER_TRIDIAGONAL"):
+            for kind in ("CANONICAL_VIEWS", "SINGLE_LINKAGE"):
+                st = build_visibility_cluster_structure(
+                    vis, preconditioner_type=getattr(tc.PreconditionerType, pre),
+                    visibility_clustering_type=getattr(tc.VisibilityClusteringType, kind))
+                results[f"{cname}|{pre}|{kind}"] = dict(
+                    membership=list(st.membership), num_clusters=st.num_clusters,
+                    cluster_pairs=[list(p) for p in st.cluster_pairs], block_pairs=[list(p) for p in st.block_pairs],
+                    camera_graph_edges=[list(e) for e in st.camera_graph_edges],
+                    cluster_graph_edges=[list(e) for e in st.cluster_graph_edges])
+    np.savez_compressed(out / "clustering.npz", visibility=np.array(json.dumps(cases)),
+                        results=np.array(json.dumps(results)))
+    print(f"clustering.npz written ({len(results)} structures)", flush=True)
+
+
 def make_bal(ex, name, data, out=HERE):
     """BAL text of ``data`` (the format BALProblem.from_text reads,
     examples/simple_bundle_adjuster.py:33-70) and what the reference parser returns."""
@@ -308,6 +357,21 @@ def main():
         make_covariance(tc, ex, "ba_covariance_gauge", cvg, constant_cameras=())
     if want("bal_text"):
         make_bal(ex, "bal_text", S.make_small_ba(7, 60, 3, seed=13))
+    if want("clustering"):
+        make_clustering(tc)
+    if want("ba_cluster_jacobi"):
+        make_case(tc, ex, "ba_cluster_jacobi", S.make_sequence_ba(12, 200, 3, seed=14), solver="ITERATIVE_SCHUR",
+                  preconditioner="CLUSTER_JACOBI")
+    if want("ba_cluster_tridiagonal"):
+        make_case(tc, ex, "ba_cluster_tridiagonal", S.make_sequence_ba(16, 240, 3, seed=15, loss=("cauchy", 2.0)),
+                  solver="ITERATIVE_SCHUR", preconditioner="CLUSTER_TRIDIAGONAL")
+    if want("ba_cluster_single_linkage"):
+        make_case(tc, ex, "ba_cluster_single_linkage", S.make_sequence_ba(10, 150, 4, seed=16, closed=True),
+                  solver="ITERATIVE_SCHUR", preconditioner="CLUSTER_TRIDIAGONAL", clustering="SINGLE_LINKAGE",
+                  constant_cameras=(0,))
+    if want("ba_cluster_uniform"):
+        make_case(tc, ex, "ba_cluster_uniform", S.make_small_ba(8, 80, 3, seed=17), solver="ITERATIVE_SCHUR",
+                  preconditioner="CLUSTER_JACOBI", clustering="SINGLE_LINKAGE")
     if args.big and want("config0_dense"):
         make_case(tc, ex, "config0_dense", S.ba_config(0), solver="DENSE_SCHUR")
     if args.big and want("config1_small"):

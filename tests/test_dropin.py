@@ -124,8 +124,11 @@ def test_route_decisions():
     ok, why = dropin.route(ct.SolverOptions(linear_solver_type=ct.LinearSolverType.DENSE_QR), problem)
     assert not ok and "Schur" in why
     ok, why = dropin.route(ct.SolverOptions(linear_solver_type=ct.LinearSolverType.ITERATIVE_SCHUR,
-                                            preconditioner_type=ct.PreconditionerType.CLUSTER_JACOBI), problem)
-    assert not ok and "CLUSTER_JACOBI" in why
+                                            preconditioner_type=ct.PreconditionerType.CLUSTER_TRIDIAGONAL), problem)
+    assert not ok and "CUDA" in why  # the preconditioner is a GPU one; the tensors are not on a GPU
+    ok, why = dropin.route(ct.SolverOptions(linear_solver_type=ct.LinearSolverType.CGNR,
+                                            preconditioner_type=ct.PreconditionerType.SUBSET), problem)
+    assert not ok and "Schur" in why
     ok, why = dropin.route(ct.SolverOptions(minimizer_type=ct.MinimizerType.LINE_SEARCH,
                                             linear_solver_type=ct.LinearSolverType.DENSE_SCHUR), problem)
     assert not ok

@@ -30,7 +30,8 @@ def _ref_loss(spec):
 
 
 @pytest.mark.parametrize("name,precision,rtol", [("ba_small_sparse", "fp64", 1e-9), ("config1_small", "fp64", 1e-9),
-                                                 ("ba_cauchy", "fp64", 1e-9), ("ba_cauchy", "mixed", 1e-6)])
+                                                 ("ba_cauchy", "fp64", 1e-9), ("ba_cauchy", "mixed", 1e-6),
+                                                 ("ba_cluster_tridiagonal", "fp64", 1e-9)])
 def test_reference_solve_routes_to_the_gpu_and_matches_its_fixture(name, precision, rtol):
     d = G.load(name)
     meta = d["meta"]

@@ -211,7 +211,7 @@ def test_unsupported_problems_fail_loudly():
         tc.solve(opts, problem)  # CPU tensors: no CPU path
     with pytest.raises(NotImplementedError, match="SCHUR"):
         tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.DENSE_QR), problem)
-    with pytest.raises(NotImplementedError, match="CLUSTER_JACOBI"):
+    with pytest.raises(NotImplementedError, match="CUDA"):  # a GPU preconditioner, CPU tensors
         tc.solve(tc.SolverOptions(linear_solver_type=tc.LinearSolverType.ITERATIVE_SCHUR,
                                   preconditioner_type=tc.PreconditionerType.CLUSTER_JACOBI), problem)
 
