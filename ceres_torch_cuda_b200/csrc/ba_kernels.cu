@@ -1801,49 +1801,167 @@ __global__ void k_cluster_zero(ClusterArgs cl, long long num_elements, int pass)
 }
 
 // In-place inversion of every component matrix by the symmetric sweep operator, all
-// components at once, pivot k of each in step k, a grid barrier per step. Sweeping pivot
-// k with d = a_kk: a_kk <- -1/d, a_ik <- a_ik / d, a_kj <- a_kj / d, a_ij <- a_ij - a_ik a_kj / d.
-// The matrix stays symmetric, so column k is row k, and row k is read from a copy made
-// in the previous step (piv, two rows per component, alternating), which lets every
-// element be updated in place in one step. After the last pivot the matrix is -A^-1;
-// the epilogue negates it. The pivots d are those of A's LDL^T factorisation: all are
-// positive exactly when A is positive definite (the test torch.linalg.cholesky makes,
-// linear.py:1141-1145); a non-positive pivot sets flags[pass], a zero or non-finite one
-// flags[2]. Pass 1 runs only when pass 0 found its matrix not positive definite.
+// components at once, in blocks of kSweepBlock pivots. Sweeping the pivot set K of a
+// symmetric A = [[A11, A12], [A21, A22]] (1 = K):
+//   A11 <- -A11^-1,  A12 <- A11^-1 A12,  A21 <- A21 A11^-1,  A22 <- A22 - A21 A11^-1 A12;
+// sweeping every pivot once leaves -A^-1 (the epilogue negates it). Per block, three
+// phases with a grid barrier after each:
+//   1. the block's rows are copied (P = A[K, :]); the CTA of each component inverts A11
+//      (taken from P: the current Schur complement) by the single-pivot sweep in shared
+//      memory, whose pivots are A's LDL^T pivots: all positive exactly when A is positive
+//      definite (the test torch.linalg.cholesky makes, linear.py:1141-1145); a
+//      non-positive one sets flags[pass], a zero or non-finite one flags[2];
+//   2. W = A11^-1 P (kSweepBlock x dim);
+//   3. every element in 32 x 32 tiles: A22 -= P^T W (A21 = P^T by symmetry), A12 = W,
+//      A21 = W^T, A11 = -A11^-1; the tile's P and W columns staged in shared memory.
+// A tile may go to a different CTA in each block, so A is read with ld.global.cg (L1 is
+// not coherent across SMs).
+// Pass 1 runs only when pass 0 found its matrix not positive definite.
+constexpr int kSweepBlock = 32;
+constexpr int kSweepTile = 32;
+
 __global__ void __launch_bounds__(256) k_cluster_sweep(ClusterArgs cl, GridBarrier gb, int pass) {
   if (pass == 1 && *reinterpret_cast<volatile unsigned*>(cl.flags) == 0u) return;
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nthreads = (long long)gridDim.x * blockDim.x;
-  for (int c = 0; c < cl.num_components; ++c) {
-    const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
-    const double* M = cl.inv + cl.comp_base[c];
-    double* pv = cl.piv + cl.comp_piv[c];
-    for (long long j = tid; j < dim; j += nthreads) pv[j] = M[j];
-  }
-  if (!grid_sync(gb)) return;
-  for (int k = 0; k < cl.max_dim; ++k) {
+  __shared__ double sa[kSweepBlock][kSweepBlock + 1];
+  __shared__ double spi[kSweepBlock][kSweepTile];  // P[:, I]
+  __shared__ double swi[kSweepBlock][kSweepTile];  // W[:, I]
+  __shared__ double swj[kSweepBlock][kSweepTile];  // W[:, J]
+  __shared__ double sd;
+  const int tid = threadIdx.x;
+  const long long gtid = blockIdx.x * (long long)blockDim.x + tid;
+  const long long gthreads = (long long)gridDim.x * blockDim.x;
+  const int nblocks = (cl.max_dim + kSweepBlock - 1) / kSweepBlock;
+  for (int kb = 0; kb < nblocks; ++kb) {
+    const int k0 = kb * kSweepBlock;
+    // ---- phase 1: P = A[K, :]; A11^-1 per component (component c on CTA c mod grid)
     for (int c = 0; c < cl.num_components; ++c) {
       const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
-      if (dim <= k) continue;
-      double* __restrict__ M = cl.inv + cl.comp_base[c];
-      const double* __restrict__ pk = cl.piv + cl.comp_piv[c] + (size_t)(k & 1) * dim;
-      double* __restrict__ pn = cl.piv + cl.comp_piv[c] + (size_t)((k + 1) & 1) * dim;
-      const double d = ld_cross(pk + k);
-      const double rd = 1.0 / d;
-      const unsigned udim = (unsigned)dim, n2 = udim * udim;  // dim <= 16384 (checked on the host)
-      for (unsigned e = (unsigned)tid; e < n2; e += (unsigned)nthreads) {
-        const int i = (int)(e / udim), j = (int)(e - (unsigned)i * udim);
-        double v;
-        if (i == k) v = (j == k) ? -rd : ld_cross(pk + j) * rd;
-        else if (j == k) v = ld_cross(pk + i) * rd;
-        else v = M[e] - ld_cross(pk + i) * ld_cross(pk + j) * rd;
-        M[e] = v;
-        if (i == k + 1) pn[j] = v;
+      if (dim <= k0) continue;
+      const int bk = min(kSweepBlock, dim - k0);
+      const double* A = cl.inv + cl.comp_base[c];
+      double* P = cl.piv + cl.comp_piv[c];
+      const long long n = (long long)bk * dim;
+      for (long long e = gtid; e < n; e += gthreads) {
+        const int k = (int)(e / dim), j = (int)(e - (long long)k * dim);
+        P[e] = ld_cross(A + (size_t)(k0 + k) * dim + j);
       }
-      if (tid == 0) {
-        if (!(d > 0.0)) atomicOr(cl.flags + pass, 1u);
-        if (d == 0.0 || !isfinite(d)) atomicOr(cl.flags + 2, 1u);
+    }
+    for (int c = blockIdx.x; c < cl.num_components; c += gridDim.x) {
+      const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
+      if (dim <= k0) continue;
+      const int bk = min(kSweepBlock, dim - k0);
+      const double* A = cl.inv + cl.comp_base[c];
+      double* Ainv = cl.piv + cl.comp_piv[c] + 2 * (size_t)kSweepBlock * dim;
+      for (int e = tid; e < bk * bk; e += blockDim.x) {
+        const int i = e / bk, j = e - (e / bk) * bk;
+        sa[i][j] = ld_cross(A + (size_t)(k0 + i) * dim + k0 + j);
       }
+      __syncthreads();
+      for (int k = 0; k < bk; ++k) {
+        if (tid == 0) {
+          const double d = sa[k][k];
+          sd = d;
+          if (!(d > 0.0)) atomicOr(cl.flags + pass, 1u);
+          if (d == 0.0 || !isfinite(d)) atomicOr(cl.flags + 2, 1u);
+        }
+        __syncthreads();
+        const double rd = 1.0 / sd;
+        // the single-pivot sweep of k; every element read before any thread writes (256
+        // threads x 4 >= 32 x 32 elements)
+        double v[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int e = tid + 256 * m;
+          v[m] = 0.0;
+          if (e < bk * bk) {
+            const int i = e / bk, j = e - (e / bk) * bk;
+            if (i == k) v[m] = (j == k) ? -rd : sa[k][j] * rd;
+            else if (j == k) v[m] = sa[i][k] * rd;
+            else v[m] = sa[i][j] - sa[i][k] * sa[k][j] * rd;
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int e = tid + 256 * m;
+          if (e < bk * bk) sa[e / bk][e - (e / bk) * bk] = v[m];
+        }
+        __syncthreads();
+      }
+      for (int e = tid; e < bk * bk; e += blockDim.x) Ainv[e] = -sa[e / bk][e - (e / bk) * bk];  // +A11^-1
+      __syncthreads();
+    }
+    if (!grid_sync(gb)) return;
+    // ---- phase 2: W = A11^-1 P
+    for (int c = 0; c < cl.num_components; ++c) {
+      const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
+      if (dim <= k0) continue;
+      const int bk = min(kSweepBlock, dim - k0);
+      const double* P = cl.piv + cl.comp_piv[c];
+      double* W = cl.piv + cl.comp_piv[c] + (size_t)kSweepBlock * dim;
+      const double* Ainv = cl.piv + cl.comp_piv[c] + 2 * (size_t)kSweepBlock * dim;
+      const long long n = (long long)bk * dim;
+      for (long long e = gtid; e < n; e += gthreads) {
+        const int k = (int)(e / dim), j = (int)(e - (long long)k * dim);
+        double w = 0.0;
+        for (int m = 0; m < bk; ++m) w += ld_cross(Ainv + k * bk + m) * ld_cross(P + (size_t)m * dim + j);
+        W[e] = w;
+      }
+    }
+    if (!grid_sync(gb)) return;
+    // ---- phase 3: the tiles (a global tile index over the components, CTA-strided)
+    long long tile_base = 0;
+    const int ty = tid / 16, tx = tid - 16 * (tid / 16);  // 16 x 16 threads, 2 x 2 elements each
+    for (int c = 0; c < cl.num_components; ++c) {
+      const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
+      if (dim <= k0) continue;
+      const int bk = min(kSweepBlock, dim - k0);
+      const int nt = (dim + kSweepTile - 1) / kSweepTile;
+      const long long ntiles = (long long)nt * nt;
+      double* A = cl.inv + cl.comp_base[c];
+      const double* P = cl.piv + cl.comp_piv[c];
+      const double* W = cl.piv + cl.comp_piv[c] + (size_t)kSweepBlock * dim;
+      const double* Ainv = cl.piv + cl.comp_piv[c] + 2 * (size_t)kSweepBlock * dim;
+      long long t = ((blockIdx.x - tile_base) % gridDim.x + gridDim.x) % gridDim.x;
+      for (; t < ntiles; t += gridDim.x) {
+        const int i0 = (int)(t / nt) * kSweepTile, j0 = (int)(t % nt) * kSweepTile;
+        for (int e = tid; e < bk * kSweepTile; e += blockDim.x) {
+          const int k = e / kSweepTile, l = e - (e / kSweepTile) * kSweepTile;
+          const bool ri = i0 + l < dim, rj = j0 + l < dim;
+          spi[k][l] = ri ? ld_cross(P + (size_t)k * dim + i0 + l) : 0.0;
+          swi[k][l] = ri ? ld_cross(W + (size_t)k * dim + i0 + l) : 0.0;
+          swj[k][l] = rj ? ld_cross(W + (size_t)k * dim + j0 + l) : 0.0;
+        }
+        __syncthreads();
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        for (int k = 0; k < bk; ++k) {
+          const double pa0 = spi[k][2 * ty], pa1 = spi[k][2 * ty + 1];
+          const double wb0 = swj[k][2 * tx], wb1 = swj[k][2 * tx + 1];
+          acc[0][0] += pa0 * wb0;
+          acc[0][1] += pa0 * wb1;
+          acc[1][0] += pa1 * wb0;
+          acc[1][1] += pa1 * wb1;
+        }
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+          const int i = i0 + 2 * ty + a;
+          if (i >= dim) continue;
+          const bool ik = i >= k0 && i < k0 + bk;
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            const int j = j0 + 2 * tx + b;
+            if (j >= dim) continue;
+            const bool jk = j >= k0 && j < k0 + bk;
+            double* out = A + (size_t)i * dim + j;
+            if (ik && jk) *out = -ld_cross(Ainv + (i - k0) * bk + (j - k0));
+            else if (ik) *out = swj[i - k0][2 * tx + b];
+            else if (jk) *out = swi[j - k0][2 * ty + a];
+            else *out = ld_cross(out) - acc[a][b];
+          }
+        }
+        __syncthreads();
+      }
+      tile_base += ntiles;
     }
     if (!grid_sync(gb)) return;
   }
@@ -1851,7 +1969,7 @@ __global__ void __launch_bounds__(256) k_cluster_sweep(ClusterArgs cl, GridBarri
     const int dim = 9 * (cl.comp_cam_off[c + 1] - cl.comp_cam_off[c]);
     double* M = cl.inv + cl.comp_base[c];
     const long long n2 = (long long)dim * dim;
-    for (long long e = tid; e < n2; e += nthreads) M[e] = -M[e];
+    for (long long e = gtid; e < n2; e += gthreads) M[e] = -ld_cross(M + e);
   }
 }
 

@@ -208,10 +208,16 @@ class BAEngine:
         self.cand_points = torch.zeros((npq, 3), **f64)
         self.best_points = torch.zeros((npq, 3), **f64)
         self.jac = torch.zeros((nslot, 24), dtype=T, device=dev)
-        # camera-major copy of the Jacobian store (the camera-side passes stream it instead
-        # of gathering records by slot); CERES_B200_CAMERA_COPY=0 leaves it out
-        self.camera_copy = os.environ.get("CERES_B200_CAMERA_COPY", "1") != "0" if camera_copy is None \
-            else bool(camera_copy)
+        # camera-major copy of the Jacobian store: the camera-side passes stream it instead of
+        # gathering records by slot. It pays for itself with 96-byte float32 records (6.0M
+        # observations: 1.68 against 1.80 ms per LM iteration) but not with 192-byte float64
+        # records, whose second copy costs the evaluator more (0.85 against 0.44 ms) than the
+        # streaming saves (2.53 against 2.41 ms per LM iteration), so by default only the
+        # mixed path keeps it. CERES_B200_CAMERA_COPY=1/0 overrides the default.
+        env = os.environ.get("CERES_B200_CAMERA_COPY")
+        if camera_copy is None:
+            camera_copy = (env != "0") if env is not None else precision == "mixed"
+        self.camera_copy = bool(camera_copy)
         self.cm_jac = torch.zeros((max(self.no, 1), 24), dtype=T, device=dev) if self.camera_copy else None
         self.res = torch.zeros((nslot, 2), **f64)
         self.point_raw = torch.zeros((npq, 9), **f64)
@@ -464,7 +470,7 @@ class ClusterPlan:
         comp_cams = np.concatenate([active[g] for g in comps]).astype(np.int32)
         comp_cam_off = np.concatenate([[0], np.cumsum([g.size for g in comps])]).astype(np.int32)
         comp_base = np.concatenate([[0], np.cumsum(dims * dims)]).astype(np.int64)
-        comp_piv = np.concatenate([[0], np.cumsum(2 * dims)]).astype(np.int64)
+        comp_piv = np.concatenate([[0], np.cumsum(64 * dims + 32 * 32)]).astype(np.int64)  # P, W, A11^-1
         # every camera's observations by point lane (the pair kernel looks points up)
         L = eng.layout
         ents = L.cam_entries[:eng.no].to(torch.int64)

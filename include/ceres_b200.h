@@ -349,9 +349,11 @@ typedef struct ceres_b200_clusters {
   const int32_t* comp_cam_off; /* [num_components + 1] */
   const int64_t* comp_base;    /* [num_components + 1] first element of the component's
                                 * matrix in inv (row-major, dim x dim) */
-  const int64_t* comp_piv;     /* [num_components + 1] first element of its two pivot rows in piv */
+  const int64_t* comp_piv;     /* [num_components + 1] first element of its sweep workspace in piv:
+                                * 64 x dim + 32 x 32 doubles (a block's 32 rows, A11^-1 times them,
+                                * and the block's inverse) */
   double* inv;                 /* [comp_base[num_components]] the kept matrices, then their inverses */
-  double* piv;                 /* [comp_piv[num_components]] pivot rows of the sweep */
+  double* piv;                 /* [comp_piv[num_components]] sweep workspace */
   uint32_t* flags;             /* [8], zeroed by cluster_factor: [0] the kept matrix was not
                                 * positive definite, [1] nor was the halved one, [2] a zero
                                 * pivot, [3..5] grid barrier words ([5]: CERES_B200_DEVERR_BARRIER
@@ -365,7 +367,8 @@ int ceres_b200_clusters_struct_bytes(void);
  * Builds the kept matrices of S at the current assembly (float64 arithmetic on the
  * Jacobian store, deterministic: one warp per block pair, shared points in point order)
  * and inverts them with the symmetric sweep operator in one cooperative launch (all
- * components at once, a grid barrier per pivot). Non-positive pivots set flags[0]; with
+ * components at once, 32 pivots per block, three grid barriers per block). Non-positive
+ * pivots set flags[0]; with
  * tridiagonal set, the matrices are rebuilt with the blocks between different clusters
  * halved and inverted again (flags[1] when that one is not positive definite either,
  * where the reference falls back to a general solve of the same matrix, which the
