@@ -358,7 +358,7 @@ def run_ours(args):
 
     def ttt_solve(precision, problem=None, profile=False, k=None):
         s = tc.solve(opts, problem if problem is not None else problem_from_device(k), precision=precision,
-                     target_cost=target, stop_at_target=True, profile=profile)
+                     target_cost=target, stop_at_target=True, profile=profile, autotune=not args.no_autotune)
         return s, (s.time_to_tolerance_in_seconds if s.time_to_tolerance_in_seconds is not None else float("inf"))
 
     for _ in range(args.warmup):
@@ -395,7 +395,7 @@ def run_ours(args):
     # profile pass: per-kernel CUDA-event times on one more solve (same stream)
     prob = problem_from_device()
     s_prof, eng = tc.solve(opts, prob, precision="mixed", target_cost=target, stop_at_target=True,
-                           return_engine=True)
+                           return_engine=True, autotune=not args.no_autotune)
     prof = profile_kernels(tc, eng, opts)
 
     # e2e through the public API from pinned host buffers
@@ -450,6 +450,7 @@ def run_ours(args):
                        "N(0,1)), seed 1000 + k, the same starts for both precisions; value = median over the starts",
                        "unjittered_start": {p: {"time_to_tol_s": t, "iterations_to_tol": len(s.iterations)}
                                             for p, (s, t) in unjittered.items()}},
+            "kernel_config": {"mixed": summaries[-1].kernel_config, "fp64": fp64_runs[-1][0].kernel_config},
             "fp64": {"time_to_tol_s": fp64_ttt, "solve_to_minimum_s": fp64_seconds,
                      "iterations_to_minimum": len(s64.iterations),
                      "iterations_to_tol": len(fp64_runs[-1][0].iterations),
@@ -779,6 +780,8 @@ def main():
     ap.add_argument("--kernel-pass", action="store_true",
                     help="run one LM iteration's kernels twice (for profiler captures) and exit")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="fixed defaults instead of the single-problem autotuner (camera-major copy, item length)")
     ap.add_argument("--preconditioner", default="SCHUR_JACOBI",
                     choices=["SCHUR_JACOBI", "JACOBI", "SCHUR_POWER_SERIES_EXPANSION", "CLUSTER_JACOBI",
                              "CLUSTER_TRIDIAGONAL"],

@@ -702,7 +702,9 @@ __device__ __forceinline__ int camera_pass_item(const ceres_b200_ba_t& ba, const
                                                 const double* __restrict__ sv, int item, int lane, A y[9]) {
   const int2 it = reinterpret_cast<const int2*>(ba.items)[item];
   const int c = it.x, e0 = it.y;
-  const int e1 = min(e0 + CERES_B200_CAM_ITEM, ba.cam_offsets[c + 1]);
+  // the item ends where the camera's next item starts, or with the camera's entries
+  const int e1 = item + 1 < ba.cam_items[c + 1] ? reinterpret_cast<const int2*>(ba.items)[item + 1].y
+                                                : ba.cam_offsets[c + 1];
   const T* __restrict__ cm = reinterpret_cast<const T*>(ba.cm_jac);
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);

@@ -64,7 +64,7 @@ class Layout:
 
 
 def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observations: torch.Tensor,
-                 num_cameras: int, num_points: int) -> Layout:
+                 num_cameras: int, num_points: int, item_size: int | None = None) -> Layout:
     """Bucket observations by point (stable in observation order) into slices of
     32 points sorted by track length, and list them per camera. GPU torch ops."""
     dev = camera_index.device
@@ -111,7 +111,8 @@ def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observat
     if no:
         pk = torch.sort(pi * max(num_cameras, 1) + ci).values
         has_dup = bool((pk[1:] == pk[:-1]).any()) if no > 1 else False
-    slot_pos, cam_items, items, max_cam = camera_items(cam_entries if no else cam_entries[:0], cam_counts, num_slots)
+    slot_pos, cam_items, items, max_cam = camera_items(cam_entries if no else cam_entries[:0], cam_counts, num_slots,
+                                                       item_size)
     return Layout(
         num_slices=num_slices, num_slots=num_slots,
         max_slice_len=int(slice_len.max()) if num_slices else 0,
@@ -124,25 +125,28 @@ def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observat
     )
 
 
-def camera_items(cam_entries: torch.Tensor, cam_counts: torch.Tensor, num_slots: int):
+def camera_items(cam_entries: torch.Tensor, cam_counts: torch.Tensor, num_slots: int, item_size: int | None = None):
     """The camera-major position of every slot (inverse of cam_entries' slot column,
     -1 for padding) and the camera work items: each camera's entries cut into runs of
-    at most CAM_ITEM (include/ceres_b200.h). Returns (slot_pos, cam_items, items,
-    largest camera entry count)."""
+    ``item_size`` (default CAM_ITEM, include/ceres_b200.h). Returns (slot_pos, cam_items,
+    items, largest camera entry count)."""
+    item = int(item_size or _lib.CAM_ITEM)
+    if item < 1:
+        raise ValueError("item_size must be positive")
     dev = cam_counts.device
     no = int(cam_entries.shape[0])
     nc = int(cam_counts.numel())
     slot_pos = torch.full((max(num_slots, 1),), -1, dtype=torch.int32, device=dev)
     if no:
         slot_pos[cam_entries[:, 0].long()] = torch.arange(no, dtype=torch.int32, device=dev)
-    per_cam = (cam_counts + _lib.CAM_ITEM - 1) // _lib.CAM_ITEM
+    per_cam = (cam_counts + item - 1) // item
     cam_items = torch.zeros(nc + 1, dtype=torch.int64, device=dev)
     cam_items[1:] = torch.cumsum(per_cam, 0)
     n_items = int(cam_items[-1]) if nc else 0
     if n_items:
         item_cam = torch.repeat_interleave(torch.arange(nc, device=dev), per_cam)
         start = torch.cumsum(cam_counts, 0) - cam_counts
-        first = start[item_cam] + _lib.CAM_ITEM * (torch.arange(n_items, device=dev) - cam_items[item_cam])
+        first = start[item_cam] + item * (torch.arange(n_items, device=dev) - cam_items[item_cam])
         items = torch.stack([item_cam, first], dim=1).to(torch.int32).contiguous()
     else:
         items = torch.zeros((1, 2), dtype=torch.int32, device=dev)
@@ -156,7 +160,8 @@ class BAEngine:
     def __init__(self, cameras: torch.Tensor, points: torch.Tensor, observations: torch.Tensor,
                  camera_index: torch.Tensor, point_index: torch.Tensor, *, loss=None,
                  camera_constant: torch.Tensor | None = None, point_constant: torch.Tensor | None = None,
-                 precision: str = "fp64", layout: Layout | None = None, camera_copy: bool | None = None):
+                 precision: str = "fp64", layout: Layout | None = None, camera_copy: bool | None = None,
+                 item_size: int | None = None):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         if cameras.device.type != "cuda":
@@ -180,7 +185,8 @@ class BAEngine:
         if not torch.isfinite(observations).all():
             raise ValueError("observations must be finite")
         self.layout = layout or build_layout(camera_index.to(dev), point_index.to(dev), observations.to(dev),
-                                             self.nc, self.np)
+                                             self.nc, self.np, item_size)
+        self.item_size = int(item_size or _lib.CAM_ITEM)
         self._index = (camera_index, point_index, point_constant)
         self.clusters: ClusterPlan | None = None
         L = self.layout
@@ -345,6 +351,24 @@ class BAEngine:
             if self.clusters is None:
                 raise RuntimeError("setup_clusters() first")
             self._call("ceres_b200_ba_cluster_factor", ctypes.byref(self.clusters.struct))
+
+    def retile_items(self, item_size: int) -> None:
+        """Cut the cameras' entries into work items of ``item_size`` entries (the
+        camera pass's unit of work; the autotuner's knob) and resize the scratch."""
+        L = self.layout
+        cam_counts = (L.cam_offsets[1:] - L.cam_offsets[:-1]).to(torch.int64)
+        ents = L.cam_entries if self.no else L.cam_entries[:0]
+        _, L.cam_items, L.items, _ = camera_items(ents, cam_counts, L.num_slots, item_size)
+        self.item_size = int(item_size)
+        s = self.struct
+        s.cam_items, s.items = _ptr(L.cam_items), _ptr(L.items)
+        s.num_items = int(L.cam_items[-1]) if self.nc else 0
+        nbytes = ctypes.c_int64(0)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.ceres_b200_scratch_bytes(ctypes.byref(s), ctypes.byref(nbytes)), "scratch size")
+        if int(nbytes.value) > self.scratch.numel():
+            self.scratch = torch.zeros(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        s.scratch, s.scratch_bytes = self.scratch.data_ptr(), int(self.scratch.numel())
 
     def setup_clusters(self, tridiagonal: bool, clustering: str = "CANONICAL_VIEWS") -> bool:
         """Cluster the active cameras by visibility (linear.py:953-990) and allocate the

@@ -9,6 +9,7 @@ NotImplementedError; there is no CPU path.
 """
 from __future__ import annotations
 
+import os
 import time
 
 import torch
@@ -60,7 +61,7 @@ def _check_supported(options: SolverOptions) -> None:
 
 def solve(options: SolverOptions, problem, *, precision: str | None = None, max_refinements: int = 1,
           target_cost: float | None = None, stop_at_target: bool = False, return_engine: bool = False,
-          profile: bool = False):
+          profile: bool = False, autotune: bool | None = None):
     """Solve ``problem`` in place and return the SolverSummary.
 
     ``precision`` overrides the registered precision ("fp64" or "mixed").
@@ -69,6 +70,10 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
     ``profile`` brackets every library call with CUDA events (no extra
     synchronisation) and puts the per-entry-point device times in
     ``summary.kernel_profile``.
+    ``autotune`` (default: the CERES_B200_AUTOTUNE environment variable) picks the
+    camera-major copy and the camera work-item length by timing them on this problem
+    (``autotune.tune``, cached per size class); the choice is in
+    ``summary.kernel_config``.
     """
     if not isinstance(options, SolverOptions):
         from .dropin import options_from
@@ -109,8 +114,22 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
         raise TypeError("problem must be a Problem or a BundleAdjustmentProblem")
     if cams.device.type != "cuda":
         raise NotImplementedError("the solver runs on CUDA tensors only; move the parameter blocks to a CUDA device")
-    engine = BAEngine(cams, pts, obs, ci, pi, loss=loss, camera_constant=cam_const, point_constant=pt_const,
-                      precision=prec)
+    if autotune is None:
+        autotune = os.environ.get("CERES_B200_AUTOTUNE", "0") == "1"
+    kernel_config = {"camera_copy": None, "item_size": None, "autotuned": False}
+    if autotune and obs.shape[0] > 0 and cams.shape[0] > 0:
+        from . import autotune as _at
+
+        cfg = _at.tune(cams, pts, obs, ci, pi, loss=loss, camera_constant=cam_const, point_constant=pt_const,
+                       precision=prec, options=options)
+        kernel_config = dict(cfg.as_dict(), autotuned=True)
+        engine = BAEngine(cams, pts, obs, ci, pi, loss=loss, camera_constant=cam_const, point_constant=pt_const,
+                          precision=prec, camera_copy=cfg.camera_copy, item_size=cfg.item_size)
+    else:
+        engine = BAEngine(cams, pts, obs, ci, pi, loss=loss, camera_constant=cam_const, point_constant=pt_const,
+                          precision=prec)
+    kernel_config["camera_copy"] = engine.camera_copy
+    kernel_config["item_size"] = engine.item_size
     n_active = summary.num_effective_parameters
     if profile:
         engine.enable_profiling()
@@ -129,6 +148,7 @@ def solve(options: SolverOptions, problem, *, precision: str | None = None, max_
     summary.total_time_in_seconds = time.perf_counter() - start
     summary.time_to_tolerance_in_seconds = result.time_to_tolerance
     summary.precision = prec
+    summary.kernel_config = kernel_config
     if profile:
         summary.kernel_profile = engine.profile_report()
     if return_engine:

@@ -285,6 +285,7 @@ class SolverSummary:
     precision: str = "fp64"
     time_to_tolerance_in_seconds: float | None = None
     kernel_profile: dict | None = None
+    kernel_config: dict | None = None   # camera-major copy and work-item length used (autotune.py)
 
     def IsSolutionUsable(self) -> bool:  # noqa: N802 - ceres-torch API name
         return self.termination_type in (TerminationType.CONVERGENCE, TerminationType.NO_CONVERGENCE,

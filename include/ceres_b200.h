@@ -105,10 +105,11 @@ enum {
  * (point-major) and at its camera-major position (cm_jac[e], e the entry's index
  * in cam_entries), and the camera-side passes stream the copy; with cm_jac null
  * they gather the records by slot.
- * Camera work items cut every camera's entries into runs of at most
- * CERES_B200_CAM_ITEM entries; item i = (camera, first entry) covers entries
- * first .. min(first + CERES_B200_CAM_ITEM, cam_offsets[camera + 1]) - 1, and
- * cam_items[c] .. cam_items[c + 1] - 1 are camera c's items.
+ * Camera work items cut every camera's entries into consecutive runs; item i =
+ * (camera, first entry) covers its entries up to the next item of the same camera
+ * (or the camera's last entry), and cam_items[c] .. cam_items[c + 1] - 1 are camera
+ * c's items. The run length is the host's choice (the autotuner picks it);
+ * CERES_B200_CAM_ITEM is the default.
  */
 #define CERES_B200_CAM_ITEM 256
 typedef struct ceres_b200_ba_t {

@@ -110,3 +110,18 @@ def test_layout_of_a_ragged_problem():
     _check_invariants(L, d.camera_index, d.point_index, d.observations, d.num_cameras, d.num_points)
     # padding overhead of the sliced store stays small with length-sorted slices
     assert L.num_slots <= 1.3 * d.num_observations
+
+
+@pytest.mark.parametrize("item_size", [1, 32, 128, 256, 1024])
+def test_camera_work_items_of_any_length(item_size):
+    """The autotuner's item lengths: every camera's entries are cut into consecutive
+    runs of ``item_size`` (the last one shorter), in order, none empty."""
+    d = S.make_ring_ba(40, 900, seed=3)
+    L = build_layout(torch.as_tensor(d.camera_index), torch.as_tensor(d.point_index),
+                     torch.as_tensor(d.observations), 40, 900, item_size)
+    items, ci_off, off = L.items.numpy(), L.cam_items.numpy(), L.cam_offsets.numpy()
+    assert ci_off[-1] == sum(-(-(off[c + 1] - off[c]) // item_size) for c in range(40))
+    for c in range(40):
+        firsts = items[ci_off[c]:ci_off[c + 1]]
+        assert (firsts[:, 0] == c).all()
+        np.testing.assert_array_equal(firsts[:, 1], np.arange(off[c], off[c + 1], item_size))
