@@ -659,6 +659,29 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
     evaluator = _StepEvaluator(cost, options.max_consecutive_nonmonotonic_steps if options.use_nonmonotonic_steps else 0)
     need_assemble = False
     terminated = False
+    # After an accepted step the evaluation and assembly at the new point are launched
+    # without waiting for their statistics: the next PCG and step are queued behind them
+    # and one read after the step brings both (their statistics slots are disjoint). The
+    # gradient test of the new point then runs before anything of the next iteration is
+    # used, so the iterations, counters and terminations are those of the unpipelined
+    # loop; a solve that stops there has launched one PCG and step for nothing.
+    pending_eval = False
+
+    def take_evaluation(st) -> bool:
+        """The new point's cost and gradient from ``st``; True when its gradient test ends
+        the solve (solver.py:1165-1175)."""
+        nonlocal cost, gmax, gnorm, pending_eval, terminated
+        pending_eval = False
+        cost = float(st[_lib.STAT_COST])
+        gmax = max(st[_lib.STAT_GMAX_P], st[_lib.STAT_GMAX_C])
+        gnorm = math.sqrt(st[_lib.STAT_GSQ_P] + st[_lib.STAT_GSQ_C])
+        if gmax <= options.gradient_tolerance:
+            summary.termination_type = TerminationType.CONVERGENCE
+            summary.message = "Gradient tolerance reached."
+            summary.final_cost = cost
+            terminated = True
+            return True
+        return False
 
     def finalize() -> LMResult:
         if summary.minimizer_time_in_seconds == 0.0:
@@ -716,6 +739,11 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
                        options.eta, refinements, options.max_num_spse_iterations, options.spse_tolerance, spse_init)
         engine.step()
         st = engine.read_stats()
+        if pending_eval:
+            if take_evaluation(st):
+                summary.num_jacobian_evaluations -= 1  # this iteration never started
+                break
+            it.cost, it.gradient_norm, it.gradient_max_norm = cost, gnorm, gmax
         lin_time = time.perf_counter() - lin_start
         if kind != "dense":
             lin_iters = int(st[_lib.STAT_PCG_ITERS]) if engine.nc else 1
@@ -834,18 +862,14 @@ def run_lm(engine: BAEngine, options: SolverOptions, summary: SolverSummary, *, 
             t0 = time.perf_counter()
             engine.evaluate(True)
             engine.assemble(radius, options, precond, spse_base)
-            st = engine.read_stats()
-            jt = time.perf_counter() - t0
-            summary.jacobian_evaluation_time_in_seconds += jt
+            summary.jacobian_evaluation_time_in_seconds += time.perf_counter() - t0  # launch time
             summary.num_jacobian_evaluations += 1
-            cost = float(st[_lib.STAT_COST])
-            gmax = max(st[_lib.STAT_GMAX_P], st[_lib.STAT_GMAX_C])
-            gnorm = math.sqrt(st[_lib.STAT_GSQ_P] + st[_lib.STAT_GSQ_C])
-            if gmax <= options.gradient_tolerance:
-                summary.termination_type = TerminationType.CONVERGENCE
-                summary.message = "Gradient tolerance reached."
-                summary.final_cost = cost
-                terminated = True
+            pending_eval = True
+        stopping = radius <= options.min_trust_region_radius or \
+            time.perf_counter() - start >= options.max_solver_time_in_seconds
+        if pending_eval and (stopping or iteration == options.max_num_iterations):
+            # the new point's gradient test comes first, as in the unpipelined loop
+            if take_evaluation(engine.read_stats()):
                 break
         if radius <= options.min_trust_region_radius:
             summary.termination_type = TerminationType.CONVERGENCE

@@ -57,7 +57,10 @@ def test_tuner_picks_a_candidate_and_caches_it():
     assert (cfg.camera_copy, cfg.item_size) in cfg.timings
     assert len(cfg.timings) == 2 * len(autotune.ITEM_SIZES)
     assert all(t["estimate"] > 0 for t in cfg.timings.values())
-    assert cfg.estimate_ms == min(t["estimate"] for t in cfg.timings.values())
+    best = min(t["estimate"] for t in cfg.timings.values())
+    assert cfg.estimate_ms <= (1.0 + autotune.MARGIN) * best
+    if (cfg.camera_copy, cfg.item_size) != (True, 256):  # left the default: clearly faster
+        assert cfg.estimate_ms == best
     assert autotune.tune(*arrays, loss=tc.CauchyLoss(2.0), precision="mixed") is cfg  # cached
 
 

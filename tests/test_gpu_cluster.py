@@ -145,3 +145,43 @@ def test_cluster_solves_are_reproducible(precision):
         runs.append(([it.cost for it in s.iterations], prob.cameras.cpu().numpy(), prob.points.cpu().numpy()))
     assert runs[0][0] == runs[1][0]
     assert np.array_equal(runs[0][1], runs[1][1]) and np.array_equal(runs[0][2], runs[1][2])
+
+
+@pytest.mark.parametrize("tridiagonal", [False, True])
+def test_cluster_inverses_with_repeated_observations(tridiagonal):
+    """A camera that sees a point twice: the kept blocks sum over all of the camera's
+    observations of each shared point (the diagonal block from the camera reduction's
+    duplicate-aware sums), so the inverses still equal those of the masked explicit S."""
+    tc = _tc()
+    from ceres_torch_cuda_b200 import _lib
+    from ceres_torch_cuda_b200 import clustering as C
+    from ceres_torch_cuda_b200 import synthetic as S
+
+    d = S.make_sequence_ba(10, 150, 3, seed=21)
+    rep = np.arange(0, d.num_observations, 7)  # every 7th observation recorded twice
+    ci = np.concatenate([d.camera_index, d.camera_index[rep]])
+    pi = np.concatenate([d.point_index, d.point_index[rep]])
+    ob = np.concatenate([d.observations, d.observations[rep] + 0.5])
+    t = lambda a, dt=torch.float64: torch.as_tensor(a).to(DEV, dt)  # noqa: E731
+    eng = tc.BAEngine(t(d.cameras), t(d.points), t(ob), t(ci, torch.int64), t(pi, torch.int64), precision="fp64")
+    assert eng.layout.has_duplicate_cameras
+    assert eng.setup_clusters(tridiagonal)
+    eng.evaluate(True)
+    eng.assemble(1e3, tc.SolverOptions(), _lib.PRECOND_CLUSTER)
+    S_ = torch.zeros((9 * eng.nc, 9 * eng.nc), dtype=torch.float64, device=DEV)
+    eng._call("ceres_b200_ba_schur_matrix", S_.data_ptr())
+    eng.read_stats()
+    flags = eng.cluster_flags()
+    S_ = S_.cpu().numpy()
+    st = C.cluster_structure(tridiagonal=tridiagonal, incidence=C.incidence_from_observations(eng.nc, ci, pi))
+    keep = np.zeros((eng.nc, eng.nc), dtype=bool)
+    for a, b in st.block_pairs():
+        keep[a, b] = keep[b, a] = True
+    M = np.where(np.kron(keep, np.ones((9, 9), bool)), S_, 0.0)
+    if flags[0]:
+        cross = keep & (st.membership[:, None] != st.membership[None, :])
+        M = np.where(np.kron(cross, np.ones((9, 9), bool)), 0.5 * M, M)
+    for comp, inv in zip(eng.clusters.components, eng.clusters.matrices()):
+        idx = (9 * comp[:, None] + np.arange(9)[None, :]).reshape(-1)
+        ref = np.linalg.inv(M[np.ix_(idx, idx)])
+        np.testing.assert_allclose(inv.cpu().numpy(), ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max())
