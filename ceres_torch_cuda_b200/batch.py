@@ -218,7 +218,7 @@ class BatchSolver:
         self.winv_ga = torch.empty((NQ, 3), **f64)
         self.step_points = torch.empty((NQ, 3), **f64)
         self.cam_diag = torch.empty((NC, 9), **f64)
-        self.precond = torch.empty((NC, 81), dtype=jt, device=dev)
+        self.precond = torch.empty((NC, 81), dtype=torch.float64, device=dev)  # float64 in both precisions
         self.rhs = torch.empty((NC, 9), **f64)
         self.step_cameras = torch.empty((NC, 9), **f64)
         self.cam_acc = torch.empty((NC, 72), **f64)

@@ -337,13 +337,13 @@ __device__ void warp_camera_finish(const ceres_b200_batch_t& B, int cg, double i
   constexpr unsigned kFull = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const double* sacc = B.cam_acc + (size_t)cg * 72;
-  T* pre = reinterpret_cast<T*>(B.precond) + 81 * (size_t)cg;
+  double* pre = reinterpret_cast<double*>(B.precond) + 81 * (size_t)cg;  // float64 in both precisions
   double* dc = B.cam_diag + 9 * (size_t)cg;
   double* rh = B.rhs + 9 * (size_t)cg;
   const double mn = B.min_lm_diagonal, mx = B.max_lm_diagonal;
   if (B.cam_const[cg]) {
     if (lane < 9) { dc[lane] = 0.0; rh[lane] = 0.0; }
-    for (int i = lane; i < 81; i += 32) pre[i] = (T)((i % 10 == 0) ? 1.0 : 0.0);
+    for (int i = lane; i < 81; i += 32) pre[i] = (i % 10 == 0) ? 1.0 : 0.0;
     return;
   }
   const int i = lane < 9 ? lane : 8;
@@ -400,7 +400,7 @@ __device__ void warp_camera_finish(const ceres_b200_batch_t& B, int cg, double i
       }
       if (lane < 9) {
 #pragma unroll
-        for (int r = 0; r < 9; ++r) pre[r * 9 + lane] = (T)x[r];
+        for (int r = 0; r < 9; ++r) pre[r * 9 + lane] = x[r];
       }
     } else if (lane == 0) {
       double Sm[81], inv[81];
@@ -413,15 +413,15 @@ __device__ void warp_camera_finish(const ceres_b200_batch_t& B, int cg, double i
         }
       }
       block9_inverse(Sm, inv);
-      for (int k = 0; k < 81; ++k) pre[k] = (T)inv[k];
+      for (int k = 0; k < 81; ++k) pre[k] = inv[k];
     }
   } else if (lane < 9) {
     double sii = 0.0;
 #pragma unroll
     for (int l = 0; l < 9; ++l) sii = (l == i) ? a[l] : sii;
-    const double v = (B.preconditioner == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(sii, Eps<T>::v()) : 1.0;
+    const double v = (B.preconditioner == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(sii, kEps64) : 1.0;
 #pragma unroll
-    for (int l = 0; l < 9; ++l) pre[i * 9 + l] = (T)(l == i ? v : 0.0);
+    for (int l = 0; l < 9; ++l) pre[i * 9 + l] = l == i ? v : 0.0;
   }
 }
 
@@ -510,8 +510,7 @@ __device__ void cl_schur_product(const ceres_b200_batch_t& B, const Prob& P, con
   }
 }
 
-template <typename T>
-__device__ __forceinline__ void precond_apply_b(const T* M, const double* r, double* z) {
+__device__ __forceinline__ void precond_apply_b(const double* M, const double* r, double* z) {
   double rr[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) rr[j] = r[j];
@@ -519,7 +518,7 @@ __device__ __forceinline__ void precond_apply_b(const T* M, const double* r, dou
   for (int i = 0; i < 9; ++i) {
     double s = 0.0;
 #pragma unroll
-    for (int j = 0; j < 9; ++j) s += (double)ldx(M + i * 9 + j) * rr[j];
+    for (int j = 0; j < 9; ++j) s += ldx(M + i * 9 + j) * rr[j];
     z[i] = s;
   }
 }
@@ -547,7 +546,7 @@ __device__ PcgOut cl_pcg(const ceres_b200_batch_t& B, const Prob& P, const Ctx& 
   double* Z = B.pcg + 2 * N + o;
   double* Pb[2] = {B.pcg + 3 * N + o, B.pcg + 4 * N + o};
   double* AP = B.pcg + 5 * N + o;
-  const T* Minv = reinterpret_cast<const T*>(B.precond) + 81 * (size_t)P.cam0;
+  const double* Minv = reinterpret_cast<const double*>(B.precond) + 81 * (size_t)P.cam0;
   const double* D = B.cam_diag + o;
   // the products stream the store in T and compute in float64 (float32 arithmetic adds
   // errors of 1e-7 |U| |p| per product that swamp the small eigenvalues of S once the

@@ -506,7 +506,7 @@ template <typename T>
 __global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_ba_t ba, const double* __restrict__ acc_in,
                                                                      double inv_radius, double mn, double mx,
                                                                      int jacobi_scaling, int precond, double* partials,
-                                                                     T* __restrict__ pre_out) {
+                                                                     double* __restrict__ pre_out) {
   constexpr unsigned kFull = 0xffffffffu;
   __shared__ double sred2[2 * kFinishWarps];
   const int lane = threadIdx.x & 31;
@@ -514,12 +514,12 @@ __global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_
   double gmax = 0.0, gsq = 0.0;
   if (c < ba.num_cameras) {  // uniform in the warp
     const double* sacc = acc_in + (size_t)c * kCamAcc;
-    T* __restrict__ pre = pre_out + 81 * (size_t)c;
+    double* __restrict__ pre = pre_out + 81 * (size_t)c;
     double* dc = ba.cam_diag + 9 * (size_t)c;
     double* rh = ba.rhs + 9 * (size_t)c;
     if (ba.cam_const[c]) {
       if (lane < 9) { dc[lane] = 0.0; rh[lane] = 0.0; }
-      for (int i = lane; i < 81; i += 32) pre[i] = (T)((i % 10 == 0) ? 1.0 : 0.0);
+      for (int i = lane; i < 81; i += 32) pre[i] = (i % 10 == 0) ? 1.0 : 0.0;
     } else {
       const int i = lane < 9 ? lane : 8;  // lanes 9..31 shadow row 8 and store nothing
       const double col = jacobi_scaling ? sacc[45 + i] : 1.0;
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_
           }
           if (lane < 9) {
 #pragma unroll
-            for (int r = 0; r < 9; ++r) pre[r * 9 + lane] = (T)x[r];
+            for (int r = 0; r < 9; ++r) pre[r * 9 + lane] = x[r];
           }
         } else if (lane == 0) {
           double S[81], inv[81];
@@ -588,15 +588,15 @@ __global__ void __launch_bounds__(32 * kFinishWarps) k_camera_finish(ceres_b200_
             }
           }
           block9_inverse(S, inv);
-          for (int k = 0; k < 81; ++k) pre[k] = (T)inv[k];
+          for (int k = 0; k < 81; ++k) pre[k] = inv[k];
         }
       } else if (lane < 9) {
         double sii = 0.0;
 #pragma unroll
         for (int l = 0; l < 9; ++l) sii = (l == i) ? a[l] : sii;
-        const double v = (precond == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(sii, Eps<T>::v()) : 1.0;
+        const double v = (precond == CERES_B200_PRECOND_JACOBI) ? 1.0 / fmax(sii, kEps64) : 1.0;
 #pragma unroll
-        for (int l = 0; l < 9; ++l) pre[i * 9 + l] = (T)(l == i ? v : 0.0);
+        for (int l = 0; l < 9; ++l) pre[i * 9 + l] = l == i ? v : 0.0;
       }
     }
   }
@@ -872,7 +872,7 @@ struct PcgArgs {
   // SCHUR_POWER_SERIES_EXPANSION (linear.py:59-67, :482-497, :745-756)
   int precond_series;      // z = sum_i (B E)^i B r with B = ba.precond (inverted damped Hbb blocks)
   int init_series;         // x0 = the series applied to rhs with B = init_blocks
-  const void* init_blocks; // [nc][81] T
+  const double* init_blocks; // [nc][81]
   int series_terms;        // max_num_spse_iterations (>= 1)
   double series_tol;       // spse_tolerance
   double* part_s;          // [G][2] partials of the series norms and of |r|^2
@@ -884,10 +884,9 @@ struct PcgArgs {
 constexpr int kPcgBlock = 512;
 constexpr int kStallWindow = 20;  // float32 PCG: iterations without a 1% residual drop before it stops
 
-template <typename T>
-__device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const double* __restrict__ r,
+__device__ __forceinline__ void precond_apply(const double* __restrict__ Minv, const double* __restrict__ r,
                                               double* __restrict__ z, int c) {
-  const T* M = Minv + 81 * (size_t)c;
+  const double* M = Minv + 81 * (size_t)c;
   const double* rc = r + 9 * (size_t)c;
   double rr[9];
 #pragma unroll
@@ -896,7 +895,7 @@ __device__ __forceinline__ void precond_apply(const T* __restrict__ Minv, const 
   for (int i = 0; i < 9; ++i) {
     double s = 0.0;
 #pragma unroll
-    for (int j = 0; j < 9; ++j) s += (double)M[i * 9 + j] * rr[j];
+    for (int j = 0; j < 9; ++j) s += M[i * 9 + j] * rr[j];
     z[9 * (size_t)c + i] = s;
   }
 }
@@ -975,7 +974,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   double* __restrict__ Z = reinterpret_cast<double*>(ba.pcg_z);
   double* __restrict__ Pbuf = reinterpret_cast<double*>(ba.pcg_p);
   double* __restrict__ AP = reinterpret_cast<double*>(ba.pcg_ap);
-  const T* __restrict__ Minv = reinterpret_cast<const T*>(ba.precond);
+  const double* __restrict__ Minv = reinterpret_cast<const double*>(ba.precond);
   const GridBarrier gb{&ba.counters[kCtrBarCount], &ba.counters[kCtrBarGen], &ba.counters[kCtrBarFlag], kSpinLimit};
   const int G = gridDim.x;
   const int c0 = blockIdx.x * a.cams_per_cta;
@@ -1028,7 +1027,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
   };
   // ---- the power series (linear.py:59-67): out = sum_i (B E)^i B in over this CTA's
   // cameras; term and w are scratch vectors (term is read by every CTA).
-  auto series = [&](const T* B, const double* in, double* out, double* term, double* w) -> bool {
+  auto series = [&](const double* B, const double* in, double* out, double* term, double* w) -> bool {
     __syncthreads();
     for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) precond_apply(B, in, out, c);
     __syncthreads();
@@ -1071,7 +1070,7 @@ __global__ void __launch_bounds__(kPcgBlock, 1) k_pcg(ceres_b200_ba_t ba, PcgArg
     {
       double rz = 0.0, rr0 = 0.0;
       if (init) {
-        if (!series(reinterpret_cast<const T*>(a.init_blocks), b, X, Pbuf + n, AP)) return false;
+        if (!series(a.init_blocks, b, X, Pbuf + n, AP)) return false;
         if (!grid_sync(gb)) return false;
         if (!product(X, Z, kProdS)) return false;
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) R[j] = b[j] - Z[j];
@@ -2097,7 +2096,7 @@ int pcg_layout(const ceres_b200_ba_t& ba, PcgLayout& L) {
   off += (size_t)n * sizeof(double);
   off = (off + 255) & ~(size_t)255;
   L.spse_base = off;
-  off += (size_t)(ba.num_cameras > 0 ? ba.num_cameras : 1) * 81 * sizeof(T);
+  off += (size_t)(ba.num_cameras > 0 ? ba.num_cameras : 1) * 81 * sizeof(double);
   L.total = (off + 255) & ~(size_t)255;
   return CERES_B200_OK;
 }
@@ -2114,7 +2113,7 @@ int scratch_bytes_impl(const ceres_b200_ba_t& ba, size_t& bytes) {
 struct SeriesOpts {
   int precond = 0, init = 0, terms = 1;
   double tol = 0.0;
-  const void* init_blocks = nullptr;
+  const double* init_blocks = nullptr;
 };
 
 template <typename T>
@@ -2206,7 +2205,7 @@ void camera_assemble_impl(const ceres_b200_ba_t& ba, const PcgLayout& L, char* s
   double* acc = reinterpret_cast<double*>(scratch + L.cam_acc);
   const int nc = ba.num_cameras;
   const int fgrid = (nc + kFinishWarps - 1) / kFinishWarps;
-  T* pre = reinterpret_cast<T*>(ba.precond);
+  double* pre = reinterpret_cast<double*>(ba.precond);
   const bool spse = pc == CERES_B200_PRECOND_SCHUR_POWER_SERIES;
   count_launch(2);
   if (spse) k_camera_reduce<T, false, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
@@ -2219,7 +2218,7 @@ void camera_assemble_impl(const ceres_b200_ba_t& ba, const PcgLayout& L, char* s
     k_camera_reduce<T, false, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
     k_camera_finish<T><<<fgrid, 32 * kFinishWarps, 0, st>>>(ba, acc, inv_radius, mn, mx, jacobi_scaling,
                                                            CERES_B200_PRECOND_SCHUR_JACOBI, partials,
-                                                           reinterpret_cast<T*>(scratch + L.spse_base));
+                                                           reinterpret_cast<double*>(scratch + L.spse_base));
   }
 }
 
@@ -2240,7 +2239,8 @@ int pcg_impl(const ceres_b200_ba_t& ba, int precond, int min_it, int max_it, dou
   so.terms = series_terms;
   so.tol = series_tol;
   so.init = series_init ? 1 : 0;
-  so.init_blocks = so.precond ? ba.precond : static_cast<const void*>(scratch + L.spse_base);
+  so.init_blocks = so.precond ? reinterpret_cast<const double*>(ba.precond)
+                              : reinterpret_cast<const double*>(scratch + L.spse_base);
   rc = launch_pcg<T>(ba, min_it, max_it, tol, max_ref, st, L, scratch, so, cl);
   if (rc) return rc;
   count_launch();

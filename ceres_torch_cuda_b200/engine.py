@@ -231,7 +231,9 @@ class BAEngine:
         self.winv_ga = torch.zeros((npq, 3), **f64)
         self.step_points = torch.zeros((npq, 3), **f64)
         self.cam_diag = torch.zeros((ncq, 9), **f64)
-        self.precond = torch.zeros((ncq, 81), dtype=T, device=dev)
+        # float64 in both precisions: an inverted 9x9 block of an ill-conditioned camera
+        # rounded to float32 preconditions worse (more PCG iterations per solve)
+        self.precond = torch.zeros((ncq, 81), **f64)
         self.rhs = torch.zeros((ncq, 9), **f64)
         self.step_cameras = torch.zeros((ncq, 9), **f64)
         self.pcg_vec = {k: torch.zeros(9 * ncq, **f64) for k in ("x", "r", "z", "ap")}

@@ -39,7 +39,7 @@ def footprint_bytes(problem: BundleAdjustmentProblem, precision: str) -> int:
     per_slot = 24 * jb + 16 + 16 + 4
     per_obs = 8 + 64  # camera-major entry and layout-building temporaries
     per_point = 9 * 8 + 6 * jb + 4 * 3 * 8 + 3 * 8 + 8 + 1
-    per_camera = 4 * 9 * 8 + 81 * jb + 72 * 8 + 24 * 8 + 7 * 9 * 8
+    per_camera = 4 * 9 * 8 + 81 * 8 + 72 * 8 + 24 * 8 + 7 * 9 * 8  # preconditioner blocks float64
     return slots * per_slot + no * per_obs + nq * per_point + nc * per_camera
 
 

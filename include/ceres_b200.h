@@ -157,7 +157,7 @@ typedef struct ceres_b200_ba_t {
 
   /* camera-side Schur pieces */
   double* cam_diag;            /* [num_cameras][9] damping D_c added to the diagonal */
-  void* precond;               /* [num_cameras][81] preconditioner inverse blocks, float or double */
+  void* precond;               /* [num_cameras][81] preconditioner inverse blocks, double in both precisions */
   double* rhs;                 /* [num_cameras][9] reduced right-hand side */
   double* step_cameras;        /* [num_cameras][9] */
 
@@ -491,7 +491,7 @@ typedef struct ceres_b200_batch_t {
   double* winv_ga;              /* [points][3] */
   double* step_points;          /* [points][3] */
   double* cam_diag;             /* [cameras][9] */
-  void* precond;                /* [cameras][81] float or double */
+  void* precond;                /* [cameras][81] double in both precisions */
   double* rhs;                  /* [cameras][9] */
   double* step_cameras;         /* [cameras][9] */
   double* cam_acc;              /* [cameras][72] */
