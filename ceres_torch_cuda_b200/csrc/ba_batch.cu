@@ -451,62 +451,89 @@ __device__ void cl_assemble(const ceres_b200_batch_t& B, const Prob& P, const Ct
 }
 
 // ------------------------------------------------------------------------------------
-// Implicit Schur product over this CTA's slices (the point-major walk of
-// matvec_slices): ys += (J_c^T J_c - H_cp W^-1 H_pc) p into shared memory.
-// kCrossP: p is a global float64 vector written by other CTAs.
+// Implicit Schur product y = (J_c^T J_c - H_cp W^-1 H_pc) p of one problem in two passes
+// with no atomics, so every sum has a fixed order whatever the cluster shape:
+//   point pass  (the problem's slices over the cluster's warps, lane = point):
+//                 s_q = W_q^-1 sum_k Jp_k^T (Jc_k p_c(k)), into B.step_points (scratch
+//                 during the linear solve; the step overwrites it afterwards);
+//   cluster barrier;
+//   camera pass (the problem's cameras over the cluster's warps, lane = observation):
+//                 y_c = sum_e Jc_e^T (Jc_e p_c - Jp_e s_q(e)), the lane sums added by a
+//                 butterfly, written to ys of the CTA that owns camera c (distributed
+//                 shared memory, one writer per element).
+// The caller's cluster barrier publishes ys. kCrossP: p is a global float64 vector
+// written by other CTAs (otherwise this CTA's shared-memory copy).
 // ------------------------------------------------------------------------------------
-template <typename T, typename TP, typename A, bool kCrossP>
-__device__ void cl_schur_product(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, const TP* ps, A* ys) {
+template <typename T, typename TP, bool kCrossP>
+__device__ void cl_schur_product(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, const TP* ps, double* ys) {
   const int lane = threadIdx.x & 31;
   const T* jac = reinterpret_cast<const T*>(B.jac);
   const T* winv = reinterpret_cast<const T*>(B.winv);
+  double* sv = B.step_points;
   for (int s = P.s0 + X.cw; s < P.s0 + P.ns; s += X.CW) {
     const int q = s * 32 + lane;
     const int len = B.slice_len[s];
     const size_t base = (size_t)B.slice_base[s] + lane;
-    A t0 = 0, t1 = 0, t2 = 0;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
     for (int k = 0; k < len; ++k) {
       const size_t slot = base + 32 * (size_t)k;
       const int c = max(B.slot_cam[slot], 0);  // padding slots: zero Jacobians, camera 0 as the address
       T rv[kRec];
       rec_load<false>(jac, slot, rv);
       const TP* pc = ps + 9 * (size_t)c;
-      A u0 = 0, u1 = 0;
+      double u0 = 0.0, u1 = 0.0;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
-        const A pj = kCrossP ? (A)ldx(pc + j) : (A)pc[j];
-        u0 += (A)rv[j] * pj;
-        u1 += (A)rv[9 + j] * pj;
+        const double pj = kCrossP ? (double)ldx(pc + j) : (double)pc[j];
+        u0 += (double)rv[j] * pj;
+        u1 += (double)rv[9 + j] * pj;
       }
-      t0 += (A)rv[18] * u0 + (A)rv[21] * u1;
-      t1 += (A)rv[19] * u0 + (A)rv[22] * u1;
-      t2 += (A)rv[20] * u0 + (A)rv[23] * u1;
+      t0 += (double)rv[18] * u0 + (double)rv[21] * u1;
+      t1 += (double)rv[19] * u0 + (double)rv[22] * u1;
+      t2 += (double)rv[20] * u0 + (double)rv[23] * u1;
     }
     const T* wi = winv + 6 * (size_t)q;
-    const A w0 = (A)wi[0], w1 = (A)wi[1], w2 = (A)wi[2], w3 = (A)wi[3], w4 = (A)wi[4], w5 = (A)wi[5];
-    const A s0 = w0 * t0 + w1 * t1 + w2 * t2;
-    const A s1 = w1 * t0 + w3 * t1 + w4 * t2;
-    const A s2 = w2 * t0 + w4 * t1 + w5 * t2;
-    for (int k = 0; k < len; ++k) {
-      const size_t slot = base + 32 * (size_t)k;
-      const int c = B.slot_cam[slot];
-      if (c < 0) continue;
+    const double w0 = wi[0], w1 = wi[1], w2 = wi[2], w3 = wi[3], w4 = wi[4], w5 = wi[5];
+    sv[3 * (size_t)q] = w0 * t0 + w1 * t1 + w2 * t2;
+    sv[3 * (size_t)q + 1] = w1 * t0 + w3 * t1 + w4 * t2;
+    sv[3 * (size_t)q + 2] = w2 * t0 + w4 * t1 + w5 * t2;
+  }
+  csync();  // every point's s_q
+  const int per = (P.nc + X.G - 1) / X.G;  // cameras per CTA (Prob::c0 = rank * per)
+  for (int cl = X.cw; cl < P.nc; cl += X.CW) {
+    const int cg = P.cam0 + cl;
+    const TP* pcp = ps + 9 * (size_t)cl;
+    double pc[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) pc[j] = kCrossP ? (double)ldx(pcp + j) : (double)pcp[j];
+    double y[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) y[j] = 0.0;
+    const int e1 = B.cam_offsets[cg + 1];
+    for (int e = B.cam_offsets[cg] + lane; e < e1; e += 32) {
+      const int2 ent = reinterpret_cast<const int2*>(B.cam_entries)[e];
       T rv[kRec];
-      rec_load<false>(jac, slot, rv);
-      const TP* pc = ps + 9 * (size_t)c;
-      A u0 = 0, u1 = 0;
+      rec_load<true>(jac, (size_t)ent.x, rv);
+      const double* sq = sv + 3 * (size_t)ent.y;
+      const double s0 = ldx(sq), s1 = ldx(sq + 1), s2 = ldx(sq + 2);
+      double u0 = 0.0, u1 = 0.0;
 #pragma unroll
       for (int j = 0; j < 9; ++j) {
-        const A pj = kCrossP ? (A)ldx(pc + j) : (A)pc[j];
-        u0 += (A)rv[j] * pj;
-        u1 += (A)rv[9 + j] * pj;
+        u0 += (double)rv[j] * pc[j];
+        u1 += (double)rv[9 + j] * pc[j];
       }
-      const A v0 = u0 - ((A)rv[18] * s0 + (A)rv[19] * s1 + (A)rv[20] * s2);
-      const A v1 = u1 - ((A)rv[21] * s0 + (A)rv[22] * s1 + (A)rv[23] * s2);
-      A* yc = ys + 9 * (size_t)c;
+      const double v0 = u0 - ((double)rv[18] * s0 + (double)rv[19] * s1 + (double)rv[20] * s2);
+      const double v1 = u1 - ((double)rv[21] * s0 + (double)rv[22] * s1 + (double)rv[23] * s2);
 #pragma unroll
-      for (int j = 0; j < 9; ++j) atomicAdd(yc + j, (A)rv[j] * v0 + (A)rv[9 + j] * v1);
+      for (int j = 0; j < 9; ++j) y[j] += (double)rv[j] * v0 + (double)rv[9 + j] * v1;
     }
+    double mine = 0.0;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const double w = warp_sum(y[j]);
+      mine = (lane == j) ? w : mine;
+    }
+    if (lane < 9) remote(ys, cl / per)[9 * (size_t)cl + lane] = mine;
   }
 }
 
@@ -585,18 +612,15 @@ __device__ PcgOut cl_pcg(const ceres_b200_batch_t& B, const Prob& P, const Ctx& 
       for (int j = threadIdx.x; j < n; j += blockDim.x) {
         const double pv = (k == 0) ? ldx(Z + j) : ldx(Z + j) + beta * ldx(Pold + j);
         ps[j] = pv;
-        ys[j] = 0.0;
         if (j >= j0 && j < j1) Pnew[j] = pv;
       }
       cur = nxt;
       __syncthreads();
-      cl_schur_product<T, double, double, false>(B, P, X, ps, ys);
-      csync();  // every CTA's product accumulator is complete
+      cl_schur_product<T, double, false>(B, P, X, ps, ys);
+      csync();  // this CTA's cameras' products are complete
       double v1[1] = {0.0};
       for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-        double y = 0.0;
-        for (int r = 0; r < X.G; ++r) y += remote(ys, r)[j];
-        y += ldx(D + j) * Pnew[j];
+        const double y = ys[j] + ldx(D + j) * Pnew[j];
         AP[j] = y;
         v1[0] += Pnew[j] * y;
       }
@@ -649,7 +673,6 @@ template <typename T>
 __device__ int cl_linear_solve(const ceres_b200_batch_t& B, const Prob& P, const Ctx& X, const Smem& S) {
   const size_t N = 9 * (size_t)B.cam_off[B.num_problems];
   const size_t o = 9 * (size_t)P.cam0;
-  const int n = 9 * P.nc;
   const int j0 = 9 * P.c0, j1 = 9 * P.c1;
   double* step = B.step_cameras + o;
   const double* rhs = B.rhs + o;
@@ -662,14 +685,10 @@ __device__ int cl_linear_solve(const ceres_b200_batch_t& B, const Prob& P, const
     // solve of S dx = r64 (tolerance relative to the original |rhs|) added to the step
     double* r64 = B.pcg + 6 * N + o;
     for (int it = 0; it < B.max_refinements; ++it) {
-      for (int j = threadIdx.x; j < n; j += blockDim.x) S.y64[j] = 0.0;
-      __syncthreads();
-      cl_schur_product<T, double, double, true>(B, P, X, step, S.y64);
+      cl_schur_product<T, double, true>(B, P, X, step, S.y64);
       csync();
       for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
-        double y = 0.0;
-        for (int r = 0; r < X.G; ++r) y += remote(S.y64, r)[j];
-        r64[j] = ldx(rhs + j) - (y + ldx(B.cam_diag + o + j) * step[j]);
+        r64[j] = ldx(rhs + j) - (S.y64[j] + ldx(B.cam_diag + o + j) * step[j]);
       }
       csync();
       const PcgOut corr = cl_pcg<T>(B, P, X, S, r64, step, true, 0, B.max_linear_solver_iterations, B.eta,
