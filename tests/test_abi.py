@@ -43,7 +43,8 @@ def test_abi_version_and_struct_size(lib):
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
-@pytest.mark.parametrize("ctype,mirror", [("ceres_b200_ba_t", _lib.BAStruct), ("ceres_b200_batch_t", _lib.BatchStruct)])
+@pytest.mark.parametrize("ctype,mirror", [("ceres_b200_ba_t", _lib.BAStruct), ("ceres_b200_batch_t", _lib.BatchStruct),
+                                         ("ceres_b200_clusters_t", _lib.ClusterStruct)])
 def test_struct_field_offsets_match_c(tmp_path, ctype, mirror):
     fields = [f for f, _ in mirror._fields_]
     src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {",
@@ -88,3 +89,11 @@ def test_invalid_arguments_are_rejected_without_a_gpu(lib):
     assert lib.ceres_b200_batch_solve(ctypes.byref(b), 256, 1, 1, None) == _lib.EINVAL
     assert lib.ceres_b200_batch_solve(None, 256, 1, 1, None) == _lib.EINVAL
     assert lib.ceres_b200_batch_struct_bytes() == ctypes.sizeof(_lib.BatchStruct)
+    # the cluster preconditioner's entry points check their struct before any CUDA call
+    assert lib.ceres_b200_clusters_struct_bytes() == ctypes.sizeof(_lib.ClusterStruct)
+    s = _lib.BAStruct()
+    s.precision = _lib.FP64
+    cl = _lib.ClusterStruct()  # no arrays, no components
+    assert lib.ceres_b200_ba_cluster_factor(ctypes.byref(s), ctypes.byref(cl), None) == _lib.EINVAL
+    assert lib.ceres_b200_ba_cluster_factor(ctypes.byref(s), None, None) == _lib.EINVAL
+    assert lib.ceres_b200_ba_pcg_cluster(ctypes.byref(s), ctypes.byref(cl), 0, 10, 0.1, 0, None) == _lib.EINVAL
