@@ -71,15 +71,17 @@ def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_ind
     slice_off[1:] = np.cumsum(slices_per)
     S = int(slice_off[-1])
     i64 = dict(dtype=torch.int64, device=dev)
-    point_problem = torch.repeat_interleave(torch.arange(B, device=dev), torch.as_tensor(pt_counts, device=dev),
-                                            output_size=NP)
+    # the per-problem integers go to the device in one copy
+    host = np.concatenate([pt_counts, pt_off_in[:-1], 32 * slice_off[:-1], cam_counts, cam_off, slice_off])
+    dv = torch.from_numpy(host.astype(np.int64)).to(dev, non_blocking=False)
+    pt_counts_d, start_in, q_base, cam_counts_d, cam_off_d, slice_off_d = torch.split(
+        dv, [B, B, B, B, B + 1, B + 1])
+    point_problem = torch.repeat_interleave(torch.arange(B, device=dev), pt_counts_d, output_size=NP)
     counts = torch.zeros(NP, **i64)
     if no:
         counts.index_add_(0, pi, torch.ones(no, **i64))
     # grouped by problem, then by track length descending, stable in point id
     order = torch.argsort(point_problem * (1 << 32) + ((1 << 31) - 1 - counts), stable=True)
-    start_in = torch.as_tensor(pt_off_in[:-1], device=dev)
-    q_base = torch.as_tensor(32 * slice_off[:-1], device=dev)
     pos = torch.arange(NP, device=dev) - start_in[point_problem[order]]
     q_of_sorted = q_base[point_problem[order]] + pos
     q_of_point = torch.empty(NP, **i64)
@@ -108,9 +110,8 @@ def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_ind
     else:
         q = torch.zeros(0, **i64)
         slot = q
-    cam_problem = torch.repeat_interleave(torch.arange(B, device=dev), torch.as_tensor(cam_counts, device=dev),
-                                          output_size=NC)
-    local_cam = ci - torch.as_tensor(cam_off[:-1], device=dev)[cam_problem[ci]] if no else ci
+    cam_problem = torch.repeat_interleave(torch.arange(B, device=dev), cam_counts_d, output_size=NC)
+    local_cam = ci - cam_off_d[:-1][cam_problem[ci]] if no else ci
     slot_cam = torch.full((max(num_slots, 1),), -1, dtype=torch.int32, device=dev)
     slot_obs = torch.zeros((max(num_slots, 1), 2), dtype=torch.float64, device=dev)
     if no:
@@ -125,8 +126,7 @@ def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_ind
     cam_offsets = torch.zeros(NC + 1, **i64)
     cam_offsets[1:] = torch.cumsum(cam_counts_t, 0)
     return BatchLayout(
-        num_problems=B, cam_off=torch.as_tensor(cam_off, dtype=torch.int32, device=dev),
-        slice_off=torch.as_tensor(slice_off, dtype=torch.int32, device=dev),
+        num_problems=B, cam_off=cam_off_d.to(torch.int32), slice_off=slice_off_d.to(torch.int32),
         slice_base=slice_base.to(torch.int32).contiguous(), slice_len=slice_len.to(torch.int32).contiguous(),
         slot_cam=slot_cam, slot_obs=slot_obs, cam_offsets=cam_offsets.to(torch.int32).contiguous(),
         cam_entries=cam_entries, lane_point=lane_point, num_slots=num_slots, has_duplicate_cameras=has_dup,
@@ -183,9 +183,15 @@ class BatchSolver:
         cam_off = np.concatenate([[0], np.cumsum(cam_counts)])
         pt_off = np.concatenate([[0], np.cumsum(pt_counts)])
         self.cam_off_np, self.pt_off_np = cam_off, pt_off
-        ci = torch.cat([p.camera_index.to(dev, torch.int64) + int(cam_off[i]) for i, p in enumerate(problems)])
-        pi = torch.cat([p.point_index.to(dev, torch.int64) + int(pt_off[i]) for i, p in enumerate(problems)])
-        obs = torch.cat([p.observations.to(dev, torch.float64) for p in problems])
+        # global indices: each problem's indices plus its offsets, in a few batch-wide operations
+        obs_counts = np.array([p.num_observations for p in problems], dtype=np.int64)
+        offs = torch.from_numpy(np.concatenate([cam_off[:-1], pt_off[:-1], obs_counts])).to(dev)
+        per_obs = torch.repeat_interleave(torch.arange(len(problems), device=dev), offs[2 * len(problems):],
+                                          output_size=int(obs_counts.sum()))
+        ci = torch.cat([p.camera_index for p in problems]).to(dev, torch.int64) + offs[:len(problems)][per_obs]
+        pi = torch.cat([p.point_index for p in problems]).to(dev, torch.int64) + \
+            offs[len(problems):2 * len(problems)][per_obs]
+        obs = torch.cat([p.observations for p in problems]).to(dev, torch.float64)
         L = build_batch_layout(cam_counts, pt_counts, ci, pi, obs)
         self.layout = L
         S = L.num_slices
@@ -199,11 +205,19 @@ class BatchSolver:
         self.lane_src = torch.where(L.lane_point >= 0, L.lane_point, torch.full_like(L.lane_point, NPin))
         pts_in = torch.cat([p.points.to(**f64) for p in problems] + [torch.zeros((1, 3), **f64)])
         self.points = pts_in.index_select(0, self.lane_src).contiguous()
-        cam_const = torch.cat([(p.camera_constant if p.camera_constant is not None else
-                                torch.zeros(p.num_cameras, dtype=torch.bool, device=dev)).to(dev) for p in problems])
-        pc_in = torch.cat([(p.point_constant if p.point_constant is not None else
-                            torch.zeros(p.num_points, dtype=torch.bool, device=dev)).to(dev) for p in problems]
-                          + [torch.ones(1, dtype=torch.bool, device=dev)])  # padding lanes are constant
+        if all(p.camera_constant is None for p in problems):
+            cam_const = torch.zeros(NC, dtype=torch.bool, device=dev)
+        else:
+            cam_const = torch.cat([(p.camera_constant if p.camera_constant is not None else
+                                    torch.zeros(p.num_cameras, dtype=torch.bool, device=dev)).to(dev)
+                                   for p in problems])
+        if all(p.point_constant is None for p in problems):
+            pc_in = torch.zeros(NPin + 1, dtype=torch.bool, device=dev)
+            pc_in[NPin] = True  # padding lanes are constant
+        else:
+            pc_in = torch.cat([(p.point_constant if p.point_constant is not None else
+                                torch.zeros(p.num_points, dtype=torch.bool, device=dev)).to(dev) for p in problems]
+                              + [torch.ones(1, dtype=torch.bool, device=dev)])  # padding lanes are constant
         self.cam_const = cam_const.to(torch.uint8).contiguous()
         self.pt_const = pc_in.index_select(0, self.lane_src).to(torch.uint8).contiguous()
         self.cand_cameras = torch.empty_like(self.cameras)
@@ -288,48 +302,57 @@ class BatchSolver:
                 p.cameras.copy_(self.cameras[self.cam_off_np[i]:self.cam_off_np[i + 1]].to(p.cameras.dtype))
                 p.points.copy_(pts[self.pt_off_np[i]:self.pt_off_np[i + 1]].to(p.points.dtype))
 
+    def fetch(self) -> tuple[np.ndarray, np.ndarray]:
+        """The per-problem results and iteration records, copied to the host."""
+        return self.result.cpu().numpy(), self.trace.cpu().numpy()
+
     def summaries(self) -> list[SolverSummary]:
-        res = self.result.cpu().numpy()
-        tr = self.trace.cpu().numpy()
-        out = []
-        for i, p in enumerate(self.problems):
-            r = res[i]
-            s = _new_summary(self.options)
-            s.num_parameter_blocks = p.num_cameras + p.num_points
-            s.num_parameters = 9 * p.num_cameras + 3 * p.num_points
-            ncc = int(p.camera_constant.sum()) if p.camera_constant is not None else 0
-            npc = int(p.point_constant.sum()) if p.point_constant is not None else 0
-            s.num_effective_parameters = 9 * (p.num_cameras - ncc) + 3 * (p.num_points - npc)
-            s.num_residual_blocks = p.num_observations
-            s.num_residuals = 2 * p.num_observations
-            s.initial_cost = float(r[_lib.BR_INITIAL_COST])
-            s.final_cost = float(r[_lib.BR_FINAL_COST])
-            s.termination_type = _TERMS[int(r[_lib.BR_TERMINATION])]
-            s.message = _lib.MESSAGES[int(r[_lib.BR_MESSAGE])]
-            if s.num_effective_parameters == 0:
-                s.termination_type = TerminationType.CONVERGENCE
-                s.message = "No active parameters."
-            s.num_successful_steps = int(r[_lib.BR_SUCCESSFUL])
-            s.num_unsuccessful_steps = int(r[_lib.BR_UNSUCCESSFUL])
-            s.num_jacobian_evaluations = int(r[_lib.BR_JACOBIAN_EVALS])
-            s.num_residual_evaluations = int(r[_lib.BR_RESIDUAL_EVALS])
-            s.num_linear_solves = int(r[_lib.BR_LINEAR_SOLVES])
-            s.precision = self.precision
-            n = min(int(r[_lib.BR_RECORDS]), self.max_trace)
-            for k in range(n):
-                t = tr[i, k]
-                flags = int(t[_lib.BT_FLAGS])
-                s.iterations.append(IterationSummary(
-                    iteration=k, step_is_valid=bool(flags & 1), step_is_successful=bool(flags & 2),
-                    step_is_nonmonotonic=bool(flags & 4), cost=float(t[_lib.BT_COST]),
-                    cost_change=float(t[_lib.BT_COST_CHANGE]), gradient_max_norm=float(t[_lib.BT_GMAX]),
-                    gradient_norm=float(t[_lib.BT_GNORM]), step_norm=float(t[_lib.BT_STEP_NORM]),
-                    relative_decrease=float(t[_lib.BT_RHO]), trust_region_radius=float(t[_lib.BT_RADIUS]),
-                    eta=self.options.eta, linear_solver_iterations=int(t[_lib.BT_LINEAR_ITERATIONS])))
-            if int(r[_lib.BR_ERROR]):
-                raise _lib.NativeLibraryError(f"batched solve of problem {i}: device error bits {int(r[_lib.BR_ERROR])}")
-            out.append(s)
-        return out
+        res, tr = self.fetch()
+        return [self.summary_of(i, res, tr) for i in range(len(self.problems))]
+
+    def summary_of(self, i: int, res: np.ndarray, tr: np.ndarray) -> SolverSummary:
+        """Problem i's SolverSummary from the fetched arrays."""
+        return summary_from_arrays(self.problems[i], self.options, self.precision, self.max_trace, res[i], tr[i], i)
+
+
+def summary_from_arrays(p: BundleAdjustmentProblem, options: SolverOptions, precision: str, max_trace: int,
+                        r: np.ndarray, trace: np.ndarray, i: int = 0) -> SolverSummary:
+    """A batched problem's SolverSummary from its result row and iteration records."""
+    s = _new_summary(options)
+    s.num_parameter_blocks = p.num_cameras + p.num_points
+    s.num_parameters = 9 * p.num_cameras + 3 * p.num_points
+    ncc = int(p.camera_constant.sum()) if p.camera_constant is not None else 0
+    npc = int(p.point_constant.sum()) if p.point_constant is not None else 0
+    s.num_effective_parameters = 9 * (p.num_cameras - ncc) + 3 * (p.num_points - npc)
+    s.num_residual_blocks = p.num_observations
+    s.num_residuals = 2 * p.num_observations
+    s.initial_cost = float(r[_lib.BR_INITIAL_COST])
+    s.final_cost = float(r[_lib.BR_FINAL_COST])
+    s.termination_type = _TERMS[int(r[_lib.BR_TERMINATION])]
+    s.message = _lib.MESSAGES[int(r[_lib.BR_MESSAGE])]
+    if s.num_effective_parameters == 0:
+        s.termination_type = TerminationType.CONVERGENCE
+        s.message = "No active parameters."
+    s.num_successful_steps = int(r[_lib.BR_SUCCESSFUL])
+    s.num_unsuccessful_steps = int(r[_lib.BR_UNSUCCESSFUL])
+    s.num_jacobian_evaluations = int(r[_lib.BR_JACOBIAN_EVALS])
+    s.num_residual_evaluations = int(r[_lib.BR_RESIDUAL_EVALS])
+    s.num_linear_solves = int(r[_lib.BR_LINEAR_SOLVES])
+    s.precision = precision
+    n = min(int(r[_lib.BR_RECORDS]), max_trace)
+    for k in range(n):
+        t = trace[k]
+        flags = int(t[_lib.BT_FLAGS])
+        s.iterations.append(IterationSummary(
+            iteration=k, step_is_valid=bool(flags & 1), step_is_successful=bool(flags & 2),
+            step_is_nonmonotonic=bool(flags & 4), cost=float(t[_lib.BT_COST]),
+            cost_change=float(t[_lib.BT_COST_CHANGE]), gradient_max_norm=float(t[_lib.BT_GMAX]),
+            gradient_norm=float(t[_lib.BT_GNORM]), step_norm=float(t[_lib.BT_STEP_NORM]),
+            relative_decrease=float(t[_lib.BT_RHO]), trust_region_radius=float(t[_lib.BT_RADIUS]),
+            eta=options.eta, linear_solver_iterations=int(t[_lib.BT_LINEAR_ITERATIONS])))
+    if int(r[_lib.BR_ERROR]):
+        raise _lib.NativeLibraryError(f"batched solve of problem {i}: device error bits {int(r[_lib.BR_ERROR])}")
+    return s
 
 
 # CTA shapes (threads per CTA, resident CTAs per SM) the library is compiled for; the

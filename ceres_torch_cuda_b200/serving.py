@@ -25,7 +25,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from .batch import BatchSolver
+from .batch import BatchSolver, summary_from_arrays
 from .problem import BundleAdjustmentProblem
 from .types import SolverOptions, SolverSummary
 
@@ -44,6 +44,7 @@ def footprint_bytes(problem: BundleAdjustmentProblem, precision: str) -> int:
 
 
 _STREAMS: dict = {}
+SCAN_FACTOR = 4  # waiting requests looked at per admission, in units of max_batch
 
 
 def _stream_pool(device: torch.device, count: int) -> list:
@@ -62,12 +63,28 @@ class Request:
     arrival: float                       # time.perf_counter() at submission
     footprint: int = 0
     admitted: float | None = None
-    done: float | None = None
-    summary: SolverSummary | None = None
+    done: float | None = None            # when the solution was in the problem's tensors
+    _summary: SolverSummary | None = field(default=None, repr=False)
+    _result: tuple | None = field(default=None, repr=False)   # (options, precision, max records, results, records)
 
     @property
     def latency(self) -> float | None:
         return None if self.done is None else self.done - self.arrival
+
+    @property
+    def summary(self) -> SolverSummary | None:
+        """The SolverSummary, built from the batch's fetched results when first asked for
+        (the server's loop only copies the results to the host)."""
+        if self._summary is None and self._result is not None:
+            options, precision, max_trace, r, tr = self._result
+            self._summary = summary_from_arrays(self.problem, options, precision, max_trace, r, tr)
+            self._result = None
+        return self._summary
+
+    @summary.setter
+    def summary(self, value: SolverSummary | None) -> None:
+        self._summary = value
+        self._result = None
 
 
 @dataclass
@@ -140,10 +157,11 @@ class BAServer:
         for f in self._flights:
             if f.event.query():
                 f.solver.write_back()
-                sums = f.solver.summaries()
+                res, tr = f.solver.fetch()  # also waits for the write-back copies
                 now = time.perf_counter()
-                for r, s in zip(f.requests, sums):
-                    r.summary = s
+                sv = f.solver
+                for k, r in enumerate(f.requests):
+                    r._result = (sv.options, sv.precision, sv.max_trace, res[k], tr[k])  # no device buffers kept
                     r.done = now
                     self.completed.append(r)
                 self._in_use -= f.footprint
@@ -162,23 +180,22 @@ class BAServer:
                 time.perf_counter() - self._waiting[0].arrival < self.batch_window_s:
             return False
         # the oldest request sets the cluster size; waiting requests of the same size class
-        # join it in arrival order
+        # join it in arrival order. Only the first SCAN_FACTOR * max_batch waiting requests
+        # are looked at, so an admission costs the same however long the queue is.
         G = self._cluster_for(self._waiting[0])
-        batch, size, rest = [], 0, deque()
-        while self._waiting:
+        if self._in_use + self._waiting[0].footprint > self.memory_budget:
+            return False  # the oldest does not fit yet: keep the order and wait
+        batch, size, skipped = [], 0, []
+        scan = SCAN_FACTOR * self.max_batch
+        while self._waiting and len(batch) < self.max_batch and scan > 0:
             r = self._waiting.popleft()
-            if (len(batch) < self.max_batch and self._cluster_for(r) == G
-                    and self._in_use + size + r.footprint <= self.memory_budget):
+            scan -= 1
+            if self._cluster_for(r) == G and self._in_use + size + r.footprint <= self.memory_budget:
                 batch.append(r)
                 size += r.footprint
             else:
-                rest.append(r)
-                if not batch:  # the oldest does not fit yet: keep the order and wait
-                    rest.extend(self._waiting)
-                    self._waiting.clear()
-        self._waiting = rest
-        if not batch:
-            return False
+                skipped.append(r)
+        self._waiting.extendleft(reversed(skipped))
         busy = {id(f.stream) for f in self._flights}
         stream = next(s for s in self._streams if id(s) not in busy)
         now = time.perf_counter()
