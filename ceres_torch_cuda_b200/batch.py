@@ -199,11 +199,11 @@ class BatchSolver:
         NC = int(cam_off[-1])
         f64 = dict(dtype=torch.float64, device=dev)
         jt = torch.float32 if precision == "mixed" else torch.float64
-        self.cameras = torch.cat([p.cameras.to(**f64) for p in problems]).contiguous()
+        self.cameras = torch.cat([p.cameras for p in problems]).to(**f64).contiguous()
         # lanes -> input points; padding lanes (-1) read a zero row appended at the end
         NPin = int(pt_off[-1])
         self.lane_src = torch.where(L.lane_point >= 0, L.lane_point, torch.full_like(L.lane_point, NPin))
-        pts_in = torch.cat([p.points.to(**f64) for p in problems] + [torch.zeros((1, 3), **f64)])
+        pts_in = torch.cat([p.points for p in problems] + [problems[0].points.new_zeros((1, 3))]).to(**f64)
         self.points = pts_in.index_select(0, self.lane_src).contiguous()
         if all(p.camera_constant is None for p in problems):
             cam_const = torch.zeros(NC, dtype=torch.bool, device=dev)
@@ -297,10 +297,10 @@ class BatchSolver:
         """Solved parameters into each problem's tensors."""
         pts = torch.empty((int(self.pt_off_np[-1]) + 1, 3), dtype=torch.float64, device=self.device)
         pts.index_copy_(0, self.lane_src, self.points)  # padding lanes land in the extra last row
-        for i, p in enumerate(self.problems):
-            with torch.no_grad():
-                p.cameras.copy_(self.cameras[self.cam_off_np[i]:self.cam_off_np[i + 1]].to(p.cameras.dtype))
-                p.points.copy_(pts[self.pt_off_np[i]:self.pt_off_np[i + 1]].to(p.points.dtype))
+        with torch.no_grad():
+            for i, p in enumerate(self.problems):
+                p.cameras.copy_(self.cameras[self.cam_off_np[i]:self.cam_off_np[i + 1]])
+                p.points.copy_(pts[self.pt_off_np[i]:self.pt_off_np[i + 1]])
 
     def fetch(self) -> tuple[np.ndarray, np.ndarray]:
         """The per-problem results and iteration records, copied to the host."""
