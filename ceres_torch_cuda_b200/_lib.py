@@ -16,7 +16,7 @@ c_int64 = ctypes.c_int64
 c_double = ctypes.c_double
 c_void_p = ctypes.c_void_p
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 OK = 0
 EINVAL = -1
@@ -70,6 +70,8 @@ class BAStruct(ctypes.Structure):
         ("num_items", c_int32), ("max_camera_obs", c_int32),
         ("scratch", c_void_p), ("scratch_bytes", c_int64),
         ("counters", c_void_p), ("stats", c_void_p),
+        ("schur_blocks", c_void_p), ("schur_block_start", c_void_p), ("schur_contrib", c_void_p),
+        ("num_schur_blocks", c_int64),
     ]
 
 

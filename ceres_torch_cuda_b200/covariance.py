@@ -136,8 +136,7 @@ class Covariance:
         eng._call("ceres_b200_ba_point_assemble", math.inf, 0.0, 0.0, 0)
         eng._call("ceres_b200_ba_camera_assemble", math.inf, 0.0, 0.0, 0, _lib.PRECOND_IDENTITY)
         n = 9 * nc
-        S = torch.empty((max(n, 1), max(n, 1)), dtype=torch.float64, device=eng.device)
-        eng._call("ceres_b200_ba_schur_matrix", S.data_ptr())
+        S = eng.schur_matrix()
         S0 = S.clone()
         inv = torch.empty_like(S)
         flags = torch.zeros(4, dtype=torch.int32, device=eng.device)

@@ -1525,6 +1525,74 @@ __global__ void __launch_bounds__(kWarpBlock) k_schur_explicit(ceres_b200_ba_t b
   }
 }
 
+// The explicit S in a fixed order: one warp per listed block (a, b), a <= b, summing the
+// block's contributions (slot i, slot j, point q) in list order (points ascending):
+// -G_i W_q^-1 G_j^T, G = Jc^T Jp of one observation, plus Jc_i^T Jc_i when i == j (the
+// diagonal blocks list every observation of the camera with itself and every ordered
+// pair of its observations of one point). Float64 arithmetic on the store; lane l
+// holds entries l, l + 32, l + 64 of the block; G, W^-1 G and Jc go through the warp's
+// shared memory. A diagonal block is written from its upper triangle. k_dense_diag
+// then adds the damping.
+template <typename T>
+__global__ void __launch_bounds__(kWarpBlock) k_schur_ordered(ceres_b200_ba_t ba, double* S, int n) {
+  __shared__ double sg[kWarpBlock / 32][4][27];
+  const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
+  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
+  const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
+  double* Ga = sg[wid][0];
+  double* Gb = sg[wid][1];
+  double* Ha = sg[wid][2];
+  double* Ja = sg[wid][3];
+  const int gi = lane / 3, gk = lane - 3 * (lane / 3);
+  const int c0 = gk == 0 ? 0 : (gk == 1 ? 1 : 2);  // column gk of the packed symmetric 3 x 3
+  const int c1 = gk == 0 ? 1 : (gk == 1 ? 3 : 4);
+  const int c2 = gk == 0 ? 2 : (gk == 1 ? 4 : 5);
+  for (long long bi = gw; bi < ba.num_schur_blocks; bi += nw) {
+    const int a = ba.schur_blocks[2 * bi], b = ba.schur_blocks[2 * bi + 1];
+    double acc[3] = {0.0, 0.0, 0.0};
+    const long long e1 = ba.schur_block_start[bi + 1];
+    for (long long ci = ba.schur_block_start[bi]; ci < e1; ++ci) {
+      const int sa = ba.schur_contrib[3 * ci], sb = ba.schur_contrib[3 * ci + 1], q = ba.schur_contrib[3 * ci + 2];
+      const bool self = sa == sb;
+      const T* ra = jac + (size_t)kRec * (size_t)sa;
+      if (lane < 27) {
+        const T* rb = jac + (size_t)kRec * (size_t)sb;
+        Ga[lane] = (double)ra[gi] * (double)ra[18 + gk] + (double)ra[9 + gi] * (double)ra[21 + gk];
+        Gb[lane] = (double)rb[gi] * (double)rb[18 + gk] + (double)rb[9 + gi] * (double)rb[21 + gk];
+      }
+      if (self && lane < 18) Ja[lane] = (double)ra[lane];
+      __syncwarp();
+      if (lane < 27) {
+        const T* w = winv + 6 * (size_t)q;
+        Ha[lane] = Ga[3 * gi] * (double)w[c0] + Ga[3 * gi + 1] * (double)w[c1] + Ga[3 * gi + 2] * (double)w[c2];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const int idx = lane + 32 * m;
+        if (idx < 81) {
+          const int i = idx / 9, j = idx - 9 * (idx / 9);
+          const double jj = self ? Ja[i] * Ja[j] + Ja[9 + i] * Ja[9 + j] : 0.0;
+          acc[m] += jj - (Ha[3 * i] * Gb[3 * j] + Ha[3 * i + 1] * Gb[3 * j + 1] + Ha[3 * i + 2] * Gb[3 * j + 2]);
+        }
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int idx = lane + 32 * m;
+      if (idx >= 81) continue;
+      const int i = idx / 9, j = idx - 9 * (idx / 9);
+      if (a == b && i > j) continue;
+      S[(size_t)(9 * a + i) * n + 9 * b + j] = acc[m];
+      S[(size_t)(9 * b + j) * n + 9 * a + i] = acc[m];
+    }
+  }
+}
+
 __global__ void k_dense_diag(ceres_b200_ba_t ba, double* S, int n) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const int c = j / 9;
@@ -2569,6 +2637,35 @@ int ceres_b200_dense_schur_bytes(const ceres_b200_ba_t* ba, int64_t* bytes_out) 
   return CERES_B200_OK;
 }
 
+namespace {
+// The explicit S (undamped; k_dense_diag adds the damping): in the listed fixed order when
+// the struct carries the contribution list, else with float64 atomics.
+int assemble_explicit_schur(const ceres_b200_ba_t& ba, double* S, int n, cudaStream_t st) {
+  const DevInfo d = device_info();
+  if (ba.schur_blocks != nullptr) {
+    if (!ba.schur_block_start || !ba.schur_contrib || ba.num_schur_blocks < 0) return CERES_B200_EINVAL;
+    if (ba.num_schur_blocks > 0) {
+      long long grid = (ba.num_schur_blocks * 32 + kWarpBlock - 1) / kWarpBlock;
+      if (grid > 16LL * d.sms) grid = 16LL * d.sms;
+      count_launch();
+      if (ba.precision == CERES_B200_FP32)
+        k_schur_ordered<float><<<(unsigned)grid, kWarpBlock, 0, st>>>(ba, S, n);
+      else
+        k_schur_ordered<double><<<(unsigned)grid, kWarpBlock, 0, st>>>(ba, S, n);
+    }
+    return CERES_B200_OK;
+  }
+  if (ba.num_slices > 0) {
+    count_launch();
+    if (ba.precision == CERES_B200_FP32)
+      k_schur_explicit<float><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, S, n);
+    else
+      k_schur_explicit<double><<<slice_grid(ba, d), kWarpBlock, 0, st>>>(ba, S, n);
+  }
+  return CERES_B200_OK;
+}
+}  // namespace
+
 int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, void* stream) {
   if (!valid(ba) || !ba->step_cameras) return CERES_B200_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
@@ -2577,13 +2674,8 @@ int ceres_b200_ba_dense_schur_solve(const ceres_b200_ba_t* ba, double* work, voi
   if (!work) return CERES_B200_EINVAL;
   const DevInfo d = device_info();
   if (cudaMemsetAsync(work, 0, (size_t)n * n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
-  if (ba->num_slices > 0) {
-    count_launch();
-    if (ba->precision == CERES_B200_FP32)
-      k_schur_explicit<float><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, work, n);
-    else
-      k_schur_explicit<double><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, work, n);
-  }
+  const int arc = assemble_explicit_schur(*ba, work, n, st);
+  if (arc) return arc;
   count_launch();
   k_dense_diag<<<(n + 255) / 256, 256, 0, st>>>(*ba, work, n);
   if (n <= kCholSmemMax) {
@@ -2686,13 +2778,8 @@ int ceres_b200_ba_schur_matrix(const ceres_b200_ba_t* ba, double* S, void* strea
   if (n == 0) return CERES_B200_OK;
   const DevInfo d = device_info();
   if (cudaMemsetAsync(S, 0, (size_t)n * n * sizeof(double), st) != cudaSuccess) return CERES_B200_ECUDA;
-  if (ba->num_slices > 0) {
-    count_launch();
-    if (ba->precision == CERES_B200_FP32)
-      k_schur_explicit<float><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, S, n);
-    else
-      k_schur_explicit<double><<<slice_grid(*ba, d), kWarpBlock, 0, st>>>(*ba, S, n);
-  }
+  const int arc = assemble_explicit_schur(*ba, S, n, st);
+  if (arc) return arc;
   count_launch();
   k_dense_diag<<<(n + 255) / 256, 256, 0, st>>>(*ba, S, n);
   return check_launch();

@@ -32,6 +32,7 @@ _PRECOND = {
     PreconditionerType.CLUSTER_TRIDIAGONAL: _lib.PRECOND_CLUSTER,
 }
 _CLUSTER_MAX_DIM = 16384  # 9 x cameras of the largest component (the sweep's 32-bit element index)
+SCHUR_ORDER_MAX = 1 << 26  # contributions of the ordered explicit S (12 B each); longer lists sum with atomics
 
 PRECISIONS = ("fp64", "mixed")
 
@@ -125,6 +126,64 @@ def build_layout(camera_index: torch.Tensor, point_index: torch.Tensor, observat
     )
 
 
+def schur_contributions(L: Layout, nc: int, cam_const: torch.Tensor, pt_const: torch.Tensor, np_pad: int,
+                        limit: int = SCHUR_ORDER_MAX):
+    """The fixed summation order of the explicit reduced camera matrix: for every active
+    camera, each of its observations with itself and every ordered pair of its
+    observations of one active point (the diagonal block); for every two active cameras
+    a < b, each pair of their observations of one active point; grouped by block and
+    sorted by (point, slot i, slot j). Returns (blocks [B, 2] int32, block_start [B + 1]
+    int64, contributions [C, 3] int32 (slot i, slot j, point lane), B), or None when the
+    list's bound (the observations plus twice the pairs of observations of one point)
+    exceeds ``limit``. Torch ops on the layout's device."""
+    dev = L.cam_offsets.device
+    i64 = dict(dtype=torch.int64, device=dev)
+    no = int(L.cam_offsets[-1]) if nc else 0
+    ents = L.cam_entries[:no].to(torch.int64)                     # (slot, q), sorted by (camera, slot)
+    cam = torch.repeat_interleave(torch.arange(nc, **i64), (L.cam_offsets[1:] - L.cam_offsets[:-1]).to(torch.int64))
+    act = cam_const.to(dev)[cam] == 0
+    slot, q, cam = ents[act, 0], ents[act, 1], cam[act]
+    # the observations of active points, grouped by point (a stable sort keeps (camera, slot))
+    sel = torch.nonzero(pt_const.to(dev)[q] == 0).flatten()
+    sel = sel[torch.sort(q[sel], stable=True).indices]
+    ps, pq, pc = slot[sel], q[sel], cam[sel]
+    n = int(pq.numel())
+    idx = torch.arange(n, **i64)
+    if n:
+        start = torch.ones(n, dtype=torch.bool, device=dev)
+        start[1:] = pq[1:] != pq[:-1]
+        grp = torch.cumsum(start.to(torch.int64), 0) - 1
+        later = (torch.cumsum(torch.bincount(grp), 0) - 1)[grp] - idx  # observations after this one at its point
+    else:
+        later = idx
+    total = int(later.sum()) if n else 0
+    if int(slot.numel()) + 2 * total > limit:
+        return None
+    i = torch.repeat_interleave(idx, later)
+    j = i + 1 + torch.arange(total, **i64) - (torch.cumsum(later, 0) - later)[i]
+    ca, cb = pc[i], pc[j]
+    cross = ca != cb
+    dup = ~cross
+    lo, hi = torch.minimum(ca, cb), torch.maximum(ca, cb)
+    swap = ca > cb
+    # rows (block key, q, slot i, slot j): self pairs of every observation, the cross pairs
+    # oriented a < b, the same-camera pairs in both orders
+    blk = torch.cat([cam * nc + cam, (lo * nc + hi)[cross], (ca * nc + ca)[dup], (ca * nc + ca)[dup]])
+    qq = torch.cat([q, pq[i][cross], pq[i][dup], pq[i][dup]])
+    si = torch.cat([slot, torch.where(swap, ps[j], ps[i])[cross], ps[i][dup], ps[j][dup]])
+    sj = torch.cat([slot, torch.where(swap, ps[i], ps[j])[cross], ps[j][dup], ps[i][dup]])
+    o = torch.sort(si * max(L.num_slots, 1) + sj, stable=True).indices
+    o = o[torch.sort((blk * max(np_pad, 1) + qq)[o], stable=True).indices]
+    blk, qq, si, sj = blk[o], qq[o], si[o], sj[o]
+    uniq, cnt = torch.unique_consecutive(blk, return_counts=True)
+    blocks = torch.stack([uniq // max(nc, 1), uniq % max(nc, 1)], dim=1).to(torch.int32).contiguous()
+    bstart = torch.zeros(int(uniq.numel()) + 1, **i64)
+    bstart[1:] = torch.cumsum(cnt, 0)
+    contrib = torch.stack([si, sj, qq], dim=1).to(torch.int32).contiguous()
+    pad = torch.zeros(3, dtype=torch.int32, device=dev)  # non-null pointers for an empty list
+    return (blocks if blocks.numel() else pad, bstart, contrib if contrib.numel() else pad, int(uniq.numel()))
+
+
 def camera_items(cam_entries: torch.Tensor, cam_counts: torch.Tensor, num_slots: int, item_size: int | None = None):
     """The camera-major position of every slot (inverse of cam_entries' slot column,
     -1 for padding) and the camera work items: each camera's entries cut into runs of
@@ -188,6 +247,7 @@ class BAEngine:
                                              self.nc, self.np, item_size)
         self.item_size = int(item_size or _lib.CAM_ITEM)
         self._index = (camera_index, point_index, point_constant)
+        self._schur_order = None
         self.clusters: ClusterPlan | None = None
         L = self.layout
         self.np_pad = 32 * L.num_slices
@@ -400,9 +460,40 @@ class BAEngine:
             self._call("ceres_b200_ba_pcg", int(precond), int(min_iterations), int(max_iterations), float(tolerance),
                        int(max_refinements))
 
+    def ensure_schur_order(self) -> bool:
+        """Give the explicit-S paths (dense_schur_solve, schur_matrix) the fixed summation
+        order of ``schur_contributions`` (built once per problem); returns whether it is in
+        place (a list longer than SCHUR_ORDER_MAX is not built and the atomic summation
+        stays)."""
+        if self._schur_order is None:
+            order = schur_contributions(self.layout, self.nc, self.cam_const[:self.nc], self.pt_const, self.np_pad)
+            self._schur_order = order or ()
+            if order:
+                st = self.struct
+                st.schur_blocks, st.schur_block_start, st.schur_contrib = (_ptr(t) for t in order[:3])
+                st.num_schur_blocks = int(order[3])
+        return bool(self._schur_order)
+
+    def schur_matrix(self, ordered: bool = True) -> torch.Tensor:
+        """The explicit reduced camera matrix [9 nc, 9 nc] (float64) of the last assembly,
+        damping included; ``ordered``: in the fixed summation order where the list fits."""
+        if ordered:
+            self.ensure_schur_order()
+        n = 9 * self.nc
+        S = torch.empty((max(n, 1), max(n, 1)), dtype=torch.float64, device=self.device)
+        kept = self.struct.schur_blocks
+        if not ordered:
+            self.struct.schur_blocks = None
+        try:
+            self._call("ceres_b200_ba_schur_matrix", S.data_ptr())
+        finally:
+            self.struct.schur_blocks = kept
+        return S
+
     def dense_solve(self) -> None:
         if self.nc == 0:
             return
+        self.ensure_schur_order()
         if self.dense_work is None:
             nbytes = ctypes.c_int64(0)
             _lib.check(self.lib.ceres_b200_dense_schur_bytes(ctypes.byref(self.struct), ctypes.byref(nbytes)),

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define CERES_B200_ABI_VERSION 4
+#define CERES_B200_ABI_VERSION 5
 
 /* status codes */
 #define CERES_B200_OK 0
@@ -181,6 +181,18 @@ typedef struct ceres_b200_ba_t {
   int64_t scratch_bytes;
   uint32_t* counters;          /* [16] zero-initialised once; kernels leave them zero */
   double* stats;               /* [CERES_B200_NSTATS] */
+
+  /* the explicit reduced camera matrix in a fixed summation order (dense_schur_solve,
+   * schur_matrix), listed block by block (cameras a <= b), each block's contributions
+   * (slot i of a, slot j of b, point lane q) with the points ascending: -G_i W_q^-1 G_j^T,
+   * plus Jc_i^T Jc_i where i == j (a diagonal block lists each observation of the
+   * camera with itself and every ordered pair of its observations of one point).
+   * Null: the blocks are summed with float64 atomics, in an order that varies from run
+   * to run. */
+  const int32_t* schur_blocks;       /* [num_schur_blocks][2] cameras a <= b */
+  const int64_t* schur_block_start;  /* [num_schur_blocks + 1] first contribution of each block */
+  const int32_t* schur_contrib;      /* [contributions][3] (slot i, slot j, point lane q) */
+  int64_t num_schur_blocks;
 } ceres_b200_ba_t;
 
 /* ABI version of the loaded library (CERES_B200_ABI_VERSION). */
