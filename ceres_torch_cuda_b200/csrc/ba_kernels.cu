@@ -355,9 +355,9 @@ struct CamObs {
   double wg[3];
 };
 
-// The record comes from the camera-major copy when there is one (entry e: consecutive
-// threads read consecutive records), else from its slot; residual and point blocks are
-// gathered by slot and point.
+// Register path (float64 store): the record comes from the camera-major copy when there
+// is one (entry e: consecutive threads read consecutive records), else from its slot;
+// residual and point blocks are gathered by slot and point.
 template <typename T>
 __device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T* __restrict__ jac,
                                              const T* __restrict__ cm, const T* __restrict__ winv, int e, int2 ent,
@@ -373,122 +373,304 @@ __device__ __forceinline__ void cam_obs_load(const ceres_b200_ba_t& ba, const T*
   for (int i = 0; i < 3; ++i) o.wg[i] = ba.winv_ga[3 * (size_t)ent.y + i];
 }
 
+// Asynchronous staging of the camera reduction's inputs (cp.async, 16- and 8-byte
+// copies). Each thread stages the observations it will reduce itself, kStages chunks
+// ahead, into its own column of a structure-of-arrays stage (conflict-free reads);
+// it only waits for its own copies (cp.async.wait_group), so no CTA barrier is needed.
+// A stage is refilled after the thread has consumed the values it read from it.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// The float32 store is staged; the float64 store's records (192 bytes) are loaded into
+// registers just before use: staged through shared memory they ran slower (0.62 instead
+// of 0.50 ms on the 6.0M-observation problem with two stages).
+template <typename T>
+struct CamStage {
+  static constexpr bool kStaged = sizeof(T) == 4;
+  static constexpr int kRecV = kRec * (int)sizeof(T) / 16;  // 16-byte pieces of a record
+  static constexpr int kWiV = 6 * (int)sizeof(T) / 8;        // 8-byte pieces of W^-1
+  static constexpr int kStages = 4;
+  // per thread: record, residual, W^-1, W^-1 g, entry
+  static constexpr size_t kStageBytes = (size_t)kCamBlock * (16 * kRecV + 16 + 8 * kWiV + 24 + 8);
+  static constexpr size_t kBytes = kStaged ? kStages * kStageBytes : 0;
+  static constexpr size_t kRes = (size_t)16 * kRecV * kCamBlock;
+  static constexpr size_t kWi = kRes + (size_t)16 * kCamBlock;
+  static constexpr size_t kWg = kWi + (size_t)8 * kWiV * kCamBlock;
+  static constexpr size_t kEnt = kWg + (size_t)24 * kCamBlock;
+};
+
+// The record comes from the camera-major copy when there is one (entry e: consecutive
+// threads read consecutive records), else from its slot; residual and point blocks are
+// gathered by slot and point.
+template <typename T>
+__device__ __forceinline__ void cam_stage_issue(const ceres_b200_ba_t& ba, const T* __restrict__ jac,
+                                                const T* __restrict__ cm, const T* __restrict__ winv, int e,
+                                                int2 ent, char* stage) {
+  using D = CamStage<T>;
+  const int t = threadIdx.x;
+  const uint4* rs = reinterpret_cast<const uint4*>(cm != nullptr ? cm + (size_t)e * kRec : jac + (size_t)ent.x * kRec);
+  uint4* rd = reinterpret_cast<uint4*>(stage);
+#pragma unroll
+  for (int i = 0; i < D::kRecV; ++i) cp_async16(rd + i * kCamBlock + t, rs + i);
+  cp_async16(reinterpret_cast<double2*>(stage + D::kRes) + t, reinterpret_cast<const double2*>(ba.res) + ent.x);
+  const uint2* ws = reinterpret_cast<const uint2*>(winv + 6 * (size_t)ent.y);
+  uint2* wd = reinterpret_cast<uint2*>(stage + D::kWi);
+#pragma unroll
+  for (int i = 0; i < D::kWiV; ++i) cp_async8(wd + i * kCamBlock + t, ws + i);
+  double* gd = reinterpret_cast<double*>(stage + D::kWg);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) cp_async8(gd + i * kCamBlock + t, ba.winv_ga + 3 * (size_t)ent.y + i);
+  reinterpret_cast<int2*>(stage + D::kEnt)[t] = ent;
+}
+
+template <typename T>
+__device__ __forceinline__ void cam_stage_read(const char* stage, CamObs<T>& o) {
+  using D = CamStage<T>;
+  const int t = threadIdx.x;
+  const uint4* rd = reinterpret_cast<const uint4*>(stage);
+#pragma unroll
+  for (int i = 0; i < D::kRecV; ++i) {
+    const uint4 v = rd[i * kCamBlock + t];
+    if constexpr (sizeof(T) == 4) {
+      o.rv[4 * i] = __uint_as_float(v.x); o.rv[4 * i + 1] = __uint_as_float(v.y);
+      o.rv[4 * i + 2] = __uint_as_float(v.z); o.rv[4 * i + 3] = __uint_as_float(v.w);
+    } else {
+      o.rv[2 * i] = __hiloint2double((int)v.y, (int)v.x);
+      o.rv[2 * i + 1] = __hiloint2double((int)v.w, (int)v.z);
+    }
+  }
+  o.r = reinterpret_cast<const double2*>(stage + D::kRes)[t];
+  const uint2* wd = reinterpret_cast<const uint2*>(stage + D::kWi);
+#pragma unroll
+  for (int i = 0; i < D::kWiV; ++i) {
+    const uint2 v = wd[i * kCamBlock + t];
+    if constexpr (sizeof(T) == 4) {
+      o.wi[2 * i] = __uint_as_float(v.x); o.wi[2 * i + 1] = __uint_as_float(v.y);
+    } else {
+      o.wi[i] = __hiloint2double((int)v.y, (int)v.x);
+    }
+  }
+  const double* gd = reinterpret_cast<const double*>(stage + D::kWg);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) o.wg[i] = gd[i * kCamBlock + t];
+  o.ent = reinterpret_cast<const int2*>(stage + D::kEnt)[t];
+}
+
+// Warp sums of 72 values, scattered over the lanes (recursive halving): at the xor
+// distances 16, 8, 4, 2, 1 each lane keeps one half of its values and adds the partner's
+// copy of that half, so it ends with the sums of (at most) 3 indices, 36 b4 + 18 b3 +
+// 9 b2 + 5 b1 + 3 b0 + k (b: the lane's bits; k < 3, 3 b0 + k < 5, index within the
+// group of 9 below 9), each added over the same xor tree as warp_sum, so the sums are
+// warp_sum's bit for bit, in about half the instructions.
+__device__ __forceinline__ void warp_reduce_scatter72(double (&v)[72], int lane) {
+  constexpr unsigned kFull = 0xffffffffu;
+  {
+    const bool hi = (lane & 16) != 0;
+#pragma unroll
+    for (int j = 0; j < 36; ++j) {
+      const double keep = hi ? v[j + 36] : v[j], send = hi ? v[j] : v[j + 36];
+      v[j] = keep + __shfl_xor_sync(kFull, send, 16);
+    }
+  }
+  {
+    const bool hi = (lane & 8) != 0;
+#pragma unroll
+    for (int j = 0; j < 18; ++j) {
+      const double keep = hi ? v[j + 18] : v[j], send = hi ? v[j] : v[j + 18];
+      v[j] = keep + __shfl_xor_sync(kFull, send, 8);
+    }
+  }
+  {
+    const bool hi = (lane & 4) != 0;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const double keep = hi ? v[j + 9] : v[j], send = hi ? v[j] : v[j + 9];
+      v[j] = keep + __shfl_xor_sync(kFull, send, 4);
+    }
+  }
+  v[9] = 0.0;  // 9 values: padded to 10
+  {
+    const bool hi = (lane & 2) != 0;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const double keep = hi ? v[j + 5] : v[j], send = hi ? v[j] : v[j + 5];
+      v[j] = keep + __shfl_xor_sync(kFull, send, 2);
+    }
+  }
+  v[5] = 0.0;  // 5 values: padded to 6
+  {
+    const bool hi = (lane & 1) != 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double keep = hi ? v[j + 3] : v[j], send = hi ? v[j] : v[j + 3];
+      v[j] = keep + __shfl_xor_sync(kFull, send, 1);
+    }
+  }
+}
+
 // Phase 1: one CTA per camera reduces the 72 sums over the camera's observations
 // into acc_out[c][72] (float64). kHbb: the camera block is the Hbb block sum Jc^T Jc
 // (M = I below) instead of the Schur block; the base of SCHUR_POWER_SERIES_EXPANSION.
+// Thread t reduces the camera's entries t, t + 128, ...; with the float32 store their
+// inputs arrive through the cp.async stages (CamStage), kStages observations ahead.
+// (Cutting the camera-major list into equal ranges, one resident CTA each, with
+// per-camera segment sums folded afterwards, ran slower: 0.42 instead of 0.39 ms mixed
+// and 0.64 instead of 0.55 ms float64 for the assembly of the 6.0M-observation problem.)
 template <typename T, bool kDup, bool kHbb = false>
 __global__ void __launch_bounds__(kCamBlock) k_camera_reduce(ceres_b200_ba_t ba, double* __restrict__ acc_out) {
   using A = double;
+  using D = CamStage<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double sred[kCamAcc * (kCamBlock / 32)];
   const int c = blockIdx.x;
   const T* __restrict__ jac = reinterpret_cast<const T*>(ba.jac);
   const T* __restrict__ cm = reinterpret_cast<const T*>(ba.cm_jac);
   const T* __restrict__ winv = reinterpret_cast<const T*>(ba.winv);
-  A av[54];      // Schur block (upper triangle, 45), column sums (9)
-  double ag[18]; // gradient (9), reduced rhs (9)
-#pragma unroll
-  for (int i = 0; i < 54; ++i) av[i] = (A)0;
-#pragma unroll
-  for (int i = 0; i < 18; ++i) ag[i] = 0.0;
-  const bool cconst = ba.cam_const[c] != 0;
   const int e0 = ba.cam_offsets[c], e1 = ba.cam_offsets[c + 1];
-  if (!cconst) {
-    const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);
-    const int stride = blockDim.x;
-    const int first = e0 + threadIdx.x;
-    // entries are read two observations ahead, so each observation waits for one
-    // gather (its data) instead of two (entry, then data): 0.43 -> 0.39 ms on the
-    // 6.0M-observation problem (float32 store). Holding the next observation's data in
-    // registers as well spilled and ran slower.
-    int2 en1 = first < e1 ? ents[first] : make_int2(0, 0);
-    int2 en2 = first + stride < e1 ? ents[first + stride] : make_int2(0, 0);
-    for (int e = first; e < e1; e += stride) {
-      CamObs<T> cur;
-      cam_obs_load(ba, jac, cm, winv, e, en1, cur);
-      en1 = en2;
-      en2 = e + 2 * stride < e1 ? ents[e + 2 * stride] : make_int2(0, 0);
-      const size_t slot = (size_t)cur.ent.x;
-      const int q = cur.ent.y;
-      const T* rv = cur.rv;
-      const double2 r = cur.r;
-      A wi[6];
+  {
+    A av[54];      // Schur block (upper triangle, 45), column sums (9)
+    double ag[18]; // gradient (9), reduced rhs (9)
 #pragma unroll
-      for (int i = 0; i < 6; ++i) wi[i] = (A)cur.wi[i];
-      const double* wg = cur.wg;
-      A jp0[3], jp1[3];
+    for (int i = 0; i < 54; ++i) av[i] = (A)0;
 #pragma unroll
-      for (int m = 0; m < 3; ++m) { jp0[m] = (A)rv[18 + m]; jp1[m] = (A)rv[21 + m]; }
-      // P = Jp W^-1 (2x3); B = P Jp^T (2x2); a = Jp W^-1 g_a
-      A P0[3], P1[3];
-      P0[0] = wi[0] * jp0[0] + wi[1] * jp0[1] + wi[2] * jp0[2];
-      P0[1] = wi[1] * jp0[0] + wi[3] * jp0[1] + wi[4] * jp0[2];
-      P0[2] = wi[2] * jp0[0] + wi[4] * jp0[1] + wi[5] * jp0[2];
-      P1[0] = wi[0] * jp1[0] + wi[1] * jp1[1] + wi[2] * jp1[2];
-      P1[1] = wi[1] * jp1[0] + wi[3] * jp1[1] + wi[4] * jp1[2];
-      P1[2] = wi[2] * jp1[0] + wi[4] * jp1[1] + wi[5] * jp1[2];
-      const A B00 = P0[0] * jp0[0] + P0[1] * jp0[1] + P0[2] * jp0[2];
-      const A B01 = P0[0] * jp1[0] + P0[1] * jp1[1] + P0[2] * jp1[2];
-      const A B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
-      const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
-      const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
-      const A M00 = kHbb ? (A)1 : (A)1 - B00, M01 = kHbb ? (A)0 : -B01, M11 = kHbb ? (A)1 : (A)1 - B11;
-      A K0[9], K1[9];
+    for (int i = 0; i < 18; ++i) ag[i] = 0.0;
+    const bool cconst = ba.cam_const[c] != 0;
+    if (!cconst) {
+      const int2* __restrict__ ents = reinterpret_cast<const int2*>(ba.cam_entries);
+      const int stride = blockDim.x;
+      const int first = e0 + threadIdx.x;
+      char* stages = reinterpret_cast<char*>(smem_raw);
+      int en_i = first, st = 0;
+      int2 en_next = make_int2(0, 0), en2 = make_int2(0, 0);
+      if constexpr (D::kStaged) {
 #pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        const A c0 = (A)rv[j], c1 = (A)rv[9 + j];
-        K0[j] = M00 * c0 + M01 * c1;
-        K1[j] = M01 * c0 + M11 * c1;
-        av[45 + j] += c0 * c0 + c1 * c1;
-        const double d0 = (double)rv[j], d1 = (double)rv[9 + j];
-        ag[j] += d0 * r.x + d1 * r.y;
-        ag[9 + j] += d0 * (r.x + a0) + d1 * (r.y + a1);
+        for (int k = 0; k < D::kStages; ++k) {
+          const int e = first + k * stride;
+          if (e < e1) cam_stage_issue<T>(ba, jac, cm, winv, e, ents[e], stages + k * D::kStageBytes);
+          cp_async_commit();
+        }
+        en_i = first + D::kStages * stride;                  // the next entry to stage
+        en_next = en_i < e1 ? ents[en_i] : make_int2(0, 0);  // its (slot, point), read one chunk early
+      } else {
+        // entries are read two observations ahead, so each observation waits for one
+        // gather (its data) instead of two (entry, then data)
+        en_next = first < e1 ? ents[first] : make_int2(0, 0);
+        en2 = first + stride < e1 ? ents[first + stride] : make_int2(0, 0);
       }
+      for (int e = first; e < e1; e += stride) {
+        CamObs<T> cur;
+        if constexpr (D::kStaged) {
+          cp_async_wait<D::kStages - 1>();
+          cam_stage_read<T>(stages + st * D::kStageBytes, cur);
+        } else {
+          cam_obs_load<T>(ba, jac, cm, winv, e, en_next, cur);
+          en_next = en2;
+          en2 = e + 2 * stride < e1 ? ents[e + 2 * stride] : make_int2(0, 0);
+        }
+        const size_t slot = (size_t)cur.ent.x;
+        const int q = cur.ent.y;
+        const T* rv = cur.rv;
+        const double2 r = cur.r;
+        A wi[6];
 #pragma unroll
-      for (int j = 0; j < 9; ++j)
+        for (int i = 0; i < 6; ++i) wi[i] = (A)cur.wi[i];
+        const double* wg = cur.wg;
+        A jp0[3], jp1[3];
 #pragma unroll
-        for (int l = j; l < 9; ++l) av[tri9(j, l)] += (A)rv[j] * K0[l] + (A)rv[9 + j] * K1[l];
+        for (int m = 0; m < 3; ++m) { jp0[m] = (A)rv[18 + m]; jp1[m] = (A)rv[21 + m]; }
+        // P = Jp W^-1 (2x3); B = P Jp^T (2x2); a = Jp W^-1 g_a
+        A P0[3], P1[3];
+        P0[0] = wi[0] * jp0[0] + wi[1] * jp0[1] + wi[2] * jp0[2];
+        P0[1] = wi[1] * jp0[0] + wi[3] * jp0[1] + wi[4] * jp0[2];
+        P0[2] = wi[2] * jp0[0] + wi[4] * jp0[1] + wi[5] * jp0[2];
+        P1[0] = wi[0] * jp1[0] + wi[1] * jp1[1] + wi[2] * jp1[2];
+        P1[1] = wi[1] * jp1[0] + wi[3] * jp1[1] + wi[4] * jp1[2];
+        P1[2] = wi[2] * jp1[0] + wi[4] * jp1[1] + wi[5] * jp1[2];
+        const A B00 = P0[0] * jp0[0] + P0[1] * jp0[1] + P0[2] * jp0[2];
+        const A B01 = P0[0] * jp1[0] + P0[1] * jp1[1] + P0[2] * jp1[2];
+        const A B11 = P1[0] * jp1[0] + P1[1] * jp1[1] + P1[2] * jp1[2];
+        const double a0 = (double)rv[18] * wg[0] + (double)rv[19] * wg[1] + (double)rv[20] * wg[2];
+        const double a1 = (double)rv[21] * wg[0] + (double)rv[22] * wg[1] + (double)rv[23] * wg[2];
+        const A M00 = kHbb ? (A)1 : (A)1 - B00, M01 = kHbb ? (A)0 : -B01, M11 = kHbb ? (A)1 : (A)1 - B11;
+        A K0[9], K1[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+          const A c0 = (A)rv[j], c1 = (A)rv[9 + j];
+          K0[j] = M00 * c0 + M01 * c1;
+          K1[j] = M01 * c0 + M11 * c1;
+          av[45 + j] += c0 * c0 + c1 * c1;
+          const double d0 = (double)rv[j], d1 = (double)rv[9 + j];
+          ag[j] += d0 * r.x + d1 * r.y;
+          ag[9 + j] += d0 * (r.x + a0) + d1 * (r.y + a1);
+        }
+#pragma unroll
+        for (int j = 0; j < 9; ++j)
+#pragma unroll
+          for (int l = j; l < 9; ++l) av[tri9(j, l)] += (A)rv[j] * K0[l] + (A)rv[9 + j] * K1[l];
 
-      if (kDup && !kHbb) {
-        // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
-        const int sidx = q >> 5, ln = q & 31;
-        const int len = ba.slice_len[sidx];
-        const size_t sb = (size_t)ba.slice_base[sidx];
-        for (int k = 0; k < len; ++k) {
-          const size_t slot2 = sb + 32 * (size_t)k + ln;
-          if (slot2 == slot || ba.slot_cam[slot2] != c) continue;
-          T rk[kRec];
-          load_rec(jac, slot2, rk);
-          const A C00 = P0[0] * (A)rk[18] + P0[1] * (A)rk[19] + P0[2] * (A)rk[20];
-          const A C01 = P0[0] * (A)rk[21] + P0[1] * (A)rk[22] + P0[2] * (A)rk[23];
-          const A C10 = P1[0] * (A)rk[18] + P1[1] * (A)rk[19] + P1[2] * (A)rk[20];
-          const A C11 = P1[0] * (A)rk[21] + P1[1] * (A)rk[22] + P1[2] * (A)rk[23];
+        if (kDup && !kHbb) {
+          // other observations of the same point in this camera: -Jc_i^T P_i Jp_k^T Jc_k
+          const int sidx = q >> 5, ln = q & 31;
+          const int len = ba.slice_len[sidx];
+          const size_t sb = (size_t)ba.slice_base[sidx];
+          for (int k = 0; k < len; ++k) {
+            const size_t slot2 = sb + 32 * (size_t)k + ln;
+            if (slot2 == slot || ba.slot_cam[slot2] != c) continue;
+            T rk[kRec];
+            load_rec(jac, slot2, rk);
+            const A C00 = P0[0] * (A)rk[18] + P0[1] * (A)rk[19] + P0[2] * (A)rk[20];
+            const A C01 = P0[0] * (A)rk[21] + P0[1] * (A)rk[22] + P0[2] * (A)rk[23];
+            const A C10 = P1[0] * (A)rk[18] + P1[1] * (A)rk[19] + P1[2] * (A)rk[20];
+            const A C11 = P1[0] * (A)rk[21] + P1[1] * (A)rk[22] + P1[2] * (A)rk[23];
 #pragma unroll
-          for (int j = 0; j < 9; ++j) {
-            const A t0 = (A)rv[j] * C00 + (A)rv[9 + j] * C10;
-            const A t1 = (A)rv[j] * C01 + (A)rv[9 + j] * C11;
+            for (int j = 0; j < 9; ++j) {
+              const A t0 = (A)rv[j] * C00 + (A)rv[9 + j] * C10;
+              const A t1 = (A)rv[j] * C01 + (A)rv[9 + j] * C11;
 #pragma unroll
-            for (int l = j; l < 9; ++l) av[tri9(j, l)] -= t0 * (A)rk[l] + t1 * (A)rk[9 + l];
+              for (int l = j; l < 9; ++l) av[tri9(j, l)] -= t0 * (A)rk[l] + t1 * (A)rk[9 + l];
+            }
           }
         }
+        if constexpr (D::kStaged) {
+          // refill this stage with the observation kStages chunks ahead (its values are consumed)
+          if (en_i < e1) cam_stage_issue<T>(ba, jac, cm, winv, en_i, en_next, stages + st * D::kStageBytes);
+          cp_async_commit();
+          en_i += stride;
+          en_next = en_i < e1 ? ents[en_i] : make_int2(0, 0);
+          st = st + 1 == D::kStages ? 0 : st + 1;
+        }
       }
+      if constexpr (D::kStaged) cp_async_wait<0>();
     }
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    {
+      double v[72];
 #pragma unroll
-  for (int i = 0; i < 54; ++i) {
-    const double v = warp_sum((double)av[i]);
-    if (lane == 0) sred[i * nw + wid] = v;
-  }
+      for (int i = 0; i < 54; ++i) v[i] = (double)av[i];
 #pragma unroll
-  for (int i = 0; i < 18; ++i) {
-    const double v = warp_sum(ag[i]);
-    if (lane == 0) sred[(54 + i) * nw + wid] = v;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x) {
-    double sum = 0.0;
-    for (int w = 0; w < nw; ++w) sum += sred[i * nw + w];
-    acc_out[(size_t)c * kCamAcc + i] = sum;
+      for (int i = 0; i < 18; ++i) v[54 + i] = ag[i];
+      warp_reduce_scatter72(v, lane);
+      const int base = 36 * ((lane >> 4) & 1) + 18 * ((lane >> 3) & 1) + 9 * ((lane >> 2) & 1);
+      const int l0 = 5 * ((lane >> 1) & 1), s0 = 3 * (lane & 1);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (s0 + k < 5 && l0 + s0 + k < 9) sred[(base + l0 + s0 + k) * nw + wid] = v[k];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kCamAcc; i += blockDim.x) {
+      double sum = 0.0;
+      for (int w = 0; w < nw; ++w) sum += sred[i * nw + w];
+      acc_out[(size_t)c * kCamAcc + i] = sum;
+    }
   }
 }
 
@@ -2266,9 +2448,19 @@ int matvec64(const ceres_b200_ba_t& ba, const double* x, double* y, cudaStream_t
 // blocks for the SPSE initial point as well, into the scratch. Each block set is one
 // reduction over the camera-major lists; the damping, rhs and gradient stats come
 // out of every reduction alike.
+template <typename T, bool kDup, bool kHbb = false>
+int launch_camera_reduce(const ceres_b200_ba_t& ba, double* acc, cudaStream_t st) {
+  const size_t smem = CamStage<T>::kBytes;
+  if (cudaFuncSetAttribute(k_camera_reduce<T, kDup, kHbb>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return CERES_B200_ESMEM;
+  k_camera_reduce<T, kDup, kHbb><<<ba.num_cameras, kCamBlock, smem, st>>>(ba, acc);
+  return CERES_B200_OK;
+}
+
 template <typename T>
-void camera_assemble_impl(const ceres_b200_ba_t& ba, const PcgLayout& L, char* scratch, double inv_radius,
-                          double mn, double mx, int jacobi_scaling, int pc, int flags, cudaStream_t st) {
+int camera_assemble_impl(const ceres_b200_ba_t& ba, const PcgLayout& L, char* scratch, double inv_radius,
+                         double mn, double mx, int jacobi_scaling, int pc, int flags, cudaStream_t st) {
   double* partials = reinterpret_cast<double*>(scratch);
   double* acc = reinterpret_cast<double*>(scratch + L.cam_acc);
   const int nc = ba.num_cameras;
@@ -2276,18 +2468,21 @@ void camera_assemble_impl(const ceres_b200_ba_t& ba, const PcgLayout& L, char* s
   double* pre = reinterpret_cast<double*>(ba.precond);
   const bool spse = pc == CERES_B200_PRECOND_SCHUR_POWER_SERIES;
   count_launch(2);
-  if (spse) k_camera_reduce<T, false, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
-  else if (ba.has_duplicate_cameras) k_camera_reduce<T, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
-  else k_camera_reduce<T, false><<<nc, kCamBlock, 0, st>>>(ba, acc);
+  int rc = spse ? launch_camera_reduce<T, false, true>(ba, acc, st)
+                : (ba.has_duplicate_cameras ? launch_camera_reduce<T, true>(ba, acc, st)
+                                            : launch_camera_reduce<T, false>(ba, acc, st));
+  if (rc) return rc;
   k_camera_finish<T><<<fgrid, 32 * kFinishWarps, 0, st>>>(ba, acc, inv_radius, mn, mx, jacobi_scaling,
                                                          spse ? CERES_B200_PRECOND_SCHUR_JACOBI : pc, partials, pre);
   if ((flags & CERES_B200_PRECOND_FLAG_SPSE_BASE) && !spse) {
     count_launch(2);
-    k_camera_reduce<T, false, true><<<nc, kCamBlock, 0, st>>>(ba, acc);
+    rc = launch_camera_reduce<T, false, true>(ba, acc, st);
+    if (rc) return rc;
     k_camera_finish<T><<<fgrid, 32 * kFinishWarps, 0, st>>>(ba, acc, inv_radius, mn, mx, jacobi_scaling,
                                                            CERES_B200_PRECOND_SCHUR_JACOBI, partials,
                                                            reinterpret_cast<double*>(scratch + L.spse_base));
   }
+  return CERES_B200_OK;
 }
 
 template <typename T>
@@ -2510,10 +2705,12 @@ int ceres_b200_ba_camera_assemble(const ceres_b200_ba_t* ba, double radius, doub
   cudaStream_t st = (cudaStream_t)stream;
   const double inv_radius = 1.0 / fmax(radius, kEps64);
   char* scratch = reinterpret_cast<char*>(ba->scratch);
-  if (ba->precision == CERES_B200_FP32)
-    camera_assemble_impl<float>(*ba, L, scratch, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, pc, flags, st);
-  else
-    camera_assemble_impl<double>(*ba, L, scratch, inv_radius, min_diagonal, max_diagonal, jacobi_scaling, pc, flags, st);
+  const int rc = ba->precision == CERES_B200_FP32
+                     ? camera_assemble_impl<float>(*ba, L, scratch, inv_radius, min_diagonal, max_diagonal,
+                                                   jacobi_scaling, pc, flags, st)
+                     : camera_assemble_impl<double>(*ba, L, scratch, inv_radius, min_diagonal, max_diagonal,
+                                                    jacobi_scaling, pc, flags, st);
+  if (rc) return rc;
   return check_launch();
 }
 
