@@ -145,6 +145,10 @@ __global__ void k_camera_frames(const double* __restrict__ cams, double* __restr
 // cost partials in slice_part (scratch); otherwise (the allocation-free entry, no
 // scratch) every observation computes its camera's rotation and the CTAs take fixed
 // slice sets (next_cta_slice) with per-CTA partials.
+// Staging each lane's next two frames and observations into shared memory with cp.async
+// (as the camera reduction does) ran slower here, 0.56 instead of 0.50 ms on the
+// 6.0M-observation problem: the kernel is bound by its L1 data path (62% busy; 78% with
+// the staging's copies and shared-memory reads), not by the latency of the gathers.
 template <typename T, bool kJac, bool kFrames>
 __global__ void __launch_bounds__(kWarpBlock, kJac ? CERES_B200_EVAL_MIN_BLOCKS : CERES_B200_EVAL_NOJAC_MIN_BLOCKS)
 k_evaluate(ceres_b200_ba_t ba, double* partials, const double* __restrict__ frames, double* __restrict__ slice_part) {
