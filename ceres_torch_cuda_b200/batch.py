@@ -49,12 +49,33 @@ class BatchLayout:
     num_slices: int
 
 
+def batch_ints(cam_counts: np.ndarray, pt_counts: np.ndarray) -> np.ndarray:
+    """The per-problem integers build_batch_layout needs on the device, in its order."""
+    B = len(cam_counts)
+    pt_off_in = np.zeros(B + 1, dtype=np.int64)
+    pt_off_in[1:] = np.cumsum(pt_counts)
+    cam_off = np.zeros(B + 1, dtype=np.int64)
+    cam_off[1:] = np.cumsum(cam_counts)
+    slice_off = np.zeros(B + 1, dtype=np.int64)
+    slice_off[1:] = np.cumsum((pt_counts + 31) // 32)
+    return np.concatenate([pt_counts, pt_off_in[:-1], 32 * slice_off[:-1], cam_counts, cam_off, slice_off]).astype(
+        np.int64)
+
+
 def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_index: torch.Tensor,
-                       point_index: torch.Tensor, observations: torch.Tensor) -> BatchLayout:
+                       point_index: torch.Tensor, observations: torch.Tensor, *, ints: torch.Tensor | None = None,
+                       obs_counts: np.ndarray | None = None, track_stats: list | None = None) -> BatchLayout:
     """``camera_index`` / ``point_index`` are global (problem offsets added). Points are
     sorted by track length (descending, stable in point id) within their problem, and
-    each problem is padded to whole slices of 32. Device work on the current stream with
-    one device-to-host read (the slot count and the duplicate-camera flag)."""
+    each problem is padded to whole slices of 32. Device work on the current stream.
+
+    ``ints``: batch_ints(cam_counts, pt_counts) already on the device (else copied here).
+    ``track_stats``: each problem's (most observations of one point, duplicate flag) with
+    ``obs_counts``; the slot count is then taken from the host bound
+    sum_p (32 max_track_p + no_p) (slice s >= 1 of a problem is no longer than the mean
+    track of slice s - 1, so a problem's slices hold at most 32 max_track + no slots) and
+    the layout is built with no device-to-host read; without them, one read (the slot
+    count and the duplicate flag)."""
     dev = camera_index.device
     B = len(cam_counts)
     ci = camera_index.to(torch.int64)
@@ -62,20 +83,12 @@ def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_ind
     no = int(ci.numel())
     NP = int(pt_counts.sum())
     NC = int(cam_counts.sum())
-    pt_off_in = np.zeros(B + 1, dtype=np.int64)
-    pt_off_in[1:] = np.cumsum(pt_counts)
-    cam_off = np.zeros(B + 1, dtype=np.int64)
-    cam_off[1:] = np.cumsum(cam_counts)
-    slices_per = (pt_counts + 31) // 32
-    slice_off = np.zeros(B + 1, dtype=np.int64)
-    slice_off[1:] = np.cumsum(slices_per)
-    S = int(slice_off[-1])
+    S = int(((pt_counts + 31) // 32).sum())
     i64 = dict(dtype=torch.int64, device=dev)
-    # the per-problem integers go to the device in one copy
-    host = np.concatenate([pt_counts, pt_off_in[:-1], 32 * slice_off[:-1], cam_counts, cam_off, slice_off])
-    dv = torch.from_numpy(host.astype(np.int64)).to(dev, non_blocking=False)
+    if ints is None:
+        ints = torch.from_numpy(batch_ints(cam_counts, pt_counts)).to(dev)
     pt_counts_d, start_in, q_base, cam_counts_d, cam_off_d, slice_off_d = torch.split(
-        dv, [B, B, B, B, B + 1, B + 1])
+        ints, [B, B, B, B, B + 1, B + 1])
     point_problem = torch.repeat_interleave(torch.arange(B, device=dev), pt_counts_d, output_size=NP)
     counts = torch.zeros(NP, **i64)
     if no:
@@ -93,13 +106,17 @@ def build_batch_layout(cam_counts: np.ndarray, pt_counts: np.ndarray, camera_ind
     slice_len = counts_q.view(S, 32).amax(dim=1) if S else counts_q[:0]
     csum = torch.cumsum(slice_len, 0)
     slice_base = 32 * (csum - slice_len)
-    dup = torch.zeros((), **i64)
-    if no > 1:
-        pk = torch.sort(pi * max(NC, 1) + ci).values
-        dup = (pk[1:] == pk[:-1]).any().to(torch.int64)
-    info = torch.stack([csum[-1] if S else torch.zeros((), **i64), dup]).cpu()
-    num_slots = 32 * int(info[0])
-    has_dup = bool(info[1])
+    if track_stats is not None and obs_counts is not None:
+        num_slots = int(sum(32 * t[0] for t in track_stats) + int(np.sum(obs_counts)))
+        has_dup = any(bool(t[1]) for t in track_stats)
+    else:
+        dup = torch.zeros((), **i64)
+        if no > 1:
+            pk = torch.sort(pi * max(NC, 1) + ci).values
+            dup = (pk[1:] == pk[:-1]).any().to(torch.int64)
+        info = torch.stack([csum[-1] if S else torch.zeros((), **i64), dup]).cpu()
+        num_slots = 32 * int(info[0])
+        has_dup = bool(info[1])
     if no:
         obs_sorted = torch.argsort(pi, stable=True)
         pstart = torch.cumsum(counts, 0) - counts
@@ -183,16 +200,23 @@ class BatchSolver:
         cam_off = np.concatenate([[0], np.cumsum(cam_counts)])
         pt_off = np.concatenate([[0], np.cumsum(pt_counts)])
         self.cam_off_np, self.pt_off_np = cam_off, pt_off
-        # global indices: each problem's indices plus its offsets, in a few batch-wide operations
+        # global indices: each problem's indices plus its offsets, in a few batch-wide
+        # operations; every per-problem integer goes up in one asynchronous copy from
+        # pinned memory, so the host does not wait for the stream
+        nb = len(problems)
         obs_counts = np.array([p.num_observations for p in problems], dtype=np.int64)
-        offs = torch.from_numpy(np.concatenate([cam_off[:-1], pt_off[:-1], obs_counts])).to(dev)
-        per_obs = torch.repeat_interleave(torch.arange(len(problems), device=dev), offs[2 * len(problems):],
+        host = torch.from_numpy(np.concatenate([cam_off[:-1], pt_off[:-1], obs_counts,
+                                                batch_ints(cam_counts, pt_counts)])).pin_memory()
+        dv = host.to(dev, non_blocking=True)
+        offs, ints = dv[:3 * nb], dv[3 * nb:]
+        per_obs = torch.repeat_interleave(torch.arange(nb, device=dev), offs[2 * nb:],
                                           output_size=int(obs_counts.sum()))
-        ci = torch.cat([p.camera_index for p in problems]).to(dev, torch.int64) + offs[:len(problems)][per_obs]
-        pi = torch.cat([p.point_index for p in problems]).to(dev, torch.int64) + \
-            offs[len(problems):2 * len(problems)][per_obs]
+        ci = torch.cat([p.camera_index for p in problems]).to(dev, torch.int64) + offs[:nb][per_obs]
+        pi = torch.cat([p.point_index for p in problems]).to(dev, torch.int64) + offs[nb:2 * nb][per_obs]
         obs = torch.cat([p.observations for p in problems]).to(dev, torch.float64)
-        L = build_batch_layout(cam_counts, pt_counts, ci, pi, obs)
+        stats = [p.track_stats for p in problems]
+        L = build_batch_layout(cam_counts, pt_counts, ci, pi, obs, ints=ints, obs_counts=obs_counts,
+                               track_stats=None if any(t is None for t in stats) else stats)
         self.layout = L
         S = L.num_slices
         NQ = 32 * S

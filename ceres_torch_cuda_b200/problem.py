@@ -291,16 +291,50 @@ class BundleAdjustmentProblem:
     camera_constant: Optional[torch.Tensor] = None
     point_constant: Optional[torch.Tensor] = None
     _engine_cache: dict = field(default_factory=dict, repr=False)
+    _track_stats: Optional[tuple] = field(default=None, repr=False)
+
+    # host statistics are taken for problems up to this many observations (the batched
+    # and served sizes); larger problems go through the single-problem path
+    TRACK_STATS_MAX = 1 << 20
 
     @classmethod
     def from_arrays(cls, cameras, points, observations, camera_index, point_index, *, loss=None,
                     device: str | torch.device = "cuda", camera_constant=None, point_constant=None):
         def t(x, dt):
             return torch.as_tensor(x).to(device=device, dtype=dt).contiguous()
-        return cls(t(cameras, torch.float64), t(points, torch.float64), t(observations, torch.float64),
+        prob = cls(t(cameras, torch.float64), t(points, torch.float64), t(observations, torch.float64),
                    t(camera_index, torch.int64), t(point_index, torch.int64), loss,
                    None if camera_constant is None else t(camera_constant, torch.bool),
                    None if point_constant is None else t(point_constant, torch.bool))
+        if not isinstance(camera_index, torch.Tensor) or camera_index.device.type == "cpu":
+            ci = np.asarray(camera_index.cpu() if isinstance(camera_index, torch.Tensor) else camera_index,
+                            dtype=np.int64).reshape(-1)
+            pi = np.asarray(point_index.cpu() if isinstance(point_index, torch.Tensor) else point_index,
+                            dtype=np.int64).reshape(-1)
+            if ci.size <= cls.TRACK_STATS_MAX and ci.size == pi.size:
+                prob._set_track_stats(ci, pi)
+        return prob
+
+    def _set_track_stats(self, ci: np.ndarray, pi: np.ndarray) -> None:
+        """Record, from the host copy of the indices, the most observations of one point
+        and whether a camera observes a point more than once, tied to the index tensors'
+        version counters (an in-place change of either drops them)."""
+        no, npts, nc = ci.size, self.num_points, self.num_cameras
+        if no == 0 or pi.min() < 0 or pi.max() >= npts or ci.min() < 0 or ci.max() >= nc:
+            return
+        max_track = int(np.bincount(pi, minlength=npts).max())
+        key = np.sort(pi * max(nc, 1) + ci)
+        dup = bool(no > 1 and (key[1:] == key[:-1]).any())
+        self._track_stats = (max_track, dup, self.camera_index._version, self.point_index._version)
+
+    @property
+    def track_stats(self) -> Optional[tuple[int, bool]]:
+        """(most observations of one point, whether a camera observes a point twice), when
+        recorded from host indices and the index tensors are unchanged since; else None."""
+        st = self._track_stats
+        if st is None or st[2] != self.camera_index._version or st[3] != self.point_index._version:
+            return None
+        return st[0], st[1]
 
     @classmethod
     def from_bal_text(cls, text: str, *, loss=None, device: str | torch.device = "cuda"):

@@ -195,3 +195,43 @@ def test_batch_autotune_shapes_give_the_same_float64_results():
         np.testing.assert_allclose(costs, first, rtol=1e-10, err_msg=str(shape))
     chosen = B.autotune(_options(), _problems(datas), precision="fp64")
     assert tuple(chosen) in {tuple(s) for s in B.SHAPES}
+
+
+def test_batch_layout_from_host_track_stats():
+    """With each problem's largest track and duplicate flag known on the host, the slot
+    count comes from the bound sum_p (32 max_track_p + no_p) and no device read is made;
+    every array equals the one built with the read (the extra slots are padding)."""
+    datas = S.make_batched_instances(7, seed=5, max_points=200)
+    cam_counts, pt_counts, co, po, ci, pi, obs = _concat(datas)
+    ref = build_batch_layout(cam_counts, pt_counts, ci, pi, obs)
+    stats, counts = [], []
+    for d in datas:
+        track = np.bincount(d.point_index, minlength=d.num_points)
+        stats.append((int(track.max()), False))
+        counts.append(d.num_observations)
+    L = build_batch_layout(cam_counts, pt_counts, ci, pi, obs, obs_counts=np.array(counts), track_stats=stats)
+    assert L.num_slots >= ref.num_slots
+    assert L.num_slots == sum(32 * t + n for (t, _), n in zip(stats, counts))
+    assert L.has_duplicate_cameras == ref.has_duplicate_cameras
+    for name in ("slice_base", "slice_len", "cam_offsets", "cam_entries", "lane_point", "cam_off", "slice_off"):
+        np.testing.assert_array_equal(getattr(L, name).numpy(), getattr(ref, name).numpy())
+    n = ref.num_slots
+    np.testing.assert_array_equal(L.slot_cam.numpy()[:n], ref.slot_cam.numpy()[:n])
+    np.testing.assert_array_equal(L.slot_obs.numpy()[:n], ref.slot_obs.numpy()[:n])
+    assert (L.slot_cam.numpy()[n:] == -1).all()
+
+
+def test_track_stats_follow_the_index_tensors():
+    import ceres_torch_cuda_b200 as tc
+
+    d = S.make_small_ba(6, 80, 3, seed=2)
+    ci = np.concatenate([d.camera_index, d.camera_index[:1]])
+    pi = np.concatenate([d.point_index, d.point_index[:1]])
+    ob = np.concatenate([d.observations, d.observations[:1]])
+    p = tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, ob, ci, pi, device="cpu")
+    assert p.track_stats == (int(np.bincount(pi).max()), True)
+    q = tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, d.observations, d.camera_index,
+                                               d.point_index, device="cpu")
+    assert q.track_stats == (int(np.bincount(d.point_index).max()), False)
+    q.point_index[0] = 1  # an in-place change drops the statistics
+    assert q.track_stats is None
