@@ -2245,6 +2245,10 @@ bool valid(const ceres_b200_ba_t* ba) {
   if (ba->num_cameras > 0 && (!ba->cam_offsets || !ba->cam_const || !ba->cam_diag || !ba->rhs || !ba->precond))
     return false;
   if ((reinterpret_cast<uintptr_t>(ba->jac) & 31) != 0) return false;  // 256-bit record loads
+  // the camera reduction's cp.async copies: 16-byte residual pairs, 8-byte W^-1 pieces
+  if ((reinterpret_cast<uintptr_t>(ba->res) & 15) != 0 || (reinterpret_cast<uintptr_t>(ba->winv) & 7) != 0 ||
+      (reinterpret_cast<uintptr_t>(ba->winv_ga) & 7) != 0)
+    return false;
   if (ba->num_observations > 0) {
     if (!ba->cam_entries || !ba->cam_items || !ba->items || ba->num_items <= 0) return false;
     if (ba->cm_jac && (!ba->slot_pos || (reinterpret_cast<uintptr_t>(ba->cm_jac) & 31) != 0)) return false;

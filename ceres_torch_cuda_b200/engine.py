@@ -32,7 +32,7 @@ _PRECOND = {
     PreconditionerType.CLUSTER_TRIDIAGONAL: _lib.PRECOND_CLUSTER,
 }
 _CLUSTER_MAX_DIM = 16384  # 9 x cameras of the largest component (the sweep's 32-bit element index)
-SCHUR_ORDER_MAX = 1 << 26  # contributions of the ordered explicit S (12 B each); longer lists sum with atomics
+SCHUR_ORDER_MAX = 1 << 24  # contributions of the ordered explicit S (12 B each); longer lists sum with atomics
 
 PRECISIONS = ("fp64", "mixed")
 

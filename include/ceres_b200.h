@@ -147,12 +147,12 @@ typedef struct ceres_b200_ba_t {
 
   /* per-slot evaluation */
   void* jac;                   /* [num_slots][24] float or double, 32-byte aligned */
-  double* res;                 /* [num_slots][2] corrected residuals */
+  double* res;                 /* [num_slots][2] corrected residuals, 16-byte aligned */
 
   /* point-side Schur pieces */
   double* point_raw;           /* [num_points][9] J_p^T J_p (symmetric, 6) and J_p^T r (3), written by evaluate */
-  void* winv;                  /* [num_points][6] (W + D_p)^-1, symmetric, float or double */
-  double* winv_ga;             /* [num_points][3] W^-1 g_a with g_a = -J_p^T r */
+  void* winv;                  /* [num_points][6] (W + D_p)^-1, symmetric, float or double, 8-byte aligned */
+  double* winv_ga;             /* [num_points][3] W^-1 g_a with g_a = -J_p^T r, 8-byte aligned */
   double* step_points;         /* [num_points][3] */
 
   /* camera-side Schur pieces */

@@ -97,3 +97,13 @@ def test_invalid_arguments_are_rejected_without_a_gpu(lib):
     assert lib.ceres_b200_ba_cluster_factor(ctypes.byref(s), ctypes.byref(cl), None) == _lib.EINVAL
     assert lib.ceres_b200_ba_cluster_factor(ctypes.byref(s), None, None) == _lib.EINVAL
     assert lib.ceres_b200_ba_pcg_cluster(ctypes.byref(s), ctypes.byref(cl), 0, 10, 0.1, 0, None) == _lib.EINVAL
+    # misaligned sources of the camera reduction's asynchronous copies (addresses only,
+    # never dereferenced: the check comes first)
+    for field, addr in (("res", 0x10008), ("winv", 0x10004), ("winv_ga", 0x10004), ("jac", 0x10010)):
+        s = _lib.BAStruct()
+        s.precision = _lib.FP32
+        s.counters, s.stats = 0x10000, 0x10000
+        s.jac, s.res, s.winv, s.winv_ga = 0x10000, 0x10000, 0x10000, 0x10000
+        s.scratch, s.cand_cameras, s.cand_points, s.step_points = 0x10000, 0x10000, 0x10000, 0x10000
+        setattr(s, field, addr)  # every other argument of the step passes its check
+        assert lib.ceres_b200_ba_step(ctypes.byref(s), None) == _lib.EINVAL, field
