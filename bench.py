@@ -760,6 +760,7 @@ def serving_result(rate: float, duration: float) -> dict:
         out[prec] = st
     rel = [abs(a - b) / max(b, 1e-300) for a, b in zip(out["mixed"].pop("final_costs"), out["fp64"].pop("final_costs"))]
     m = out["mixed"]
+    shape_srv = server  # the settings both streams ran with (the defaults)
     line = {
         "metric": "served BA solve latency p99 (configuration 4, continuous batching)", "value": m["p99_ms"],
         "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": m["wall_s"] * 1e3,
@@ -768,8 +769,9 @@ def serving_result(rate: float, duration: float) -> dict:
                                f"track~Poisson(4)+2", "requests": count,
                    "observations": int(sum(d.num_observations for d in datas)),
                    "server": {"cluster_size": "4 / 8 / 16 below 20k / 80k / above observations",
-                              "max_inflight": 16, "max_batch": 16, "min_batch": 4, "batch_window_ms": 1.0,
-                              "threads_per_cta": 256}},
+                              "max_inflight": shape_srv.max_inflight, "max_batch": shape_srv.max_batch,
+                              "min_batch": shape_srv.min_batch, "batch_window_ms": 1e3 * shape_srv.batch_window_s,
+                              "threads_per_cta": shape_srv.threads_per_cta, "ctas_per_sm": shape_srv.ctas_per_sm}},
         "mixed": m, "fp64": out["fp64"],
         "max_rel_final_cost_mixed_vs_fp64": max(rel), "median_rel_final_cost_mixed_vs_fp64": statistics.median(rel),
         "e2e": {"value": m["p99_ms"], "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,

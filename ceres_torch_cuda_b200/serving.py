@@ -107,6 +107,12 @@ class BAServer:
     (``size_classes``: small requests on small clusters leave room for more of them). A launch waits until ``min_batch`` requests are waiting or
     the oldest has waited ``batch_window_s`` (fewer, larger launches for less host time
     per request).
+
+    ``threads_per_cta`` x ``ctas_per_sm``: the batched kernel's CTA shape. 128 x 4 (the
+    kernel at 128 registers, four CTAs per SM) holds four times the requests of 256 x 1
+    on the GPU at once; measured on configuration-4 streams (mixed): 4,827 instead of
+    3,628 solves/s at 5,000 req/s, p99 30 instead of 155-271 ms at 2,000 req/s, and
+    p99 about 20 ms at 1,000 req/s either way.
     """
 
     options: SolverOptions
@@ -114,8 +120,8 @@ class BAServer:
     memory_budget: int | None = None
     max_inflight: int = 16
     max_batch: int = 16
-    threads_per_cta: int = 256
-    ctas_per_sm: int = 1
+    threads_per_cta: int = 128
+    ctas_per_sm: int = 4
     cluster_size: int = 0                # 0: by request size (size_classes)
     size_classes: tuple = ((20_000, 4), (80_000, 8), (None, 16))  # (observations below, cluster size)
     min_batch: int = 4                   # launch once this many requests wait ...

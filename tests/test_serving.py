@@ -39,7 +39,9 @@ def test_server_results_equal_alone_and_batches_overlap():
     server.drain()
     assert server.launches >= 4
     assert server.peak_inflight >= 2
-    alone = [tc.solve_batch(opts, [p], precision="fp64", cluster_size=1 if p.num_observations < cut else 2)[0]
+    # the same CTA shape as the server's (the shape fixes the order of the block sums)
+    alone = [tc.solve_batch(opts, [p], precision="fp64", cluster_size=1 if p.num_observations < cut else 2,
+                            threads_per_cta=server.threads_per_cta, ctas_per_sm=server.ctas_per_sm)[0]
              for p in probs()]
     for r, a in zip(reqs, alone):
         assert r.summary is not None and r.latency is not None and r.latency >= 0
@@ -71,7 +73,8 @@ def test_mixed_server_results_equal_alone():
     reqs = [server.submit(p) for p in probs()]
     server.drain()
     assert server.peak_inflight >= 2
-    alone = [tc.solve_batch(opts, [p], precision="mixed", cluster_size=1)[0] for p in probs()]
+    alone = [tc.solve_batch(opts, [p], precision="mixed", cluster_size=1, threads_per_cta=server.threads_per_cta,
+                            ctas_per_sm=server.ctas_per_sm)[0] for p in probs()]
     for r, a in zip(reqs, alone):
         assert r.summary.final_cost == a.final_cost
         assert [it.cost for it in r.summary.iterations] == [it.cost for it in a.iterations]
