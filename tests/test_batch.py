@@ -228,10 +228,11 @@ def test_track_stats_follow_the_index_tensors():
     ci = np.concatenate([d.camera_index, d.camera_index[:1]])
     pi = np.concatenate([d.point_index, d.point_index[:1]])
     ob = np.concatenate([d.observations, d.observations[:1]])
-    p = tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, ob, ci, pi, device="cpu")
+    p = tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, ob, ci, pi, device="cpu", track_stats=True)
     assert p.track_stats == (int(np.bincount(pi).max()), True)
+    assert tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, ob, ci, pi, device="cpu").track_stats is None
     q = tc.BundleAdjustmentProblem.from_arrays(d.cameras, d.points, d.observations, d.camera_index,
-                                               d.point_index, device="cpu")
+                                               d.point_index, device="cpu", track_stats=True)
     assert q.track_stats == (int(np.bincount(d.point_index).max()), False)
     q.point_index[0] = 1  # an in-place change drops the statistics
     assert q.track_stats is None
