@@ -236,3 +236,28 @@ def test_track_stats_follow_the_index_tensors():
     assert q.track_stats == (int(np.bincount(d.point_index).max()), False)
     q.point_index[0] = 1  # an in-place change drops the statistics
     assert q.track_stats is None
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_slot_bound_holds_for_any_track_lengths(seed):
+    """The host slot bound used without a device read: for track lengths sorted in
+    descending order and cut into slices of 32, 32 * sum of the slice maxima is at most
+    32 * max_track + no (each slice after the first is no longer than the mean of the
+    slice before it)."""
+    rng = np.random.default_rng(seed)
+    npts = int(rng.integers(1, 3000))
+    kind = seed % 4
+    if kind == 0:
+        c = rng.integers(1, 8, npts)
+    elif kind == 1:
+        c = rng.geometric(0.2, npts)
+    elif kind == 2:  # one very long track among short ones
+        c = np.ones(npts, dtype=np.int64)
+        c[rng.integers(npts)] = int(rng.integers(50, 5000))
+    else:  # steps just across slice boundaries
+        c = np.repeat(rng.integers(1, 40, (npts + 32) // 33), 33)[:npts]
+    c = np.sort(c)[::-1]
+    pad = np.zeros(32 * ((npts + 31) // 32), dtype=np.int64)
+    pad[:npts] = c
+    slots = 32 * int(pad.reshape(-1, 32).max(axis=1).sum())
+    assert slots <= 32 * int(c.max()) + int(c.sum())
