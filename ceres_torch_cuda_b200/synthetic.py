@@ -250,7 +250,7 @@ def make_sequence_ba(num_cameras: int, num_points: int, window: int, *, seed: in
 
 def make_small_ba(num_cameras: int, num_points: int, track: int, *, seed: int = 0, loss=("trivial",),
                   outlier_fraction: float = 0.0) -> BAData:
-    """Small instance with the configs[0] camera/point model (tests, fixtures)."""
+    """Small instance with the configuration-0 camera/point model (tests, fixtures)."""
     return make_uniform_ba(num_cameras, num_points, track, seed=seed, loss=loss,
                            outlier_fraction=outlier_fraction)
 
@@ -305,4 +305,4 @@ def ba_config(index: int, *, scale: float = 1.0, seed: int | None = None) -> BAD
         return make_ring_ba(max(3, int(1500 * min(1.0, scale * 10))), max(1, int(1_000_000 * scale)),
                             seed=102 if seed is None else seed,
                             description="config2 ring nc=1500 np=1000000 track=Geometric(0.2)+2<=100 cauchy(2)")
-    raise ValueError("configs 3 and 4 are collections; use make_batched_instances / make_serving_requests")
+    raise ValueError("configurations 3 and 4 are collections; use make_batched_instances / make_serving_requests")
