@@ -35,6 +35,9 @@ def footprint_bytes(problem: BundleAdjustmentProblem, precision: str) -> int:
     jb = 4 if precision == "mixed" else 8
     no, npts, nc = problem.num_observations, problem.num_points, problem.num_cameras
     slots = int(no * 1.15) + 32 * 8
+    stats = getattr(problem, "track_stats", None)
+    if stats is not None:  # the batch allocates the host bound's slot count for these
+        slots = max(slots, 32 * int(stats[0]) + no)
     nq = 32 * ((npts + 31) // 32)
     per_slot = 24 * jb + 16 + 16 + 4
     per_obs = 8 + 64  # camera-major entry and layout-building temporaries

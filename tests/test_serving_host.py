@@ -155,3 +155,13 @@ def test_inflight_cap_and_distinct_streams(fakes):
     assert s.launches == 3
     running = [id(f.stream) for f in s._flights]
     assert len(running) == len(set(running)) == 2
+
+
+def test_footprint_covers_the_host_slot_bound():
+    """A request with host track statistics is laid out with 32 max_track + no slots; its
+    footprint counts at least that many."""
+    long_track = SimpleNamespace(num_observations=6000, num_cameras=10, num_points=1000, track_stats=(5000, False))
+    plain = SimpleNamespace(num_observations=6000, num_cameras=10, num_points=1000)
+    per_slot = 24 * 4 + 16 + 16 + 4
+    assert SV.footprint_bytes(long_track, "mixed") - SV.footprint_bytes(plain, "mixed") == \
+        per_slot * (32 * 5000 + 6000 - (int(6000 * 1.15) + 256))
